@@ -1,0 +1,144 @@
+/*
+ * mat3d_b200.h -- C ABI of the B200 FFT-homogenization solver (libmat3d_b200.so).
+ *
+ * Plain C: opaque handle, plain pointers and sizes, int status codes.  The
+ * drop-in C++ classes FFT_Analysis3D / FFT_analysis3d_thermal
+ * (include/FFT_analysis3D.hpp, include/FFT_thermal3D.hpp) and the Python
+ * package are thin layers over these calls.
+ *
+ * Each entry point replaces a public method of the reference classes
+ * (paths are relative to the reference project, FayyazNo/MAT3d):
+ *   m3d_create                 FFT_Analysis3D(Nx,Ny,Nz,mater_behav)      include/FFT_analysis3D.hpp:196
+ *                              FFT_analysis3d_thermal(Nx,Ny,Nz)          include/FFT_thermal3D.hpp:133
+ *   m3d_set_material_mech      FFT_Analysis3D::material(mat,RVE,noPh)    include/FFT_analysis3D.hpp:200
+ *   m3d_set_material_thermal   FFT_analysis3d_thermal::material(km,ki,RVE) include/FFT_thermal3D.hpp:138
+ *   m3d_set_load               setLoad(E,X0) / setLoad(E)                include/FFT_analysis3D.hpp:202, FFT_thermal3D.hpp:140
+ *   m3d_run                    runAnalysis(tol_field,tol_eq[,nInc])      include/FFT_analysis3D.hpp:206, FFT_thermal3D.hpp:145
+ *   m3d_homogenize             homogenization(tol_field,tol_eq,name)     include/FFT_analysis3D.hpp:209, FFT_thermal3D.hpp:148
+ *   m3d_get_field              public fields epsilon/sigma, tempGradient/heatFlux,
+ *                              epsilon_p_eff, d                          include/FFT_analysis3D.hpp:98-99,146,152;
+ *                                                                        FFT_thermal3D.hpp:82,92
+ *   m3d_get_means / m3d_get_stats / m3d_get_increments
+ *                              epHomo/sigHomo, prop_homogenized, the per-iteration
+ *                              console report of convergenceCheck        src/3d/FFT_analysis3D.cpp:394-412,722-746
+ *   m3d_destroy                ~FFT_Analysis3D / ~FFT_analysis3d_thermal
+ *   m3d_get_stream / m3d_set_stream
+ *                              no counterpart (the reference is CPU-only); lets a
+ *                              caller order the solve on its own CUDA stream
+ *
+ * Layout conventions (as the reference): grid Nx x Ny x Nz, voxel index
+ * v = z + Nz*(y + Ny*x); fields exchanged as AoS doubles out[v*c + comp]
+ * (the reference's Eigen 6 x N^3 / 3 x N^3 column-major storage); Voigt order
+ * [11,22,33,23,13,12] with tensor (not engineering) shear; phase id 1 =
+ * matrix, 0 = inclusion.
+ *
+ * Errors: every call returns an m3d_status; none exits the process.  The
+ * message of the last failure on the calling thread is m3d_last_error().
+ * Threading: one handle = one CUDA stream; a handle must not be used by two
+ * threads at once; different handles are independent.
+ */
+#ifndef MAT3D_B200_H
+#define MAT3D_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define M3D_ABI_VERSION 1
+
+typedef enum {
+    M3D_OK = 0,
+    M3D_ERR_ARG = 1,           /* invalid argument */
+    M3D_ERR_CUDA = 2,          /* CUDA runtime error (no device, launch failure...) */
+    M3D_ERR_OOM = 3,           /* device allocation failed */
+    M3D_NOT_CONVERGED = 4,     /* iteration cap reached (results still available) */
+    M3D_ERR_NAN = 5,           /* non-finite residual */
+    M3D_ERR_STATE = 6,         /* call order violated (e.g. run before material) */
+    M3D_ERR_UNSUPPORTED = 7,   /* valid request this build does not provide */
+    M3D_ERR_TIMEOUT = 8        /* a bounded device wait expired */
+} m3d_status;
+
+enum { M3D_KIND_MECH = 1, M3D_KIND_THERMAL = 2 };
+/* mater_behav "e", "ep", "ed" (src/3d/FFT_analysis3D.cpp:56-98,610-617) */
+enum { M3D_BEHAV_ELASTIC = 0, M3D_BEHAV_J2 = 1, M3D_BEHAV_DAMAGE = 2 };
+/* arithmetic of the sweeps: FP64; FP32; FP32 sweeps with FP64 defect correction */
+enum { M3D_PREC_FP64 = 0, M3D_PREC_FP32 = 1, M3D_PREC_FP32_REFINE = 2 };
+/* stop rule: the reference's stationarity test (convergenceCheck), or the
+   rms residual |x_c - x| / |E| of the accelerated scheme */
+enum { M3D_CRIT_REFERENCE = 0, M3D_CRIT_RESIDUAL = 1 };
+/* scheme: automatic as the reference, strain/gradient-based, stress/flux-based */
+enum { M3D_SCHEME_AUTO = 0, M3D_SCHEME_PRIMAL = 1, M3D_SCHEME_DUAL = 2 };
+/* fields: strain (temperature gradient), stress (heat flux), eq. plastic strain, damage */
+enum { M3D_FIELD_STRAIN = 0, M3D_FIELD_STRESS = 1, M3D_FIELD_EPS_P = 2, M3D_FIELD_DAMAGE = 3 };
+
+typedef struct m3d_solver m3d_solver;
+
+typedef struct {
+    long long sweeps;        /* all sweeps (FP32 + FP64) of the last run, summed over the batch */
+    long long sweeps_fp64;   /* FP64 sweeps among them */
+    long long sweeps_fp32;   /* FP32 sweeps among them */
+    int iters;               /* sweeps of batch entry 0 in its last solve (reference itNo) */
+    int scheme;              /* 1 strain/gradient-based, 2 stress/flux-based */
+    int status;              /* status of the last run */
+    int n_increments;        /* increments completed (ep/ed) */
+    double residual;         /* last residual of entry 0 */
+    double eqvar;            /* last reference equilibrium variable of entry 0 */
+    double diff_sum;         /* last reference diff_sum_field of entry 0 */
+    double diff_eq;          /* last reference diff_avr_eqVar of entry 0 */
+    double solve_ms;         /* wall time of the last run/homogenize on the stream */
+    double la0, mu0;         /* reference medium (mech) */
+    double k0;               /* reference conductivity (thermal) */
+    double vol_fraction[16]; /* per phase id */
+    long long kernel_launches; /* kernels this handle launched since creation */
+} m3d_stats;
+
+/* Create a solver for an Nx x Ny x Nz grid.  `batch` independent solves
+   (load cases) share the phase map and run together. */
+int m3d_create(int kind, int Nx, int Ny, int Nz, int behav, int precision, int batch, m3d_solver** out);
+int m3d_destroy(m3d_solver* h);
+
+/* Phase properties, rows [E, nu, sigma_y, H, n, P, Y0] (row-major nph x 7), and
+   the phase id of every voxel (0 <= id < nph, at most 16 phases). */
+int m3d_set_material_mech(m3d_solver* h, const double* mat, int nph, const int32_t* phase, int scheme);
+/* km: matrix (id != 0), ki: inclusion (id == 0). */
+int m3d_set_material_thermal(m3d_solver* h, double km, double ki, const int32_t* phase, int scheme);
+
+/* Load of batch entry b (b = -1: all entries): E has 6 (mech) or 3 (thermal)
+   values; X0 (mech, may be NULL) is the stress direction of mixed control. */
+int m3d_set_load(m3d_solver* h, int b, const double* E, const double* X0);
+
+/* One analysis of every batch entry (runAnalysis). nInc is the number of load
+   increments (ep/ed; ignored for e and thermal).  max_iter <= 0 picks the
+   reference's caps (2000 mech, 500 thermal). */
+int m3d_run(m3d_solver* h, double tol_field, double tol_eq, int nInc, int criterion, int max_iter);
+
+/* Effective tensor from 6 (mech) / 3 (thermal) load cases run as one batch
+   (homogenization).  Ceff, Seff: 36 or 9 doubles, row-major.  ep_means,
+   sig_means (optional): the reference's epHomo / sigHomo matrices. */
+int m3d_homogenize(m3d_solver* h, double tol_field, double tol_eq, int criterion, int max_iter, double* Ceff,
+                   double* Seff, double* ep_means, double* sig_means);
+
+/* Copy a field of batch entry b to host memory: AoS doubles out[v*c + comp]
+   (c = 6 mech, 3 thermal; scalar fields: out[v]). */
+int m3d_get_field(m3d_solver* h, int which, int b, double* out);
+/* Volume averages of the strain-like and stress-like fields of entry b. */
+int m3d_get_means(m3d_solver* h, int b, double* strain_mean, double* stress_mean);
+int m3d_get_stats(const m3d_solver* h, m3d_stats* out);
+/* Per-increment averages of the ep/ed path (prop_homogenized, nInc x 9). */
+int m3d_get_increments(const m3d_solver* h, double* out, int max_rows);
+
+/* The CUDA stream (cudaStream_t) all work of the handle is ordered on.
+   m3d_set_stream replaces it with a caller-owned stream (NULL: the handle's own). */
+void* m3d_get_stream(const m3d_solver* h);
+int m3d_set_stream(m3d_solver* h, void* stream);
+
+const char* m3d_status_string(int status);
+const char* m3d_last_error(void);
+int m3d_abi_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,325 @@
+"""mat3d_b200 -- B200-native FFT homogenization (Lippmann-Schwinger) solver.
+
+Python host layer over the C ABI of ``libmat3d_b200.so`` (include/mat3d_b200.h).
+It mirrors the reference's two solver classes (FayyazNo/MAT3d
+include/FFT_analysis3D.hpp:36-215 and include/FFT_thermal3D.hpp:37-154):
+same class names, method names, argument meaning and public result fields,
+with numpy arrays in place of Eigen matrices (``epsilon``/``sigma`` are
+``(6, N^3)`` arrays laid out like the reference's column-major 6 x N^3
+matrices, i.e. voxel-major in memory).
+
+There is no CPU fallback: the solve always runs on the GPU, and importing the
+library raises if the compiled extension is missing.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+__all__ = [
+    "Solver", "FFT_Analysis3D", "FFT_analysis3d_thermal", "load_library", "M3DError",
+    "KIND_MECH", "KIND_THERMAL", "ELASTIC", "J2", "DAMAGE", "FP64", "FP32", "FP32_REFINE",
+    "CRIT_REFERENCE", "CRIT_RESIDUAL",
+]
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libmat3d_b200.so")
+
+KIND_MECH, KIND_THERMAL = 1, 2
+ELASTIC, J2, DAMAGE = 0, 1, 2
+FP64, FP32, FP32_REFINE = 0, 1, 2
+CRIT_REFERENCE, CRIT_RESIDUAL = 0, 1
+SCHEME_AUTO, SCHEME_PRIMAL, SCHEME_DUAL = 0, 1, 2
+FIELD_STRAIN, FIELD_STRESS, FIELD_EPS_P, FIELD_DAMAGE = 0, 1, 2, 3
+OK, NOT_CONVERGED = 0, 4
+
+_PRECISIONS = {"fp64": FP64, "fp32": FP32, "fp32_refine": FP32_REFINE, FP64: FP64, FP32: FP32, FP32_REFINE: FP32_REFINE}
+_BEHAV = {"e": ELASTIC, "ep": J2, "ed": DAMAGE}
+
+
+class M3DError(RuntimeError):
+    def __init__(self, status, msg):
+        super().__init__(f"{msg} (status {status})")
+        self.status = status
+
+
+class Stats(ctypes.Structure):
+    _fields_ = [
+        ("sweeps", ctypes.c_longlong), ("sweeps_fp64", ctypes.c_longlong), ("sweeps_fp32", ctypes.c_longlong),
+        ("iters", ctypes.c_int), ("scheme", ctypes.c_int), ("status", ctypes.c_int), ("n_increments", ctypes.c_int),
+        ("residual", ctypes.c_double), ("eqvar", ctypes.c_double), ("diff_sum", ctypes.c_double),
+        ("diff_eq", ctypes.c_double), ("solve_ms", ctypes.c_double), ("la0", ctypes.c_double),
+        ("mu0", ctypes.c_double), ("k0", ctypes.c_double), ("vol_fraction", ctypes.c_double * 16),
+        ("kernel_launches", ctypes.c_longlong),
+    ]
+
+    def as_dict(self):
+        d = {k: getattr(self, k) for k, _ in self._fields_ if k != "vol_fraction"}
+        d["vol_fraction"] = list(self.vol_fraction)
+        return d
+
+
+_lib = None
+
+# every symbol the C ABI header declares
+EXPORTS = [
+    "m3d_create", "m3d_destroy", "m3d_set_material_mech", "m3d_set_material_thermal", "m3d_set_load", "m3d_run",
+    "m3d_homogenize", "m3d_get_field", "m3d_get_means", "m3d_get_stats", "m3d_get_increments",
+    "m3d_status_string", "m3d_last_error", "m3d_abi_version", "m3d_get_stream", "m3d_set_stream",
+]
+
+
+def load_library(path: str | None = None):
+    """Load libmat3d_b200.so (built in-tree by ``python -m mat3d_b200.build``)."""
+    global _lib
+    if _lib is not None and path is None:
+        return _lib
+    p = path or LIB_PATH
+    if not os.path.exists(p):
+        raise ImportError(f"{p} is missing: build it with `python -m mat3d_b200.build` (no CPU fallback exists)")
+    L = ctypes.CDLL(p)
+    vp, i, d, dp = ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.POINTER(ctypes.c_double)
+    L.m3d_create.argtypes = [i, i, i, i, i, i, i, ctypes.POINTER(vp)]
+    L.m3d_destroy.argtypes = [vp]
+    L.m3d_set_material_mech.argtypes = [vp, vp, i, vp, i]
+    L.m3d_set_material_thermal.argtypes = [vp, d, d, vp, i]
+    L.m3d_set_load.argtypes = [vp, i, vp, vp]
+    L.m3d_run.argtypes = [vp, d, d, i, i, i]
+    L.m3d_homogenize.argtypes = [vp, d, d, i, i, vp, vp, vp, vp]
+    L.m3d_get_field.argtypes = [vp, i, i, vp]
+    L.m3d_get_means.argtypes = [vp, i, vp, vp]
+    L.m3d_get_stats.argtypes = [vp, ctypes.POINTER(Stats)]
+    L.m3d_get_increments.argtypes = [vp, vp, i]
+    L.m3d_status_string.restype = ctypes.c_char_p
+    L.m3d_status_string.argtypes = [i]
+    L.m3d_last_error.restype = ctypes.c_char_p
+    L.m3d_abi_version.restype = i
+    for name in EXPORTS:
+        if name not in ("m3d_status_string", "m3d_last_error", "m3d_get_stream"):
+            getattr(L, name).restype = ctypes.c_int
+    L.m3d_get_stream.restype = vp
+    L.m3d_get_stream.argtypes = [vp]
+    L.m3d_set_stream.argtypes = [vp, vp]
+    if path is None:
+        _lib = L
+    return L
+
+
+def _ptr(a):
+    return a.ctypes.data_as(ctypes.c_void_p) if a is not None else None
+
+
+def _check(L, rc, what, allow_not_converged=True):
+    if rc == OK or (allow_not_converged and rc == NOT_CONVERGED):
+        return rc
+    raise M3DError(rc, f"{what}: {L.m3d_status_string(rc).decode()}: {L.m3d_last_error().decode()}")
+
+
+class Solver:
+    """Thin handle over the C ABI (one CUDA stream, `batch` solves at once)."""
+
+    def __init__(self, kind, Nx, Ny, Nz, behav=ELASTIC, precision=FP64, batch=1):
+        self.L = load_library()
+        self.kind, self.shape, self.batch = kind, (Nx, Ny, Nz), batch
+        self.V = Nx * Ny * Nz
+        self.C = 6 if kind == KIND_MECH else 3
+        self.behav = behav
+        h = ctypes.c_void_p()
+        _check(self.L, self.L.m3d_create(kind, Nx, Ny, Nz, behav, _PRECISIONS[precision], batch, ctypes.byref(h)),
+               "m3d_create")
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.m3d_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_material_mech(self, mat, phase, scheme=SCHEME_AUTO):
+        mat = np.ascontiguousarray(mat, np.float64)
+        ph = np.ascontiguousarray(np.asarray(phase).ravel(), np.int32)
+        _check(self.L, self.L.m3d_set_material_mech(self.h, _ptr(mat), mat.shape[0], _ptr(ph), scheme), "material")
+
+    def set_material_thermal(self, km, ki, phase, scheme=SCHEME_AUTO):
+        ph = np.ascontiguousarray(np.asarray(phase).ravel(), np.int32)
+        _check(self.L, self.L.m3d_set_material_thermal(self.h, float(km), float(ki), _ptr(ph), scheme), "material")
+
+    def set_load(self, E, X0=None, b=-1):
+        E = np.ascontiguousarray(E, np.float64)
+        X = None if X0 is None else np.ascontiguousarray(X0, np.float64)
+        _check(self.L, self.L.m3d_set_load(self.h, b, _ptr(E), _ptr(X)), "setLoad")
+
+    def run(self, tol_field, tol_eq=0.0, nInc=1, criterion=CRIT_RESIDUAL, max_iter=0):
+        return _check(self.L, self.L.m3d_run(self.h, tol_field, tol_eq, nInc, criterion, max_iter), "run")
+
+    def homogenize(self, tol_field, tol_eq=0.0, criterion=CRIT_RESIDUAL, max_iter=0):
+        C = self.C
+        Ce, Se, ep, sg = (np.zeros((C, C)) for _ in range(4))
+        rc = _check(self.L, self.L.m3d_homogenize(self.h, tol_field, tol_eq, criterion, max_iter,
+                                                  _ptr(Ce), _ptr(Se), _ptr(ep), _ptr(sg)), "homogenize")
+        return Ce, Se, ep, sg, rc
+
+    def field(self, which=FIELD_STRAIN, b=0):
+        scalar = which in (FIELD_EPS_P, FIELD_DAMAGE)
+        out = np.zeros(self.V if scalar else self.V * self.C)
+        _check(self.L, self.L.m3d_get_field(self.h, which, b, _ptr(out)), "get_field")
+        return out if scalar else out.reshape(self.V, self.C).T  # (C, V) view of AoS data
+
+    def means(self, b=0):
+        e = np.zeros(self.C)
+        s = np.zeros(self.C)
+        _check(self.L, self.L.m3d_get_means(self.h, b, _ptr(e), _ptr(s)), "get_means")
+        return e, s
+
+    def stats(self):
+        st = Stats()
+        _check(self.L, self.L.m3d_get_stats(self.h, ctypes.byref(st)), "get_stats")
+        return st.as_dict()
+
+    def stream_ptr(self):
+        """cudaStream_t of the handle (for timing with events on the launching stream)."""
+        return self.L.m3d_get_stream(self.h)
+
+    def increments(self, max_rows=100000):
+        st = self.stats()
+        n = max(st["n_increments"], 0)
+        out = np.zeros((max(n, 1), 9))
+        rows = self.L.m3d_get_increments(self.h, _ptr(out), n)
+        return out[:rows]
+
+
+def _iso_C(la, mu):
+    C = np.zeros((6, 6))
+    C[:3, :3] = la
+    C[[0, 1, 2], [0, 1, 2]] = la + 2 * mu
+    C[[3, 4, 5], [3, 4, 5]] = 2 * mu
+    return C
+
+
+class FFT_Analysis3D:
+    """Drop-in mirror of the reference's ``FFT_Analysis3D`` (include/FFT_analysis3D.hpp:36-215)."""
+
+    def __init__(self, Nx, Ny, Nz, mater_behav="e", precision="fp64", criterion=CRIT_REFERENCE):
+        if mater_behav not in _BEHAV:
+            raise ValueError('mater_behav must be "e", "ep" or "ed"')
+        self.Nx, self.Ny, self.Nz = Nx, Ny, Nz
+        self.xyz = Nx * Ny * Nz
+        self.mater_behav = mater_behav
+        self.precision = precision
+        self.criterion = criterion
+        self._s = Solver(KIND_MECH, Nx, Ny, Nz, _BEHAV[mater_behav], precision, 1)
+        self.epsilon = np.zeros((6, self.xyz))
+        self.sigma = np.zeros((6, self.xyz))
+
+    # material(), src/3d/FFT_analysis3D.cpp:420-549
+    def material(self, mat, RVE, noPhases=None):
+        mat = np.asarray(mat, np.float64)
+        self.noPhases = mat.shape[0] if noPhases is None else noPhases
+        self._mat = mat[: self.noPhases].copy()
+        self._rve = np.asarray(RVE).ravel().astype(np.int32)
+        self._s.set_material_mech(self._mat, self._rve)
+        st = self._s.stats()
+        self.strainBase = st["scheme"] == 1
+        self.stressBase = not self.strainBase
+        self.la0, self.mu0 = st["la0"], st["mu0"]
+        self.vol_fractions = np.array(st["vol_fraction"][: self.noPhases])
+        El, v = self._mat[:, 0], self._mat[:, 1]
+        self.mu = El / (1 + v) / 2.0
+        self.la = v * El / (1 + v) / (1 - 2 * v)
+        self.K = self.la + 2.0 / 3.0 * self.mu
+        self.C = [_iso_C(self.la[i], self.mu[i]) for i in range(self.noPhases)]
+        self.S = [np.linalg.inv(c) for c in self.C]
+        self.C0 = _iso_C(self.la0, self.mu0)
+        self.S0 = np.linalg.inv(self.C0)
+
+    def setLoad(self, E, X0=None):
+        self.E = np.asarray(E, np.float64).ravel().copy()
+        self.X0 = np.zeros(6) if X0 is None else np.asarray(X0, np.float64).ravel().copy()
+        self._s.set_load(self.E, self.X0)
+
+    def runAnalysis(self, tol_field, tol_eq, nInc=1):
+        rc = self._s.run(tol_field, tol_eq, nInc, self.criterion)
+        self._fetch()
+        return rc
+
+    def _fetch(self, b=0):
+        self.epsilon = np.ascontiguousarray(self._s.field(FIELD_STRAIN, b))
+        self.sigma = np.ascontiguousarray(self._s.field(FIELD_STRESS, b))
+        if self.mater_behav == "ep":
+            self.epsilon_p_eff = self._s.field(FIELD_EPS_P, b)
+        if self.mater_behav == "ed":
+            self.d = self._s.field(FIELD_DAMAGE, b)
+        if self.mater_behav != "e":
+            self.prop_homogenized = self._s.increments()
+        self.itNo = self._s.stats()["iters"]
+
+    # homogenization(), src/3d/FFT_analysis3D.cpp:856-999
+    def homogenization(self, tol_field, tol_eq, outputName=None):
+        if self.mater_behav != "e":
+            s = Solver(KIND_MECH, self.Nx, self.Ny, self.Nz, ELASTIC, self.precision, 6)
+            s.set_material_mech(self._mat, self._rve)
+            self._s, self.mater_behav = s, "e"
+        Ce, Se, ep, sg, _ = self._s.homogenize(tol_field, tol_eq, self.criterion)
+        self.CHomo, self.SHomo, self.epHomo, self.sigHomo = Ce, Se, ep, sg
+        self.E11, self.E22, self.E33 = 1 / Se[0, 0], 1 / Se[1, 1], 1 / Se[2, 2]
+        self._fetch(5)
+        return self.E11 + self.E22 + self.E33
+
+    def stats(self):
+        return self._s.stats()
+
+
+class FFT_analysis3d_thermal:
+    """Drop-in mirror of the reference's ``FFT_analysis3d_thermal`` (include/FFT_thermal3D.hpp:37-154)."""
+
+    def __init__(self, Nx, Ny, Nz, precision="fp64", criterion=CRIT_REFERENCE):
+        self.Nx, self.Ny, self.Nz = Nx, Ny, Nz
+        self.xyz = Nx * Ny * Nz
+        self.criterion = criterion
+        self._s = Solver(KIND_THERMAL, Nx, Ny, Nz, ELASTIC, precision, 1)
+        self._E = None
+
+    def material(self, km, ki, RVE):
+        self._s.set_material_thermal(km, ki, np.asarray(RVE).ravel().astype(np.int32))
+        st = self._s.stats()
+        self.tempGradientBase = st["scheme"] == 1
+        self.heatFluxBase = not self.tempGradientBase
+        self.k0 = st["k0"]
+        self.Km, self.Ki, self.K0 = np.eye(3) * km, np.eye(3) * ki, np.eye(3) * self.k0
+        if self._E is not None:
+            self._s.set_load(self._E)
+
+    def setLoad(self, E):
+        self._E = np.asarray(E, np.float64).ravel().copy()
+        self.E = self._E
+        try:
+            self._s.set_load(self._E)
+        except M3DError:
+            pass
+
+    def runAnalysis(self, tol_field, tol_eq):
+        rc = self._s.run(tol_field, tol_eq, 1, self.criterion)
+        self._fetch()
+        return rc
+
+    def _fetch(self, b=0):
+        self.tempGradient = np.ascontiguousarray(self._s.field(FIELD_STRAIN, b))
+        self.heatFlux = np.ascontiguousarray(self._s.field(FIELD_STRESS, b))
+        self.itNo = self._s.stats()["iters"]
+
+    def homogenization(self, tol_field, tol_eq, filename=None):
+        K, R, g, q, _ = self._s.homogenize(tol_field, tol_eq, self.criterion)
+        self.KHomo, self.RHomo, self.tempGradHomo, self.heatFluxHomo = K, R, g, q
+        self.K11, self.K22, self.K33 = K[0, 0], K[1, 1], K[2, 2]
+        self._fetch(2)
+        return K
+
+    def stats(self):
+        return self._s.stats()

@@ -1,0 +1,217 @@
+// fft_smem.cuh -- mixed-radix Stockham FFT stages on lines held in shared memory.
+//
+// A CTA holds a set of complex lines in shared memory and transforms all of
+// them cooperatively: in each stage every thread loops over (line, butterfly)
+// work items, reads R inputs from buffer `a`, applies the stage twiddles, does
+// an R-point DFT in registers and writes R outputs to buffer `b` (autosort, so
+// the result is in natural order without a bit-reversal pass).  Stage s with
+// radix R and Ns = product of the previous radices:
+//     v[r]  = a[j + r*(n/R)]                    r = 0..R-1, j = 0..n/R-1
+//     v[r] *= w_n^( (j mod Ns) * r * n/(Ns*R) )
+//     v     = DFT_R(v)
+//     b[(j/Ns)*Ns*R + (j mod Ns) + r*Ns] = v[r]
+// Twiddles come from a per-length table tw[m] = exp(-2 pi i m / n) in shared
+// memory (computed on the host in long double); the inverse uses conj().
+// Radices 2, 3, 4, 5 and 8 have dedicated butterflies; any other factor
+// (e.g. 13 for n = 65) uses a direct O(R^2) DFT through the table.
+//
+// Line addressing is two-level so one routine serves every pass layout:
+//     element e of line L lives at  (L / lpg) * gstride + (L % lpg) * lstride + e * estride
+// and `lines_fast` chooses whether consecutive threads walk lines (column
+// tiles: consecutive columns are consecutive words, no bank conflicts) or
+// butterflies (contiguous lines).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace m3d {
+
+constexpr int kMaxStages = 12;
+
+struct LinePlan {
+    int n;
+    int nstages;
+    int radix[kMaxStages];
+};
+
+template <typename T> struct Cx;
+template <> struct Cx<float> { typedef float2 t; };
+template <> struct Cx<double> { typedef double2 t; };
+
+template <typename C2> __device__ __forceinline__ C2 mk(decltype(C2().x) re, decltype(C2().x) im) {
+    C2 r; r.x = re; r.y = im; return r;
+}
+template <typename C2> __device__ __forceinline__ C2 cadd(C2 a, C2 b) { return mk<C2>(a.x + b.x, a.y + b.y); }
+template <typename C2> __device__ __forceinline__ C2 csub(C2 a, C2 b) { return mk<C2>(a.x - b.x, a.y - b.y); }
+template <typename C2> __device__ __forceinline__ C2 cmul(C2 a, C2 b) {
+    return mk<C2>(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+// multiply by -i (sign < 0) or +i (sign > 0)
+template <typename C2> __device__ __forceinline__ C2 crot(C2 a, int sign) {
+    return sign < 0 ? mk<C2>(a.y, -a.x) : mk<C2>(-a.y, a.x);
+}
+template <typename C2> __device__ __forceinline__ C2 twid(const C2* tw, int m, int sign) {
+    C2 w = tw[m];
+    if (sign > 0) w.y = -w.y;
+    return w;
+}
+
+template <typename C2, int R>
+__device__ __forceinline__ void dft_small(C2 (&v)[R], const C2* tw, int n, int sign) {
+    typedef decltype(C2().x) T;
+    if constexpr (R == 2) {
+        C2 a = v[0], b = v[1];
+        v[0] = cadd(a, b);
+        v[1] = csub(a, b);
+    } else if constexpr (R == 4) {
+        C2 a0 = cadd(v[0], v[2]), a1 = csub(v[0], v[2]);
+        C2 b0 = cadd(v[1], v[3]), b1 = crot(csub(v[1], v[3]), sign);
+        v[0] = cadd(a0, b0);
+        v[1] = cadd(a1, b1);
+        v[2] = csub(a0, b0);
+        v[3] = csub(a1, b1);
+    } else if constexpr (R == 8) {
+        const T h = (T)0.70710678118654752440084436210484903928483593768847L;
+        // radix-2 across halves, then two radix-4 on even/odd outputs
+        C2 e[4], o[4];
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+            e[r] = cadd(v[r], v[r + 4]);
+            o[r] = csub(v[r], v[r + 4]);
+        }
+        // o[r] *= w^r with w = exp(sign * i pi / 4) = (h, sg*h)
+        const T sg = (T)sign;
+        {
+            const T x = o[1].x, y = o[1].y;
+            o[1] = mk<C2>(h * (x - sg * y), h * (y + sg * x));
+        }
+        o[2] = crot(o[2], sign);
+        {
+            // w^3 = (-h, sg*h)
+            const T x = o[3].x, y = o[3].y;
+            o[3] = mk<C2>(h * (-x - sg * y), h * (sg * x - y));
+        }
+        // radix-4 on e -> outputs 0,2,4,6 ; on o -> outputs 1,3,5,7
+        C2 a0 = cadd(e[0], e[2]), a1 = csub(e[0], e[2]);
+        C2 b0 = cadd(e[1], e[3]), b1 = crot(csub(e[1], e[3]), sign);
+        C2 c0 = cadd(o[0], o[2]), c1 = csub(o[0], o[2]);
+        C2 d0 = cadd(o[1], o[3]), d1 = crot(csub(o[1], o[3]), sign);
+        v[0] = cadd(a0, b0);
+        v[4] = csub(a0, b0);
+        v[2] = cadd(a1, b1);
+        v[6] = csub(a1, b1);
+        v[1] = cadd(c0, d0);
+        v[5] = csub(c0, d0);
+        v[3] = cadd(c1, d1);
+        v[7] = csub(c1, d1);
+    } else if constexpr (R == 3) {
+        const T c = (T)-0.5L;
+        const T s = (T)0.86602540378443864676372317075293618347140262690519L * (T)(sign < 0 ? -1 : 1);
+        C2 a = v[0], b = v[1], d = v[2];
+        C2 t1 = cadd(b, d);
+        C2 t2 = mk<C2>(a.x + c * t1.x, a.y + c * t1.y);
+        C2 t3 = csub(b, d);  // times i*s
+        C2 t3r = mk<C2>(-s * t3.y, s * t3.x);
+        v[0] = cadd(a, t1);
+        v[1] = cadd(t2, t3r);
+        v[2] = csub(t2, t3r);
+    } else {
+        // direct DFT through the table: w_R^m = tw[m * (n/R)]
+        C2 in[R];
+#pragma unroll
+        for (int q = 0; q < R; ++q) in[q] = v[q];
+        const int st = n / R;
+#pragma unroll
+        for (int s = 0; s < R; ++s) {
+            C2 acc = in[0];
+#pragma unroll
+            for (int q = 1; q < R; ++q) acc = cadd(acc, cmul(in[q], twid(tw, ((q * s) % R) * st, sign)));
+            v[s] = acc;
+        }
+    }
+}
+
+template <typename C2, int R>
+__device__ __forceinline__ void butterfly(const C2* __restrict__ src, C2* __restrict__ dst, int j, int n, int Ns,
+                                          int es, const C2* tw, int sign) {
+    const int nb = n / R;
+    C2 v[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) v[r] = src[(j + r * nb) * es];
+    const int k = j % Ns;
+    if (Ns > 1) {
+        const int step = n / (Ns * R);
+#pragma unroll
+        for (int r = 1; r < R; ++r) v[r] = cmul(v[r], twid(tw, k * r * step, sign));
+    }
+    dft_small<C2, R>(v, tw, n, sign);
+    const int idx = (j / Ns) * Ns * R + k;
+#pragma unroll
+    for (int r = 0; r < R; ++r) dst[(idx + r * Ns) * es] = v[r];
+}
+
+// generic-radix butterfly (any R up to kMaxGenericRadix), run-time R
+constexpr int kMaxGenericRadix = 32;
+template <typename C2>
+__device__ __noinline__ void butterfly_generic(const C2* __restrict__ src, C2* __restrict__ dst, int R, int j, int n,
+                                               int Ns, int es, const C2* tw, int sign) {
+    typedef decltype(C2().x) T;
+    const int nb = n / R;
+    C2 v[kMaxGenericRadix];
+    for (int r = 0; r < R; ++r) v[r] = src[(j + r * nb) * es];
+    const int k = j % Ns;
+    const int step = n / (Ns * R);
+    for (int r = 1; r < R; ++r) v[r] = cmul(v[r], twid(tw, k * r * step, sign));
+    const int st = n / R;
+    const int idx = (j / Ns) * Ns * R + k;
+    for (int s = 0; s < R; ++s) {
+        C2 acc = v[0];
+        for (int q = 1; q < R; ++q) acc = cadd(acc, cmul(v[q], twid(tw, ((q * s) % R) * st, sign)));
+        dst[(idx + s * Ns) * es] = acc;
+    }
+    (void)sizeof(T);
+}
+
+struct LineLayout {
+    int nlines;   // number of lines
+    int lpg;      // lines per group
+    int lstride;  // stride between lines inside a group
+    int gstride;  // stride between groups
+    int estride;  // stride between elements of a line
+    bool lines_fast;
+};
+
+// Transforms every line; returns the buffer (a or b) that holds the result.
+// Must be called by all threads of the CTA; ends with __syncthreads().
+template <typename C2>
+__device__ C2* fft_lines(C2* a, C2* b, const C2* tw, const LinePlan& p, const LineLayout& L, int sign) {
+    const int n = p.n;
+    int Ns = 1;
+    for (int s = 0; s < p.nstages; ++s) {
+        const int R = p.radix[s];
+        const int nb = n / R;
+        const int total = nb * L.nlines;
+        for (int w = threadIdx.x; w < total; w += blockDim.x) {
+            int line, j;
+            if (L.lines_fast) { line = w % L.nlines; j = w / L.nlines; }
+            else { j = w % nb; line = w / nb; }
+            const int base = (line / L.lpg) * L.gstride + (line % L.lpg) * L.lstride;
+            const C2* src = a + base;
+            C2* dst = b + base;
+            switch (R) {
+                case 2: butterfly<C2, 2>(src, dst, j, n, Ns, L.estride, tw, sign); break;
+                case 3: butterfly<C2, 3>(src, dst, j, n, Ns, L.estride, tw, sign); break;
+                case 4: butterfly<C2, 4>(src, dst, j, n, Ns, L.estride, tw, sign); break;
+                case 5: butterfly<C2, 5>(src, dst, j, n, Ns, L.estride, tw, sign); break;
+                case 8: butterfly<C2, 8>(src, dst, j, n, Ns, L.estride, tw, sign); break;
+                default: butterfly_generic<C2>(src, dst, R, j, n, Ns, L.estride, tw, sign); break;
+            }
+        }
+        __syncthreads();
+        C2* t = a; a = b; b = t;
+        Ns *= R;
+    }
+    return a;
+}
+
+}  // namespace m3d

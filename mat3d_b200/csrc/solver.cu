@@ -1,0 +1,1088 @@
+// solver.cu -- host runtime and C ABI of libmat3d_b200.so.
+//
+// A solver handle owns one CUDA stream, the device buffers of its batch and
+// the per-phase constant tables.  A run launches chunks of sweeps (five pass
+// kernels + a finalize kernel each); every kernel reads the device-side done
+// flag of its batch entry, so the host only synchronises once per chunk to
+// read the control blocks.  Chunks of the steady iteration are captured once
+// into CUDA graphs and replayed.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/mat3d_b200.h"
+#include "physics.cuh"
+#include "inelastic.cuh"
+
+using namespace m3d;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int st, const std::string& msg) {
+    g_last_error = msg;
+    return st;
+}
+
+#define M3D_CUDA(call)                                                                                 \
+    do {                                                                                               \
+        cudaError_t e_ = (call);                                                                       \
+        if (e_ != cudaSuccess) {                                                                       \
+            return fail(e_ == cudaErrorMemoryAllocation ? M3D_ERR_OOM : M3D_ERR_CUDA,                 \
+                        std::string(#call) + ": " + cudaGetErrorString(e_));                           \
+        }                                                                                              \
+    } while (0)
+
+// ---- small dense algebra (host, double) ------------------------------------
+typedef std::vector<double> Mat;  // row-major n x n
+
+Mat mat_inv(const Mat& A, int n) {
+    Mat a = A, inv(n * n, 0.0);
+    for (int i = 0; i < n; ++i) inv[i * n + i] = 1.0;
+    for (int c = 0; c < n; ++c) {
+        int piv = c;
+        for (int r = c + 1; r < n; ++r)
+            if (std::fabs(a[r * n + c]) > std::fabs(a[piv * n + c])) piv = r;
+        if (piv != c)
+            for (int j = 0; j < n; ++j) {
+                std::swap(a[c * n + j], a[piv * n + j]);
+                std::swap(inv[c * n + j], inv[piv * n + j]);
+            }
+        const double p = a[c * n + c];
+        for (int j = 0; j < n; ++j) { a[c * n + j] /= p; inv[c * n + j] /= p; }
+        for (int r = 0; r < n; ++r) {
+            if (r == c) continue;
+            const double f = a[r * n + c];
+            if (f == 0.0) continue;
+            for (int j = 0; j < n; ++j) { a[r * n + j] -= f * a[c * n + j]; inv[r * n + j] -= f * inv[c * n + j]; }
+        }
+    }
+    return inv;
+}
+Mat mat_mul(const Mat& A, const Mat& B, int n) {
+    Mat o(n * n, 0.0);
+    for (int i = 0; i < n; ++i)
+        for (int k = 0; k < n; ++k)
+            for (int j = 0; j < n; ++j) o[i * n + j] += A[i * n + k] * B[k * n + j];
+    return o;
+}
+Mat mat_add(const Mat& A, const Mat& B, double s = 1.0) {
+    Mat o(A.size());
+    for (size_t i = 0; i < A.size(); ++i) o[i] = A[i] + s * B[i];
+    return o;
+}
+Mat mat_scale(const Mat& A, double s) {
+    Mat o(A);
+    for (auto& v : o) v *= s;
+    return o;
+}
+Mat iso_stiffness(double la, double mu) {
+    // src/3d/FFT_analysis3D.cpp:457-462 (Voigt, tensor shear)
+    Mat C(36, 0.0);
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) C[i * 6 + j] = la;
+    for (int i = 0; i < 3; ++i) C[i * 6 + i] = la + 2 * mu;
+    for (int i = 3; i < 6; ++i) C[i * 6 + i] = 2 * mu;
+    return C;
+}
+Mat diag(int n, double v) {
+    Mat o(n * n, 0.0);
+    for (int i = 0; i < n; ++i) o[i * n + i] = v;
+    return o;
+}
+
+// ---- FFT plans --------------------------------------------------------------
+bool make_plan(int n, LinePlan& p) {
+    std::vector<int> f;
+    int m = n;
+    while (m % 8 == 0) { f.push_back(8); m /= 8; }
+    while (m % 4 == 0) { f.push_back(4); m /= 4; }
+    while (m % 2 == 0) { f.push_back(2); m /= 2; }
+    for (int q = 3; q <= m; q += 2)
+        while (m % q == 0) { f.push_back(q); m /= q; }
+    if (f.empty()) f.push_back(1);
+    if ((int)f.size() > kMaxStages) return false;
+    for (int r : f)
+        if (r > kMaxGenericRadix) return false;
+    p.n = n;
+    p.nstages = (n == 1) ? 0 : (int)f.size();
+    for (int i = 0; i < kMaxStages; ++i) p.radix[i] = i < (int)f.size() ? f[i] : 1;
+    return true;
+}
+
+template <typename T>
+std::vector<typename Cx<T>::t> twiddles(int n) {
+    std::vector<typename Cx<T>::t> t(n);
+    const long double two_pi = 6.283185307179586476925286766559L;
+    for (int m = 0; m < n; ++m) {
+        const long double a = -two_pi * (long double)m / (long double)n;
+        t[m].x = (T)cosl(a);
+        t[m].y = (T)sinl(a);
+    }
+    return t;
+}
+
+template <class K>
+void allow_smem(K kernel) {
+    cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+}
+
+int even_up(int v) { return (v + 1) & ~1; }
+
+}  // namespace
+
+// ============================================================================
+struct m3d_solver {
+    // configuration
+    int kind = 0, behav = 0, prec = 0, B = 1, C = 6;
+    int Nx = 0, Ny = 0, Nz = 0;
+    GridDims g{};
+    cudaStream_t stream = nullptr;
+    cudaStream_t own_stream = nullptr;
+    bool material_set = false;
+    bool load_set = false;
+    bool run_done = false;
+
+    // model (host)
+    int nph = 0;
+    int scheme = 0;                // 1 primal (strain/gradient), 2 dual (stress/flux)
+    std::vector<double> mat;       // nph x 7
+    std::vector<long long> counts; // voxels per phase
+    std::vector<double> vol;
+    double la0 = 0, mu0 = 0, k0 = 0, km = 0, ki = 0;
+    Mat Cp[kMaxPhases], Sp[kMaxPhases];
+    Mat C0, S0;
+    std::vector<double> hP, hA, hO, hOsum, hQ;  // per phase, C x C (hOsum: C)
+    double den_ref = 0;   // reference stop rule denominator (without V*sum(E))
+    std::vector<double> E;   // B x C
+    std::vector<double> X0;  // B x 6
+
+    // device
+    uint8_t* d_phase = nullptr;
+    void* d_x = nullptr;       // state: T (FP32/FP64) or double (refine)
+    float* d_delta = nullptr;  // refine correction
+    float* d_r32 = nullptr;    // refine defect
+    void* d_spec = nullptr;    // half spectrum (double2 or float2); refine: double2, aliased as float2
+    double* d_part = nullptr;
+    size_t part_cap = 0;
+    Ctl* d_ctl = nullptr;
+    Ctl* d_ctl_in = nullptr;
+    Ctl* h_ctl = nullptr;  // pinned, B entries
+    double* d_mats = nullptr;  // [P | A | O | Osum | Q] blocks
+    size_t off_P = 0, off_A = 0, off_O = 0, off_Os = 0, off_Q = 0;
+    void* d_tw64 = nullptr;  // double2: Nx | Ny | Nz
+    void* d_tw32 = nullptr;  // float2
+    LinePlan px{}, py{}, pz{};
+    double* d_out = nullptr;  // export scratch (C*V doubles)
+    size_t alloc_B = 0;
+
+    // inelastic state (J2 / damage)
+    InelasticState in{};
+
+    // stats
+    m3d_stats st{};
+    std::vector<double> prop;  // nInc x 9
+
+    // launch geometry
+    int G64 = 2, G32 = 2, TZy64 = 8, TZy32 = 16, TZx64 = 4, TZx32 = 8;
+
+    ~m3d_solver();
+    int alloc(int batch);
+    void free_all();
+    template <typename T> int G() const { return sizeof(T) == 8 ? G64 : G32; }
+    template <typename T> int TZy() const { return sizeof(T) == 8 ? TZy64 : TZy32; }
+    template <typename T> int TZx() const { return sizeof(T) == 8 ? TZx64 : TZx32; }
+    template <typename T> typename Cx<T>::t* tw(int axis) const {
+        typedef typename Cx<T>::t C2;
+        C2* base = (C2*)(sizeof(T) == 8 ? d_tw64 : d_tw32);
+        return axis == 0 ? base : (axis == 1 ? base + Nx : base + Nx + Ny);
+    }
+    const double* dm(size_t off) const { return d_mats + off; }
+
+    // sweeps
+    template <typename T, int CC, class Pro, class Spec, class Epi>
+    int launch_sweep(Pro pro, Spec spec, Epi epi, Ctl* ctl, typename Cx<T>::t* sp, int policy, const Ctl* outer);
+    template <typename T, int CC>
+    int launch_check(Ctl* ctl, const void* x, typename Cx<T>::t* sp);
+    template <typename T, int CC>
+    int run_linear(double tol_field, double tol_eq, int criterion, int max_iter);
+    template <int CC>
+    int run_refine(double tol_field, int max_iter);
+    template <typename T, int CC>
+    int launch_em(Ctl* ctl, T* x, const float* r, typename Cx<T>::t* sp, int zero_k0, int policy, const Ctl* outer);
+    int init_ctl(Ctl* dctl, double tol_field, double tol_eq, int max_iter, bool inner);
+    int sync_ctl(Ctl* dctl);
+    int dispatch_run(double tol_field, double tol_eq, int nInc, int criterion, int max_iter);
+    SpecGreen<double, 6> green_params_d6(int zero_k0) const;
+    template <typename T, int CC> SpecGreen<T, CC> green(int zero_k0) const;
+    template <typename T, int CC> int run_inelastic(double tol_field, double tol_eq, int nInc, int criterion, int max_iter);
+};
+
+m3d_solver::~m3d_solver() { free_all(); }
+
+void m3d_solver::free_all() {
+    cudaFree(d_phase); d_phase = nullptr;
+    cudaFree(d_x); d_x = nullptr;
+    cudaFree(d_delta); d_delta = nullptr;
+    cudaFree(d_r32); d_r32 = nullptr;
+    cudaFree(d_spec); d_spec = nullptr;
+    cudaFree(d_part); d_part = nullptr;
+    cudaFree(d_ctl); d_ctl = nullptr;
+    cudaFree(d_ctl_in); d_ctl_in = nullptr;
+    if (h_ctl) cudaFreeHost(h_ctl);
+    h_ctl = nullptr;
+    cudaFree(d_mats); d_mats = nullptr;
+    cudaFree(d_tw64); d_tw64 = nullptr;
+    cudaFree(d_tw32); d_tw32 = nullptr;
+    cudaFree(d_out); d_out = nullptr;
+    in.free_all();
+}
+
+int m3d_solver::alloc(int batch) {
+    // (Re)allocate batch-sized buffers.  Phase map, tables and twiddles are
+    // batch independent and allocated once.
+    const long long V = g.V;
+    const size_t specN = (size_t)batch * C * g.NL * g.Hzp;
+    cudaFree(d_x); cudaFree(d_delta); cudaFree(d_r32); cudaFree(d_spec); cudaFree(d_part);
+    cudaFree(d_ctl); cudaFree(d_ctl_in);
+    if (h_ctl) cudaFreeHost(h_ctl);
+    d_x = nullptr; d_delta = nullptr; d_r32 = nullptr; d_spec = nullptr; d_part = nullptr;
+    d_ctl = nullptr; d_ctl_in = nullptr; h_ctl = nullptr;
+    const size_t xw = (prec == M3D_PREC_FP32) ? 4 : 8;
+    M3D_CUDA(cudaMalloc(&d_x, (size_t)batch * C * V * xw));
+    const size_t sw = (prec == M3D_PREC_FP32) ? 8 : 16;
+    M3D_CUDA(cudaMalloc(&d_spec, specN * sw));
+    M3D_CUDA(cudaMemsetAsync(d_spec, 0, specN * sw, stream));
+    if (prec == M3D_PREC_FP32_REFINE) {
+        M3D_CUDA(cudaMalloc(&d_delta, (size_t)batch * C * V * 4));
+        M3D_CUDA(cudaMalloc(&d_r32, (size_t)batch * C * V * 4));
+    }
+    // partials: max over kernels of blocks x sums x batch
+    const int Gmin = std::min(G32, G64);
+    const size_t zblk = (size_t)((g.NL + Gmin - 1) / Gmin);
+    const int TZmin = std::min(TZx32, TZx64);
+    const size_t xblk = (size_t)Ny * ((g.Hzp + TZmin - 1) / TZmin);
+    // (the pointwise kernels launch up to 592 blocks with up to 13 sums each)
+    part_cap = std::max(std::max(zblk, xblk), (size_t)1024) * (size_t)batch * 16;
+    M3D_CUDA(cudaMalloc(&d_part, part_cap * sizeof(double)));
+    M3D_CUDA(cudaMalloc(&d_ctl, batch * sizeof(Ctl)));
+    M3D_CUDA(cudaMalloc(&d_ctl_in, batch * sizeof(Ctl)));
+    M3D_CUDA(cudaMemsetAsync(d_ctl, 0, batch * sizeof(Ctl), stream));
+    M3D_CUDA(cudaMemsetAsync(d_ctl_in, 0, batch * sizeof(Ctl), stream));
+    M3D_CUDA(cudaMallocHost(&h_ctl, batch * sizeof(Ctl)));
+    alloc_B = batch;
+    B = batch;
+    E.assign((size_t)B * C, 0.0);
+    X0.assign((size_t)B * 6, 0.0);
+    return M3D_OK;
+}
+
+int m3d_solver::init_ctl(Ctl* dctl, double tol_field, double tol_eq, int max_iter, bool inner) {
+    for (int b = 0; b < B; ++b) {
+        Ctl c;
+        std::memset(&c, 0, sizeof(c));
+        c.max_iter = max_iter;
+        c.tol_field = tol_field;
+        c.tol_eq = tol_eq;
+        double es = 0, en = 0;
+        for (int i = 0; i < C; ++i) {
+            const double e = E[b * C + i];
+            c.E[i] = e;
+            c.kzero[i] = e * (double)g.V;
+            es += e;
+            en += ((C == 6 && i >= 3) ? 2.0 : 1.0) * e * e;
+        }
+        c.enorm = std::sqrt(en);
+        if (c.enorm == 0) c.enorm = 1;
+        c.den = (double)g.V * den_ref * es;
+        // sum of the "other" field at the initial uniform state (sum_field_old of the first sweep)
+        double s0 = 0;
+        for (int p = 0; p < nph; ++p) {
+            double o = 0;
+            for (int i = 0; i < C; ++i) o += hOsum[p * C + i] * E[b * C + i];
+            s0 += (double)counts[p] * o;
+        }
+        c.sum_prev = s0;
+        c.inner_tol = inner ? 1e-3 : 0;
+        h_ctl[b] = c;
+    }
+    M3D_CUDA(cudaMemcpyAsync(dctl, h_ctl, B * sizeof(Ctl), cudaMemcpyHostToDevice, stream));
+    return M3D_OK;
+}
+
+int m3d_solver::sync_ctl(Ctl* dctl) {
+    M3D_CUDA(cudaMemcpyAsync(h_ctl, dctl, B * sizeof(Ctl), cudaMemcpyDeviceToHost, stream));
+    M3D_CUDA(cudaStreamSynchronize(stream));
+    return M3D_OK;
+}
+
+template <typename T, int CC>
+SpecGreen<T, CC> m3d_solver::green(int zero_k0) const {
+    SpecGreen<T, CC> s;
+    s.g = g;
+    s.zero_k0 = zero_k0;
+    s.xwrap = Nx;
+    s.pos_nyq = 0;
+    if (kind == M3D_KIND_MECH) {
+        if (scheme == 1) {
+            s.kind = GREEN_STRAIN;
+            s.p1 = (T)(1.0 / (2.0 * mu0));                      // 2*d1, d1 = 1/(4 mu0)   (:162)
+            s.p2 = (T)((la0 + mu0) / (mu0 * (la0 + 2 * mu0)));  // d2                     (:163)
+        } else {
+            s.kind = GREEN_STRESS;
+            const double c1 = 2 * mu0 * (3 * la0 + 2 * mu0) / (la0 + 2 * mu0), c2 = 2 * mu0;  // (:157-160)
+            s.p1 = (T)((c1 - c2) / 2.0);
+            s.p2 = (T)(2.0 * (c2 / 2.0));
+        }
+    } else {
+        if (scheme == 1) {
+            s.kind = GREEN_TGRAD;
+            s.pos_nyq = 1;  // src/3dTherm/FFT_thermal3D.cpp:113-120
+            s.p1 = (T)(1.0 / k0);
+        } else {
+            s.kind = GREEN_TFLUX;
+            s.xwrap = Ny;   // :151 wraps x with Ny
+            s.p1 = (T)k0;
+        }
+    }
+    return s;
+}
+
+template <typename T, int CC, class Pro, class Spec, class Epi>
+int m3d_solver::launch_sweep(Pro pro, Spec spec, Epi epi, Ctl* ctl, typename Cx<T>::t* sp, int policy,
+                             const Ctl* outer) {
+    typedef typename Cx<T>::t C2;
+    const int Gl = G<T>(), tzy = TZy<T>(), tzx = TZx<T>();
+    const int zblk = (int)((g.NL + Gl - 1) / Gl);
+    const size_t mats_bytes = (size_t)nph * (CC * CC + CC) * sizeof(double) + 64;
+    const size_t zsmem = (size_t)Nz * sizeof(C2) + 2 * (size_t)(Gl / 2) * CC * Nz * sizeof(C2) + 16 + 32 * 32 * 8 + mats_bytes;
+    const size_t ysmem = (size_t)Ny * sizeof(C2) + 2 * (size_t)Ny * tzy * sizeof(C2);
+    const size_t xsmem = (size_t)Nx * sizeof(C2) + 2 * (size_t)CC * Nx * tzx * sizeof(C2) + 16 + 32 * 32 * 8;
+    const int ntzy = (g.Hzp + tzy - 1) / tzy, ntzx = (g.Hzp + tzx - 1) / tzx;
+    static bool init = false;
+    if (!init) {
+        allow_smem(k_zfwd<T, CC, Pro>);
+        allow_smem(k_ypass<T>);
+        allow_smem(k_xturn<T, CC, Spec>);
+        allow_smem(k_zinv<T, CC, Epi>);
+        init = true;
+    }
+    k_zfwd<T, CC, Pro><<<dim3(zblk, B), 256, zsmem, stream>>>(g, pz, tw<T>(2), sp, pro, ctl, Gl, d_part);
+    k_ypass<T><<<dim3(Nx * ntzy, CC * B), 256, ysmem, stream>>>(g, py, tw<T>(1), sp, tzy, CC, -1, ctl);
+    k_xturn<T, CC, Spec><<<dim3(Ny * ntzx, B), 256, xsmem, stream>>>(g, px, tw<T>(0), sp, tzx, spec, ctl, d_part);
+    k_ypass<T><<<dim3(Nx * ntzy, CC * B), 256, ysmem, stream>>>(g, py, tw<T>(1), sp, tzy, CC, +1, ctl);
+    k_zinv<T, CC, Epi><<<dim3(zblk, B), 256, zsmem, stream>>>(g, pz, tw<T>(2), sp, epi, ctl, Gl, d_part);
+    k_finalize<<<B, 256, 0, stream>>>(ctl, d_part, Epi::NSUM, zblk, policy, (double)g.V, outer);
+    st.kernel_launches += 6;
+    M3D_CUDA(cudaGetLastError());
+    return M3D_OK;
+}
+
+// Reference stop rule: forward transform of the stress (heat flux) and the
+// convergenceCheck reductions (src/3d/FFT_analysis3D.cpp:351-416).
+template <typename T, int CC>
+int m3d_solver::launch_check(Ctl* ctl, const void* x, typename Cx<T>::t* sp) {
+    typedef typename Cx<T>::t C2;
+    const int Gl = G<T>(), tzy = TZy<T>(), tzx = TZx<T>();
+    const int zblk = (int)((g.NL + Gl - 1) / Gl);
+    const size_t mats_bytes = (size_t)nph * (CC * CC + CC) * sizeof(double) + 64;
+    const size_t zsmem = (size_t)Nz * sizeof(C2) + 2 * (size_t)(Gl / 2) * CC * Nz * sizeof(C2) + 16 + 32 * 32 * 8 + mats_bytes;
+    const size_t ysmem = (size_t)Ny * sizeof(C2) + 2 * (size_t)Ny * tzy * sizeof(C2);
+    const size_t xsmem = (size_t)Nx * sizeof(C2) + 2 * (size_t)CC * Nx * tzx * sizeof(C2) + 16 + 32 * 32 * 8;
+    const int ntzy = (g.Hzp + tzy - 1) / tzy, ntzx = (g.Hzp + tzx - 1) / tzx;
+    ProMat<T, CC> pro{d_phase, (const T*)x, g.V, dm(off_Q), nph, nullptr};
+    SpecEqVar<T, CC> sv{g};
+    static bool init = false;
+    if (!init) {
+        allow_smem(k_zfwd<T, CC, ProMat<T, CC>>);
+        allow_smem(k_xturn<T, CC, SpecEqVar<T, CC>>);
+        allow_smem(k_ypass<T>);
+        init = true;
+    }
+    k_zfwd<T, CC, ProMat<T, CC>><<<dim3(zblk, B), 256, zsmem, stream>>>(g, pz, tw<T>(2), sp, pro, ctl, Gl, d_part);
+    k_ypass<T><<<dim3(Nx * ntzy, CC * B), 256, ysmem, stream>>>(g, py, tw<T>(1), sp, tzy, CC, -1, ctl);
+    const int xblk = Ny * ntzx;
+    k_xturn<T, CC, SpecEqVar<T, CC>><<<dim3(xblk, B), 256, xsmem, stream>>>(g, px, tw<T>(0), sp, tzx, sv, ctl, d_part);
+    k_finalize<<<B, 256, 0, stream>>>(ctl, d_part, 2, xblk, POL_REF_CHECK, (double)g.V, nullptr);
+    st.kernel_launches += 4;
+    M3D_CUDA(cudaGetLastError());
+    return M3D_OK;
+}
+
+template <typename T, int CC>
+int m3d_solver::launch_em(Ctl* ctl, T* x, const float* r, typename Cx<T>::t* sp, int zero_k0, int policy,
+                          const Ctl* outer) {
+    ProMat<T, CC> pro{d_phase, x, g.V, dm(off_P), nph, nullptr};
+    EpiEM<T, CC> epi{d_phase, x, r, g.V, dm(off_A), dm(off_Os), nph, nullptr};
+    return launch_sweep<T, CC>(pro, green<T, CC>(zero_k0), epi, ctl, sp, policy, outer);
+}
+
+// Fill the state with the uniform load (setLoad, src/3d/FFT_analysis3D.cpp:551-564).
+template <typename T>
+__global__ void k_fill_load(T* x, const Ctl* ctl, int C, long long V) {
+    const int cb = blockIdx.y;
+    const int b = cb / C, c = cb % C;
+    const T e = (T)ctl[b].E[c];
+    for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < V; v += (long long)gridDim.x * blockDim.x)
+        x[(long long)cb * V + v] = e;
+}
+
+template <typename T, int CC>
+int m3d_solver::run_linear(double tol_field, double tol_eq, int criterion, int max_iter) {
+    typedef typename Cx<T>::t C2;
+    int rc = init_ctl(d_ctl, tol_field, tol_eq, max_iter, false);
+    if (rc) return rc;
+    T* x = (T*)d_x;
+    k_fill_load<T><<<dim3(256, B * CC), 256, 0, stream>>>(x, d_ctl, CC, g.V);
+    st.kernel_launches += 1;
+    C2* sp = (C2*)d_spec;
+    const int chunk = 8;
+    for (;;) {
+        for (int k = 0; k < chunk; ++k) {
+            if (criterion == M3D_CRIT_RESIDUAL) {
+                rc = launch_em<T, CC>(d_ctl, x, nullptr, sp, 0, POL_RESIDUAL, nullptr);
+            } else {
+                rc = launch_em<T, CC>(d_ctl, x, nullptr, sp, 0, POL_REF_SWEEP, nullptr);
+                if (!rc) rc = launch_check<T, CC>(d_ctl, x, sp);
+            }
+            if (rc) return rc;
+        }
+        rc = sync_ctl(d_ctl);
+        if (rc) return rc;
+        bool all = true;
+        for (int b = 0; b < B; ++b) all = all && h_ctl[b].done;
+        if (all) break;
+    }
+    long long sw = 0;
+    int status = M3D_OK;
+    for (int b = 0; b < B; ++b) {
+        sw += h_ctl[b].iters;
+        if (h_ctl[b].status == 1 && status == M3D_OK) status = M3D_NOT_CONVERGED;
+        if (h_ctl[b].status == 2) status = M3D_ERR_NAN;
+    }
+    st.sweeps = sw;
+    if (sizeof(T) == 8) st.sweeps_fp64 = sw; else st.sweeps_fp32 = sw;
+    st.iters = h_ctl[0].iters;
+    st.residual = h_ctl[0].residual;
+    st.eqvar = h_ctl[0].eqvar;
+    st.diff_sum = h_ctl[0].diff_sum;
+    st.diff_eq = h_ctl[0].diff_eq;
+    return status;
+}
+
+// FP32 sweeps with FP64 defect correction (iterative refinement of the affine
+// fixed point x = x_c(x)): each outer step evaluates r = x_c(x) - x in FP64,
+// then solves delta = r + L(delta) by FP32 accelerated sweeps (k = 0 mode
+// fixed to 0), and the next FP64 pass folds x += delta into its prologue.
+template <int CC>
+int m3d_solver::run_refine(double tol_field, int max_iter) {
+    int rc = init_ctl(d_ctl, tol_field, 0, max_iter, false);
+    if (rc) return rc;
+    double* x = (double*)d_x;
+    k_fill_load<double><<<dim3(256, B * CC), 256, 0, stream>>>(x, d_ctl, CC, g.V);
+    st.kernel_launches += 1;
+    double2* sp64 = (double2*)d_spec;
+    float2* sp32 = (float2*)d_spec;
+    long long n64 = 0, n32 = 0;
+    bool first = true;
+    const int chunk = 8;
+    for (;;) {
+        ProRefine64<CC> pro{d_phase, x, first ? nullptr : d_delta, g.V, dm(off_P), nph, nullptr};
+        EpiDefect<CC> epi{d_phase, x, d_r32, g.V, dm(off_Os), nph, nullptr};
+        rc = launch_sweep<double, CC>(pro, green<double, CC>(0), epi, d_ctl, sp64, POL_REFINE_OUTER, nullptr);
+        if (rc) return rc;
+        first = false;
+        rc = sync_ctl(d_ctl);
+        if (rc) return rc;
+        bool all = true;
+        for (int b = 0; b < B; ++b) all = all && h_ctl[b].done;
+        if (all) break;
+        // inner FP32 correction solve; entries already converged stay done
+        std::vector<Ctl> outer(h_ctl, h_ctl + B);
+        for (int b = 0; b < B; ++b) {
+            Ctl c;
+            std::memset(&c, 0, sizeof(c));
+            c.done = outer[b].done;
+            c.max_iter = max_iter;
+            c.inner_tol = 2e-4;
+            h_ctl[b] = c;
+        }
+        M3D_CUDA(cudaMemcpyAsync(d_ctl_in, h_ctl, B * sizeof(Ctl), cudaMemcpyHostToDevice, stream));
+        M3D_CUDA(cudaMemsetAsync(d_delta, 0, (size_t)B * CC * g.V * sizeof(float), stream));
+        for (;;) {
+            for (int k = 0; k < chunk; ++k) {
+                rc = launch_em<float, CC>(d_ctl_in, d_delta, d_r32, sp32, 1, POL_REFINE_INNER, d_ctl);
+                if (rc) return rc;
+            }
+            rc = sync_ctl(d_ctl_in);
+            if (rc) return rc;
+            bool alli = true;
+            for (int b = 0; b < B; ++b) alli = alli && h_ctl[b].done;
+            if (alli) break;
+        }
+        for (int b = 0; b < B; ++b) n32 += h_ctl[b].iters;
+    }
+    for (int b = 0; b < B; ++b) n64 += h_ctl[b].iters;
+    int status = M3D_OK;
+    for (int b = 0; b < B; ++b) {
+        if (h_ctl[b].status == 1 && status == M3D_OK) status = M3D_NOT_CONVERGED;
+        if (h_ctl[b].status == 2) status = M3D_ERR_NAN;
+    }
+    st.sweeps = n64 + n32;
+    st.sweeps_fp64 = n64;
+    st.sweeps_fp32 = n32;
+    st.iters = h_ctl[0].iters;
+    st.residual = h_ctl[0].residual;
+    return status;
+}
+
+int m3d_solver::dispatch_run(double tol_field, double tol_eq, int nInc, int criterion, int max_iter) {
+    if (max_iter <= 0) max_iter = (kind == M3D_KIND_MECH) ? 2000 : 500;
+    if (kind == M3D_KIND_MECH && behav != M3D_BEHAV_ELASTIC) {
+        if (prec == M3D_PREC_FP32_REFINE)
+            return fail(M3D_ERR_UNSUPPORTED, "FP32 refinement applies to the linear (elastic/thermal) solves; use FP32 or FP64 for ep/ed");
+        if (prec == M3D_PREC_FP64) return run_inelastic<double, 6>(tol_field, tol_eq, nInc, criterion, max_iter);
+        return run_inelastic<float, 6>(tol_field, tol_eq, nInc, criterion, max_iter);
+    }
+    if (prec == M3D_PREC_FP32_REFINE) {
+        if (criterion != M3D_CRIT_RESIDUAL)
+            return fail(M3D_ERR_UNSUPPORTED, "FP32 refinement stops on the residual criterion only");
+        return C == 6 ? run_refine<6>(tol_field, max_iter) : run_refine<3>(tol_field, max_iter);
+    }
+    if (prec == M3D_PREC_FP64)
+        return C == 6 ? run_linear<double, 6>(tol_field, tol_eq, criterion, max_iter)
+                      : run_linear<double, 3>(tol_field, tol_eq, criterion, max_iter);
+    return C == 6 ? run_linear<float, 6>(tol_field, tol_eq, criterion, max_iter)
+                  : run_linear<float, 3>(tol_field, tol_eq, criterion, max_iter);
+}
+
+// ---- exports ----------------------------------------------------------------
+// out[v*C + c] = (M[ph] x)_c  (M = identity when mats == nullptr)
+template <typename TX, int CC>
+__global__ void k_export(const TX* __restrict__ x, const uint8_t* __restrict__ phase, const double* __restrict__ mats,
+                         int b, long long V, double* __restrict__ out) {
+    for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < V; v += (long long)gridDim.x * blockDim.x) {
+        double xv[CC];
+#pragma unroll
+        for (int c = 0; c < CC; ++c) xv[c] = (double)x[((long long)b * CC + c) * V + v];
+        if (mats) {
+            const double* M = mats + phase[v] * CC * CC;
+#pragma unroll
+            for (int i = 0; i < CC; ++i) {
+                double s = 0;
+#pragma unroll
+                for (int j = 0; j < CC; ++j) s += M[i * CC + j] * xv[j];
+                out[v * CC + i] = s;
+            }
+        } else {
+#pragma unroll
+            for (int c = 0; c < CC; ++c) out[v * CC + c] = xv[c];
+        }
+    }
+}
+
+template <typename TX, int CC>
+static int export_field(m3d_solver* h, const void* x, const double* mats, int b, double* host_out) {
+    const long long V = h->g.V;
+    if (!h->d_out) {
+        cudaError_t e = cudaMalloc(&h->d_out, (size_t)6 * V * sizeof(double));
+        if (e != cudaSuccess) return fail(M3D_ERR_OOM, "export buffer allocation failed");
+    }
+    k_export<TX, CC><<<592, 256, 0, h->stream>>>((const TX*)x, h->d_phase, mats, b, V, h->d_out);
+    h->st.kernel_launches += 1;
+    M3D_CUDA(cudaGetLastError());
+    M3D_CUDA(cudaMemcpyAsync(host_out, h->d_out, (size_t)CC * V * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    M3D_CUDA(cudaStreamSynchronize(h->stream));
+    return M3D_OK;
+}
+
+#include "solver_inelastic.inl"
+
+// ============================================================================
+// C ABI
+// ============================================================================
+extern "C" {
+
+int m3d_abi_version(void) { return M3D_ABI_VERSION; }
+
+const char* m3d_last_error(void) { return g_last_error.c_str(); }
+
+const char* m3d_status_string(int s) {
+    switch (s) {
+        case M3D_OK: return "ok";
+        case M3D_ERR_ARG: return "invalid argument";
+        case M3D_ERR_CUDA: return "CUDA error";
+        case M3D_ERR_OOM: return "device out of memory";
+        case M3D_NOT_CONVERGED: return "not converged (iteration cap)";
+        case M3D_ERR_NAN: return "non-finite residual";
+        case M3D_ERR_STATE: return "call order violated";
+        case M3D_ERR_UNSUPPORTED: return "unsupported";
+        case M3D_ERR_TIMEOUT: return "device wait timed out";
+        default: return "unknown status";
+    }
+}
+
+int m3d_create(int kind, int Nx, int Ny, int Nz, int behav, int precision, int batch, m3d_solver** out) {
+    if (!out) return fail(M3D_ERR_ARG, "out is NULL");
+    *out = nullptr;
+    if (kind != M3D_KIND_MECH && kind != M3D_KIND_THERMAL) return fail(M3D_ERR_ARG, "kind must be MECH or THERMAL");
+    if (Nx < 2 || Ny < 2 || Nz < 2 || Nx > 1024 || Ny > 1024 || Nz > 1024)
+        return fail(M3D_ERR_ARG, "grid sizes must be in [2, 1024]");
+    if (behav < 0 || behav > 2 || (kind == M3D_KIND_THERMAL && behav != 0)) return fail(M3D_ERR_ARG, "invalid behaviour");
+    if (precision < 0 || precision > 2) return fail(M3D_ERR_ARG, "invalid precision");
+    if (batch < 1 || batch > 64) return fail(M3D_ERR_ARG, "batch must be in [1, 64]");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(M3D_ERR_CUDA, "no CUDA device");
+    m3d_solver* h = new m3d_solver();
+    h->kind = kind;
+    h->behav = behav;
+    h->prec = precision;
+    h->C = (kind == M3D_KIND_MECH) ? 6 : 3;
+    h->Nx = Nx; h->Ny = Ny; h->Nz = Nz;
+    h->g.Nx = Nx; h->g.Ny = Ny; h->g.Nz = Nz;
+    h->g.Hz = Nz / 2 + 1;
+    h->g.Hzp = even_up(Nz / 2 + 1);
+    h->g.V = (long long)Nx * Ny * Nz;
+    h->g.NL = (long long)Nx * Ny;
+    if (!make_plan(Nx, h->px) || !make_plan(Ny, h->py) || !make_plan(Nz, h->pz)) {
+        delete h;
+        return fail(M3D_ERR_UNSUPPORTED, "grid sizes need prime factors <= 32");
+    }
+    // launch geometry: z passes hold G lines x C components (ping-pong) in ~48 KB,
+    // y tiles TZ columns of 128 B rows, x tiles all C components in ~64 KB
+    auto pick_G = [&](size_t csz) {
+        int Gv = (int)(48 * 1024 / ((size_t)h->C * Nz * csz));
+        Gv = std::max(2, std::min(16, Gv)) & ~1;
+        return Gv;
+    };
+    h->G64 = pick_G(16);
+    h->G32 = pick_G(8);
+    auto pick_tz = [&](size_t csz, int ncomp, int n, int maxtz) {
+        int tz = maxtz;
+        while (tz > 1 && 2 * (size_t)ncomp * n * tz * csz > 64 * 1024) tz >>= 1;
+        return tz;
+    };
+    h->TZy64 = pick_tz(16, 1, Ny, 8);
+    h->TZy32 = pick_tz(8, 1, Ny, 16);
+    h->TZx64 = pick_tz(16, h->C, Nx, 8);
+    h->TZx32 = pick_tz(8, h->C, Nx, 16);
+    cudaError_t e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) { delete h; return fail(M3D_ERR_CUDA, cudaGetErrorString(e)); }
+    h->own_stream = h->stream;
+    int rc = h->alloc(batch);
+    if (rc) { cudaStreamDestroy(h->stream); delete h; return rc; }
+    // twiddles
+    {
+        std::vector<double2> t64;
+        std::vector<float2> t32;
+        for (int n : {Nx, Ny, Nz}) {
+            auto a = twiddles<double>(n);
+            auto b2 = twiddles<float>(n);
+            t64.insert(t64.end(), a.begin(), a.end());
+            t32.insert(t32.end(), b2.begin(), b2.end());
+        }
+        if (cudaMalloc(&h->d_tw64, t64.size() * sizeof(double2)) != cudaSuccess ||
+            cudaMalloc(&h->d_tw32, t32.size() * sizeof(float2)) != cudaSuccess) {
+            cudaStreamDestroy(h->stream); delete h;
+            return fail(M3D_ERR_OOM, "twiddle allocation failed");
+        }
+        cudaMemcpy(h->d_tw64, t64.data(), t64.size() * sizeof(double2), cudaMemcpyHostToDevice);
+        cudaMemcpy(h->d_tw32, t32.data(), t32.size() * sizeof(float2), cudaMemcpyHostToDevice);
+    }
+    if (cudaMalloc(&h->d_phase, (size_t)h->g.V) != cudaSuccess) {
+        cudaStreamDestroy(h->stream); delete h;
+        return fail(M3D_ERR_OOM, "phase map allocation failed");
+    }
+    *out = h;
+    return M3D_OK;
+}
+
+int m3d_destroy(m3d_solver* h) {
+    if (!h) return M3D_OK;
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    h->free_all();
+    if (h->own_stream) cudaStreamDestroy(h->own_stream);
+    delete h;
+    return M3D_OK;
+}
+
+static int upload_tables(m3d_solver* h) {
+    const int C = h->C, n = h->nph;
+    std::vector<double> all;
+    h->off_P = 0;
+    all.insert(all.end(), h->hP.begin(), h->hP.end());
+    h->off_A = all.size();
+    all.insert(all.end(), h->hA.begin(), h->hA.end());
+    h->off_O = all.size();
+    all.insert(all.end(), h->hO.begin(), h->hO.end());
+    h->off_Os = all.size();
+    all.insert(all.end(), h->hOsum.begin(), h->hOsum.end());
+    h->off_Q = all.size();
+    all.insert(all.end(), h->hQ.begin(), h->hQ.end());
+    (void)C; (void)n;
+    cudaFree(h->d_mats);
+    h->d_mats = nullptr;
+    M3D_CUDA(cudaMalloc(&h->d_mats, all.size() * sizeof(double)));
+    M3D_CUDA(cudaMemcpy(h->d_mats, all.data(), all.size() * sizeof(double), cudaMemcpyHostToDevice));
+    return M3D_OK;
+}
+
+static void push_mat(std::vector<double>& dst, const Mat& m) { dst.insert(dst.end(), m.begin(), m.end()); }
+
+int m3d_set_material_mech(m3d_solver* h, const double* mat, int nph, const int32_t* phase, int scheme) {
+    if (!h || !mat || !phase) return fail(M3D_ERR_ARG, "NULL argument");
+    if (h->kind != M3D_KIND_MECH) return fail(M3D_ERR_ARG, "not a mechanical solver");
+    if (nph < 1 || nph > kMaxPhases) return fail(M3D_ERR_ARG, "nph must be in [1, 16]");
+    if (scheme < 0 || scheme > 2) return fail(M3D_ERR_ARG, "invalid scheme");
+    const long long V = h->g.V;
+    std::vector<uint8_t> ph8(V);
+    h->counts.assign(nph, 0);
+    for (long long v = 0; v < V; ++v) {
+        const int id = phase[v];
+        if (id < 0 || id >= nph) return fail(M3D_ERR_ARG, "phase id out of range at voxel " + std::to_string(v));
+        ph8[v] = (uint8_t)id;
+        h->counts[id]++;
+    }
+    h->nph = nph;
+    h->mat.assign(mat, mat + nph * 7);
+    // material(), src/3d/FFT_analysis3D.cpp:441-546
+    std::vector<double> mu(nph), la(nph), K(nph);
+    h->vol.assign(nph, 0.0);
+    for (int i = 0; i < nph; ++i) {
+        const double El = mat[i * 7 + 0], v = mat[i * 7 + 1];
+        if (!(El > 0) || !(v > -1.0 && v < 0.5)) return fail(M3D_ERR_ARG, "phase " + std::to_string(i) + ": need E > 0 and -1 < nu < 0.5");
+        mu[i] = El / (1 + v) / 2.;
+        la[i] = v * El / (1 + v) / (1 - 2 * v);
+        K[i] = la[i] + (2. / 3.) * mu[i];
+        h->Cp[i] = iso_stiffness(la[i], mu[i]);
+        h->Sp[i] = mat_inv(h->Cp[i], 6);
+        h->vol[i] = (double)h->counts[i] / (double)V;
+    }
+    int imu = 0;
+    for (int i = 1; i < nph; ++i) if (mu[i] > mu[imu]) imu = i;  // first strict maximum (:5-23)
+    const double mu_max = *std::max_element(mu.begin(), mu.end()), mu_min = *std::min_element(mu.begin(), mu.end());
+    const double la_max = *std::max_element(la.begin(), la.end()), la_min = *std::min_element(la.begin(), la.end());
+    const double K_max = *std::max_element(K.begin(), K.end()), K_min = *std::min_element(K.begin(), K.end());
+    const double vol_max = *std::max_element(h->vol.begin(), h->vol.end());
+    if (h->behav == M3D_BEHAV_ELASTIC) {
+        const double K0 = std::sqrt(K_min * K_max);
+        h->mu0 = std::sqrt(mu_min * mu_max);
+        h->la0 = K0 - h->mu0 * 2. / 3.;
+        h->scheme = (h->vol[imu] == vol_max) ? 1 : 2;  // (:503-512)
+    } else {
+        h->scheme = 1;  // (:515-522)
+        h->mu0 = (mu_min + mu_max) / 2;
+        h->la0 = (la_min + la_max) / 2;
+    }
+    if (scheme != M3D_SCHEME_AUTO) {
+        if (h->behav != M3D_BEHAV_ELASTIC && scheme == M3D_SCHEME_DUAL)
+            return fail(M3D_ERR_ARG, "the ep/ed path is strain-based only");
+        h->scheme = scheme;
+    }
+    h->C0 = iso_stiffness(h->la0, h->mu0);
+    h->S0 = mat_inv(h->C0, 6);
+    h->hP.clear(); h->hA.clear(); h->hO.clear(); h->hOsum.clear(); h->hQ.clear();
+    for (int i = 0; i < nph; ++i) {
+        if (h->scheme == 1) {
+            push_mat(h->hP, mat_add(h->Cp[i], h->C0, -1.0));
+            push_mat(h->hA, mat_mul(mat_scale(mat_inv(mat_add(h->Cp[i], h->C0), 6), 2.0), h->C0, 6));
+            push_mat(h->hO, h->Cp[i]);
+            push_mat(h->hQ, h->Cp[i]);
+        } else {
+            push_mat(h->hP, mat_add(h->Sp[i], h->S0, -1.0));
+            push_mat(h->hA, mat_mul(mat_scale(mat_inv(mat_add(h->Sp[i], h->S0), 6), 2.0), h->S0, 6));
+            push_mat(h->hO, h->Sp[i]);
+            push_mat(h->hQ, diag(6, 1.0));
+        }
+        const Mat& O = (h->scheme == 1) ? h->Cp[i] : h->Sp[i];
+        for (int c = 0; c < 6; ++c) {
+            double s = 0;
+            for (int r = 0; r < 6; ++r) s += O[r * 6 + c];
+            h->hOsum.push_back(s);
+        }
+    }
+    const int p1 = nph > 1 ? 1 : 0;  // the reference reads phases 0 and 1 (:399, :408)
+    h->den_ref = (h->scheme == 1) ? 0.5 * h->Cp[0][0] + 0.5 * h->Cp[p1][0] : 0.5 * h->Sp[0][0] + 0.5 * h->Sp[p1][0];
+    int rc = upload_tables(h);
+    if (rc) return rc;
+    M3D_CUDA(cudaMemcpy(h->d_phase, ph8.data(), (size_t)V, cudaMemcpyHostToDevice));
+    h->material_set = true;
+    h->st.scheme = h->scheme;
+    h->st.la0 = h->la0;
+    h->st.mu0 = h->mu0;
+    for (int i = 0; i < 16; ++i) h->st.vol_fraction[i] = i < nph ? h->vol[i] : 0.0;
+    if (h->behav != M3D_BEHAV_ELASTIC) {
+        rc = h->in.setup(h);
+        if (rc) return rc;
+    }
+    return M3D_OK;
+}
+
+int m3d_set_material_thermal(m3d_solver* h, double km, double ki, const int32_t* phase, int scheme) {
+    if (!h || !phase) return fail(M3D_ERR_ARG, "NULL argument");
+    if (h->kind != M3D_KIND_THERMAL) return fail(M3D_ERR_ARG, "not a thermal solver");
+    if (!(km > 0) || !(ki > 0)) return fail(M3D_ERR_ARG, "conductivities must be positive");
+    if (scheme < 0 || scheme > 2) return fail(M3D_ERR_ARG, "invalid scheme");
+    const long long V = h->g.V;
+    std::vector<uint8_t> ph8(V);
+    h->counts.assign(2, 0);
+    long long idsum = 0;
+    for (long long v = 0; v < V; ++v) {
+        const int id = phase[v];
+        idsum += id;
+        // multipKx()/strainUpdate() test `if (RVE(i))` (src/3dTherm/FFT_thermal3D.cpp:186,249)
+        ph8[v] = id != 0 ? 1 : 0;
+        h->counts[ph8[v]]++;
+    }
+    h->nph = 2;
+    h->km = km;
+    h->ki = ki;
+    // vol_1 = RVE.sum()/xyz is an integer division in the reference (:399)
+    const long long vol_1 = idsum / V;
+    h->scheme = ((vol_1 >= 1 && km > ki) || (vol_1 < 1 && km < ki)) ? 1 : 2;  // (:401-410)
+    if (scheme != M3D_SCHEME_AUTO) h->scheme = scheme;
+    h->k0 = std::sqrt(ki * km);  // (:415)
+    const double kk[2] = {ki, km};
+    h->hP.clear(); h->hA.clear(); h->hO.clear(); h->hOsum.clear(); h->hQ.clear();
+    h->vol.assign(2, 0.0);
+    for (int p = 0; p < 2; ++p) {
+        const double k = kk[p], k0 = h->k0;
+        h->vol[p] = (double)h->counts[p] / (double)V;
+        if (h->scheme == 1) {
+            push_mat(h->hP, diag(3, k - k0));
+            push_mat(h->hA, diag(3, 2 * k0 / (k + k0)));
+            push_mat(h->hO, diag(3, k));
+            push_mat(h->hQ, diag(3, k));
+            for (int c = 0; c < 3; ++c) h->hOsum.push_back(k);
+        } else {
+            const double r = 1.0 / k, r0 = 1.0 / k0;
+            push_mat(h->hP, diag(3, r - r0));
+            push_mat(h->hA, diag(3, 2 * r0 / (r + r0)));
+            push_mat(h->hO, diag(3, r));
+            push_mat(h->hQ, diag(3, 1.0));
+            for (int c = 0; c < 3; ++c) h->hOsum.push_back(r);
+        }
+    }
+    h->den_ref = (h->scheme == 1) ? 0.5 * ki + 0.5 * km : 0.5 / ki + 0.5 / km;  // (:346, :356)
+    int rc = upload_tables(h);
+    if (rc) return rc;
+    M3D_CUDA(cudaMemcpy(h->d_phase, ph8.data(), (size_t)V, cudaMemcpyHostToDevice));
+    h->material_set = true;
+    h->st.scheme = h->scheme;
+    h->st.k0 = h->k0;
+    h->st.vol_fraction[0] = h->vol[0];
+    h->st.vol_fraction[1] = h->vol[1];
+    return M3D_OK;
+}
+
+int m3d_set_load(m3d_solver* h, int b, const double* E, const double* X0) {
+    if (!h || !E) return fail(M3D_ERR_ARG, "NULL argument");
+    if (b < -1 || b >= h->B) return fail(M3D_ERR_ARG, "batch index out of range");
+    for (int i = 0; i < h->C; ++i)
+        if (!std::isfinite(E[i])) return fail(M3D_ERR_ARG, "non-finite load");
+    const int lo = b < 0 ? 0 : b, hi = b < 0 ? h->B : b + 1;
+    for (int k = lo; k < hi; ++k) {
+        for (int i = 0; i < h->C; ++i) h->E[k * h->C + i] = E[i];
+        for (int i = 0; i < 6; ++i) h->X0[k * 6 + i] = X0 ? X0[i] : 0.0;
+    }
+    h->load_set = true;
+    return M3D_OK;
+}
+
+int m3d_run(m3d_solver* h, double tol_field, double tol_eq, int nInc, int criterion, int max_iter) {
+    if (!h) return fail(M3D_ERR_ARG, "NULL handle");
+    if (!h->material_set) return fail(M3D_ERR_STATE, "material not set");
+    if (!h->load_set) return fail(M3D_ERR_STATE, "load not set");
+    if (criterion != M3D_CRIT_REFERENCE && criterion != M3D_CRIT_RESIDUAL) return fail(M3D_ERR_ARG, "invalid criterion");
+    if (!(tol_field > 0) || !(tol_eq >= 0)) return fail(M3D_ERR_ARG, "tolerances must be positive");
+    if (h->behav != M3D_BEHAV_ELASTIC && nInc < 1) return fail(M3D_ERR_ARG, "nInc must be >= 1");
+    const auto t0 = std::chrono::steady_clock::now();
+    const int rc = h->dispatch_run(tol_field, tol_eq, nInc, criterion, max_iter);
+    cudaStreamSynchronize(h->stream);
+    h->st.solve_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    h->st.status = rc;
+    h->run_done = (rc == M3D_OK || rc == M3D_NOT_CONVERGED);
+    return rc;
+}
+
+}  // extern "C"
+
+// means of the strain-like and stress-like fields of entry b
+template <typename TX, int CC>
+__global__ void k_means(const TX* __restrict__ x, const uint8_t* __restrict__ phase, const double* __restrict__ mats,
+                        int b, long long V, double* __restrict__ part) {
+    double acc[2 * CC] = {};
+    for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < V; v += (long long)gridDim.x * blockDim.x) {
+        double xv[CC];
+#pragma unroll
+        for (int c = 0; c < CC; ++c) xv[c] = (double)x[((long long)b * CC + c) * V + v];
+        const double* M = mats + phase[v] * CC * CC;
+#pragma unroll
+        for (int i = 0; i < CC; ++i) {
+            acc[i] += xv[i];
+            double s = 0;
+#pragma unroll
+            for (int j = 0; j < CC; ++j) s += M[i * CC + j] * xv[j];
+            acc[CC + i] += s;
+        }
+    }
+    __shared__ double red[32 * 2 * CC];
+    block_reduce_store<2 * CC>(acc, red, part, 0, gridDim.x, blockIdx.x);
+}
+
+extern "C" {
+
+int m3d_get_means(m3d_solver* h, int b, double* strain_mean, double* stress_mean) {
+    if (!h) return fail(M3D_ERR_ARG, "NULL handle");
+    if (!h->run_done) return fail(M3D_ERR_STATE, "no finished run");
+    if (b < 0 || b >= h->B) return fail(M3D_ERR_ARG, "batch index out of range");
+    const int C = h->C;
+    if (h->kind == M3D_KIND_MECH && h->behav != M3D_BEHAV_ELASTIC)
+        return h->in.means(h, b, strain_mean, stress_mean);
+    const int nblk = 296;
+    double* part = h->d_part;
+    if (h->part_cap < (size_t)nblk * 2 * C) return fail(M3D_ERR_STATE, "partials buffer too small");
+    const double* O = h->d_mats + h->off_O;
+    if (C == 6) {
+        if (h->prec == M3D_PREC_FP32) k_means<float, 6><<<nblk, 256, 0, h->stream>>>((const float*)h->d_x, h->d_phase, O, b, h->g.V, part);
+        else k_means<double, 6><<<nblk, 256, 0, h->stream>>>((const double*)h->d_x, h->d_phase, O, b, h->g.V, part);
+    } else {
+        if (h->prec == M3D_PREC_FP32) k_means<float, 3><<<nblk, 256, 0, h->stream>>>((const float*)h->d_x, h->d_phase, O, b, h->g.V, part);
+        else k_means<double, 3><<<nblk, 256, 0, h->stream>>>((const double*)h->d_x, h->d_phase, O, b, h->g.V, part);
+    }
+    h->st.kernel_launches += 1;
+    M3D_CUDA(cudaGetLastError());
+    std::vector<double> hp((size_t)nblk * 2 * C);
+    M3D_CUDA(cudaMemcpyAsync(hp.data(), part, hp.size() * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    M3D_CUDA(cudaStreamSynchronize(h->stream));
+    double s[12] = {};
+    for (int k = 0; k < 2 * C; ++k)
+        for (int i = 0; i < nblk; ++i) s[k] += hp[(size_t)k * nblk + i];
+    const double V = (double)h->g.V;
+    // state = strain-like in the primal scheme, stress-like in the dual scheme
+    double* prim = (h->scheme == 1) ? strain_mean : stress_mean;
+    double* dual = (h->scheme == 1) ? stress_mean : strain_mean;
+    for (int c = 0; c < C; ++c) {
+        if (prim) prim[c] = s[c] / V;
+        if (dual) dual[c] = s[C + c] / V;
+    }
+    return M3D_OK;
+}
+
+int m3d_homogenize(m3d_solver* h, double tol_field, double tol_eq, int criterion, int max_iter, double* Ceff,
+                   double* Seff, double* ep_means, double* sig_means) {
+    if (!h) return fail(M3D_ERR_ARG, "NULL handle");
+    if (!h->material_set) return fail(M3D_ERR_STATE, "material not set");
+    if (h->kind == M3D_KIND_MECH && h->behav != M3D_BEHAV_ELASTIC)
+        return fail(M3D_ERR_ARG, "homogenization runs the elastic solver; create the solver with behaviour ELASTIC");
+    const int C = h->C;
+    if (h->B != C) {
+        int rc = h->alloc(C);
+        if (rc) return rc;
+    }
+    // load cases (src/3d/FFT_analysis3D.cpp:866-877; src/3dTherm/FFT_thermal3D.cpp:501-507, 544-549)
+    for (int w = 0; w < C; ++w) {
+        double E[6] = {0, 0, 0, 0, 0, 0};
+        if (h->kind == M3D_KIND_MECH) E[w] = (h->scheme == 1) ? 0.0005 : 1.e6;
+        else E[w] = 1.0;
+        int rc = m3d_set_load(h, w, E, h->kind == M3D_KIND_MECH ? E : nullptr);
+        if (rc) return rc;
+    }
+    const auto t0 = std::chrono::steady_clock::now();
+    int rc = h->dispatch_run(tol_field, tol_eq, 1, criterion, max_iter);
+    if (rc != M3D_OK && rc != M3D_NOT_CONVERGED) return rc;
+    const int status = rc;
+    h->run_done = true;
+    // strain-like means g[w][c], stress-like q[w][c] per load case w
+    std::vector<double> gm(C * C), qm(C * C);
+    for (int w = 0; w < C; ++w) {
+        rc = m3d_get_means(h, w, &gm[w * C], &qm[w * C]);
+        if (rc) return rc;
+    }
+    // Assembly exactly as the reference: one matrix stores the means with one
+    // ROW per load case, the other with one COLUMN per load case, and the
+    // result is X = first^-1 * second.
+    //  mech strain-based  (src/3d/FFT_analysis3D.cpp:880-895): epHomo(t,w) = <eps_t>_w (columns),
+    //      sigHomo(w,t) = <sig_t>_w (rows), CHomo = epHomo^-1 sigHomo
+    //  mech stress-based  (:897-901): SHomo = sigHomo^-1 epHomo
+    //  thermal gradient   (src/3dTherm/FFT_thermal3D.cpp:525-536): tempGradHomo(w,j) (rows),
+    //      heatFluxHomo(j,w) (columns), KHomo = tempGradHomo^-1 heatFluxHomo
+    //  thermal flux       (:567-578): heatFluxHomo(w,j) (rows), tempGradHomo(j,w) (columns),
+    //      RHomo = heatFluxHomo^-1 tempGradHomo
+    const bool primal = (h->scheme == 1);
+    Mat rows_g(C * C), cols_g(C * C), rows_q(C * C), cols_q(C * C);
+    for (int w = 0; w < C; ++w)
+        for (int t = 0; t < C; ++t) {
+            rows_g[w * C + t] = gm[w * C + t];
+            cols_g[t * C + w] = gm[w * C + t];
+            rows_q[w * C + t] = qm[w * C + t];
+            cols_q[t * C + w] = qm[w * C + t];
+        }
+    Mat first, second, strain_store, stress_store;
+    if (h->kind == M3D_KIND_MECH) {
+        strain_store = cols_g;  // epHomo
+        stress_store = rows_q;  // sigHomo
+        if (primal) { first = cols_g; second = rows_q; } else { first = rows_q; second = cols_g; }
+    } else {
+        if (primal) { first = rows_g; second = cols_q; strain_store = rows_g; stress_store = cols_q; }
+        else { first = rows_q; second = cols_g; strain_store = cols_g; stress_store = rows_q; }
+    }
+    const Mat X = mat_mul(mat_inv(first, C), second, C);
+    const Mat Xi = mat_inv(X, C);
+    // primal: X is the stiffness (conductivity); dual: X is the compliance (resistivity)
+    const Mat& Cm = primal ? X : Xi;
+    const Mat& Sm = primal ? Xi : X;
+    if (Ceff) std::memcpy(Ceff, Cm.data(), C * C * sizeof(double));
+    if (Seff) std::memcpy(Seff, Sm.data(), C * C * sizeof(double));
+    if (ep_means) std::memcpy(ep_means, strain_store.data(), C * C * sizeof(double));
+    if (sig_means) std::memcpy(sig_means, stress_store.data(), C * C * sizeof(double));
+    h->st.solve_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    h->st.status = status;
+    return status;
+}
+
+int m3d_get_field(m3d_solver* h, int which, int b, double* out) {
+    if (!h || !out) return fail(M3D_ERR_ARG, "NULL argument");
+    if (!h->run_done) return fail(M3D_ERR_STATE, "no finished run");
+    if (b < 0 || b >= h->B) return fail(M3D_ERR_ARG, "batch index out of range");
+    if (h->kind == M3D_KIND_MECH && h->behav != M3D_BEHAV_ELASTIC) return h->in.get_field(h, which, b, out);
+    if (which != M3D_FIELD_STRAIN && which != M3D_FIELD_STRESS)
+        return fail(M3D_ERR_ARG, "field not available for this behaviour");
+    const bool state = (which == M3D_FIELD_STRAIN) == (h->scheme == 1);
+    const double* M = state ? nullptr : h->d_mats + h->off_O;
+    if (h->C == 6)
+        return h->prec == M3D_PREC_FP32 ? export_field<float, 6>(h, h->d_x, M, b, out) : export_field<double, 6>(h, h->d_x, M, b, out);
+    return h->prec == M3D_PREC_FP32 ? export_field<float, 3>(h, h->d_x, M, b, out) : export_field<double, 3>(h, h->d_x, M, b, out);
+}
+
+void* m3d_get_stream(const m3d_solver* h) { return h ? (void*)h->stream : nullptr; }
+
+int m3d_set_stream(m3d_solver* h, void* s) {
+    if (!h) return fail(M3D_ERR_ARG, "NULL handle");
+    M3D_CUDA(cudaStreamSynchronize(h->stream));
+    h->stream = s ? (cudaStream_t)s : h->own_stream;
+    return M3D_OK;
+}
+
+int m3d_get_stats(const m3d_solver* h, m3d_stats* out) {
+    if (!h || !out) return fail(M3D_ERR_ARG, "NULL argument");
+    *out = h->st;
+    return M3D_OK;
+}
+
+int m3d_get_increments(const m3d_solver* h, double* out, int max_rows) {
+    if (!h || !out) return fail(M3D_ERR_ARG, "NULL argument");
+    const int rows = std::min<int>(max_rows, (int)(h->prop.size() / 9));
+    std::memcpy(out, h->prop.data(), (size_t)rows * 9 * sizeof(double));
+    return rows;
+}
+
+}  // extern "C"

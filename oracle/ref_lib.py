@@ -1,0 +1,100 @@
+"""ctypes wrapper of oracle/_ref/libmat3d_ref.so (the reference's own solver
+sources built by oracle/Makefile).  TEST INFRASTRUCTURE ONLY: used by the
+fixture generator, the CPU tests and the CPU-baseline legs of bench.py.
+
+Fields come back in the reference's AoS layout (voxel-major, c values per
+voxel), reshaped here to (c, V) like the reference's Eigen c x N^3 matrices.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF_SO = os.path.join(HERE, "_ref", "libmat3d_ref.so")
+
+
+def available() -> bool:
+    return os.path.exists(REF_SO)
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(ctypes.c_void_p)
+
+
+class RefLib:
+    def __init__(self, path: str = REF_SO, fft_threads: int = 3):
+        if not os.path.exists(path):
+            raise FileNotFoundError(f"{path} missing: run `make -C oracle` where the reference sources exist")
+        self.L = ctypes.CDLL(path)
+        self.threads = fft_threads
+
+    def fft_r2c(self, x):
+        Nx, Ny, Nz, c = x.shape
+        xin = np.ascontiguousarray(x, np.float64)
+        out = np.zeros((Nx, Ny, Nz // 2 + 1, c), np.complex128)
+        self.L.ref_fft_r2c(Nx, Ny, Nz, c, _p(xin), _p(out))
+        return out
+
+    def fft_c2r(self, spec, shape):
+        Nx, Ny, Nz = shape
+        c = spec.shape[-1]
+        sin = np.ascontiguousarray(spec, np.complex128)
+        out = np.zeros((Nx, Ny, Nz, c))
+        self.L.ref_fft_c2r(Nx, Ny, Nz, c, _p(sin), _p(out))
+        return out
+
+    def mech_run(self, shape, behav, mat, rve, E, X0, tol_field, tol_eq, nInc=1, force_scheme=0):
+        Nx, Ny, Nz = shape
+        V = Nx * Ny * Nz
+        mat = np.ascontiguousarray(mat, np.float64)
+        rve = np.ascontiguousarray(np.asarray(rve).ravel(), np.int32)
+        E = np.ascontiguousarray(E, np.float64)
+        X0 = np.ascontiguousarray(X0, np.float64)
+        eps, sig, ex = np.zeros(6 * V), np.zeros(6 * V), np.zeros(V)
+        prop = np.zeros(max(nInc, 1) * 9)
+        sw, sch, ni, lm = ctypes.c_longlong(), ctypes.c_int(), ctypes.c_int(), np.zeros(2)
+        D = ctypes.c_double
+        self.L.ref_mech_run(Nx, Ny, Nz, behav.encode(), _p(mat), mat.shape[0], _p(rve), _p(E), _p(X0), D(tol_field),
+                            D(tol_eq), nInc, force_scheme, self.threads, _p(eps), _p(sig), _p(ex), _p(prop),
+                            ctypes.byref(sw), ctypes.byref(sch), ctypes.byref(ni), _p(lm))
+        return dict(eps=eps.reshape(V, 6).T.copy(), sig=sig.reshape(V, 6).T.copy(), extra=ex,
+                    prop=prop.reshape(-1, 9)[: ni.value], sweeps=sw.value, scheme=sch.value, ninc=ni.value,
+                    la0=lm[0], mu0=lm[1])
+
+    def mech_homog(self, shape, mat, rve, tol_field, tol_eq, force_scheme=0):
+        Nx, Ny, Nz = shape
+        mat = np.ascontiguousarray(mat, np.float64)
+        rve = np.ascontiguousarray(np.asarray(rve).ravel(), np.int32)
+        C, S, ep, sg, E3 = np.zeros(36), np.zeros(36), np.zeros(36), np.zeros(36), np.zeros(3)
+        sw, sch = ctypes.c_longlong(), ctypes.c_int()
+        D = ctypes.c_double
+        self.L.ref_mech_homog(Nx, Ny, Nz, _p(mat), mat.shape[0], _p(rve), D(tol_field), D(tol_eq), force_scheme,
+                              self.threads, None, _p(C), _p(S), _p(ep), _p(sg), ctypes.byref(sw), ctypes.byref(sch),
+                              _p(E3))
+        return dict(C=C.reshape(6, 6), S=S.reshape(6, 6), epHomo=ep.reshape(6, 6), sigHomo=sg.reshape(6, 6),
+                    sweeps=sw.value, scheme=sch.value, E123=E3)
+
+    def therm_run(self, shape, km, ki, rve, E, tol_field, tol_eq):
+        Nx, Ny, Nz = shape
+        V = Nx * Ny * Nz
+        rve = np.ascontiguousarray(np.asarray(rve).ravel(), np.int32)
+        E = np.ascontiguousarray(E, np.float64)
+        g, q = np.zeros(3 * V), np.zeros(3 * V)
+        sw, sch = ctypes.c_longlong(), ctypes.c_int()
+        D = ctypes.c_double
+        self.L.ref_therm_run(Nx, Ny, Nz, D(km), D(ki), _p(rve), _p(E), D(tol_field), D(tol_eq), self.threads, _p(g),
+                             _p(q), ctypes.byref(sw), ctypes.byref(sch))
+        return dict(grad=g.reshape(V, 3).T.copy(), flux=q.reshape(V, 3).T.copy(), sweeps=sw.value, scheme=sch.value)
+
+    def therm_homog(self, shape, km, ki, rve, tol_field, tol_eq):
+        Nx, Ny, Nz = shape
+        rve = np.ascontiguousarray(np.asarray(rve).ravel(), np.int32)
+        K, R = np.zeros(9), np.zeros(9)
+        sw, sch = ctypes.c_longlong(), ctypes.c_int()
+        D = ctypes.c_double
+        self.L.ref_therm_homog(Nx, Ny, Nz, D(km), D(ki), _p(rve), D(tol_field), D(tol_eq), self.threads, None, _p(K),
+                               _p(R), ctypes.byref(sw), ctypes.byref(sch))
+        return dict(K=K.reshape(3, 3), R=R.reshape(3, 3), sweeps=sw.value, scheme=sch.value)

@@ -1,0 +1,86 @@
+"""Generate the golden fixtures in tests/golden/ from the reference's own solver.
+
+Runs oracle/_ref/libmat3d_ref.so -- the reference sources
+src/3d/FFT_analysis3D.cpp and src/3dTherm/FFT_thermal3D.cpp compiled
+unmodified by oracle/Makefile against stand-in FFTW/Eigen/VTK headers -- on
+small seeded inputs and stores inputs and outputs as compressed .npz files.
+The reference project ships no tests or expected outputs of its own, so these
+fixtures are the parity pin for the numpy oracle (tests/test_oracle_golden.py)
+and, through it, for the CUDA solver.
+
+    make -C oracle && python tests/golden/make_golden.py
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+from oracle.ref_lib import RefLib  # noqa: E402
+
+
+def sphere(shape, r, center=None):
+    Nx, Ny, Nz = shape
+    X, Y, Z = np.meshgrid(np.arange(Nx), np.arange(Ny), np.arange(Nz), indexing="ij")
+    c = center or (Nx / 2, Ny / 2, Nz / 2)
+    rve = np.ones(shape, np.int32)
+    rve[(X - c[0]) ** 2 + (Y - c[1]) ** 2 + (Z - c[2]) ** 2 <= r * r] = 0
+    return rve.ravel()
+
+
+MAT_A = np.array([[70e9, 0.2, 40e6, 100e6, 1, 8e-2, 8e2], [3e9, 0.35, 250e6, 8006, 0.2, 8e-4, 8e3]])
+MAT_J2 = np.array([[400e9, 0.2, 1e30, 0, 1, 0, 1e30], [70e9, 0.33, 100e6, 1e9, 1, 0, 1e30]])
+
+
+def main():
+    ref = RefLib()
+    out = {}
+    rng = np.random.default_rng(1234)
+    # FFT layout pins (guru64 r2c / c2r of the 3-D solver's plans)
+    for (shape, c) in (((6, 8, 10), 6), ((5, 6, 7), 3)):
+        x = rng.standard_normal(shape + (c,))
+        spec = ref.fft_r2c(x)
+        back = ref.fft_c2r(spec, shape)
+        np.savez_compressed(os.path.join(HERE, f"fft_{shape[0]}x{shape[1]}x{shape[2]}_c{c}.npz"),
+                            x=x, spec=spec, back=back)
+    # elastic runs: stress-based (auto) and strain-based (forced), non-cubic
+    for name, shape, force, E in (("elastic_auto_12", (12, 12, 12), 0, [1e-3, 0, 0, 0, 2e-4, 0]),
+                                  ("elastic_strain_10x12x14", (10, 12, 14), 1, [0, 1e-3, 0, 3e-4, 0, 0])):
+        rve = sphere(shape, 3.1)
+        r = ref.mech_run(shape, "e", MAT_A, rve, np.array(E, float), np.array([0, 1, 0, 0, 0, 0.0]),
+                         1e-10, 1e-10, 1, force)
+        np.savez_compressed(os.path.join(HERE, f"{name}.npz"), shape=shape, rve=rve, mat=MAT_A, E=E,
+                            force=force, tol=1e-10, **r)
+    # elastic homogenization
+    shape = (10, 10, 10)
+    rve = sphere(shape, 2.6)
+    r = ref.mech_homog(shape, MAT_A, rve, 1e-10, 1e-10)
+    np.savez_compressed(os.path.join(HERE, "homog_elastic_10.npz"), shape=shape, rve=rve, mat=MAT_A, tol=1e-10, **r)
+    # J2 and damage, 3 increments under uniaxial stress direction X0 = e_1
+    for name, behav, mat in (("j2_10", "ep", MAT_J2), ("damage_10", "ed", MAT_A)):
+        shape = (10, 10, 10)
+        rve = sphere(shape, 2.8, center=(5, 5, 5))
+        E = np.array([0.02, 0, 0, 0, 0, 0.0])
+        X0 = np.array([1.0, 0, 0, 0, 0, 0])
+        r = ref.mech_run(shape, behav, mat, rve, E, X0, 1e-8, 1e-8, 3, 0)
+        np.savez_compressed(os.path.join(HERE, f"{name}.npz"), shape=shape, rve=rve, mat=mat, E=E, X0=X0,
+                            tol=1e-8, ninc_req=3, **r)
+    # thermal: gradient-based (km < ki) and flux-based (km > ki), run + homogenization
+    for name, km, ki in (("thermal_grad_12", 1.0, 100.0), ("thermal_flux_12", 30.0, 25.0)):
+        shape = (12, 12, 12)
+        rve = sphere(shape, 3.3)
+        E = np.array([0.0, 0.3, 1.0])
+        r = ref.therm_run(shape, km, ki, rve, E, 1e-10, 1e-10)
+        h = ref.therm_homog(shape, km, ki, rve, 1e-10, 1e-10)
+        np.savez_compressed(os.path.join(HERE, f"{name}.npz"), shape=shape, rve=rve, km=km, ki=ki, E=E, tol=1e-10,
+                            **r, K=h["K"], R=h["R"], homog_sweeps=h["sweeps"])
+    print("fixtures written to", HERE)
+
+
+if __name__ == "__main__":
+    main()

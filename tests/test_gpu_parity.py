@@ -1,0 +1,200 @@
+"""GPU parity: the CUDA solver through the C ABI against the CPU oracle.
+
+The oracle (oracle/mat3d_oracle.py) restates the reference solver in numpy
+and is itself pinned to the reference's own sources (tests/test_oracle_ref.py,
+tests/test_oracle_golden.py).  Tolerances:
+  * FP64 with the reference stop rule: same sweep count, fields rel-L2 < 1e-9;
+  * FP64 effective tensors: max |dC| / |C| < 1e-9;
+  * FP32 sweeps: rel-L2 < 2e-4 against the FP64 oracle solution;
+  * FP32 sweeps + FP64 refinement to 1e-9: rel-L2 < 1e-6 and C_eff < 1e-5
+    (the 1e-5 parity gate).
+"""
+import numpy as np
+import pytest
+
+import mat3d_b200 as m3d
+from oracle import mat3d_oracle as O
+
+pytestmark = pytest.mark.gpu
+
+MAT_SOFT_MATRIX = np.array([[70e9, 0.2, 40e6, 100e6, 1, 8e-2, 8e2],     # stiff inclusions (phase 0)
+                            [3e9, 0.35, 250e6, 8006, 0.2, 8e-4, 8e3]])  # soft matrix (phase 1)
+MAT_STIFF_MATRIX = np.array([[3e9, 0.35, 1e30, 0, 1, 0, 1e30],
+                             [70e9, 0.2, 1e30, 0, 1, 0, 1e30]])
+
+
+def sphere_rve(shape, r, center=None):
+    Nx, Ny, Nz = shape
+    X, Y, Z = np.meshgrid(np.arange(Nx), np.arange(Ny), np.arange(Nz), indexing="ij")
+    c = center or (Nx / 2, Ny / 2, Nz / 2)
+    rve = np.ones(shape, np.int32)
+    rve[(X - c[0]) ** 2 + (Y - c[1]) ** 2 + (Z - c[2]) ** 2 <= r * r] = 0
+    return rve.ravel()
+
+
+def rel(a, b):
+    return np.linalg.norm(np.asarray(a) - np.asarray(b)) / max(np.linalg.norm(b), 1e-300)
+
+
+def mech_pair(shape, mat, rve, E, X0=None, behav="e", precision="fp64", criterion=O.CRIT_REFERENCE,
+              tol=1e-10, nInc=1, force=0):
+    Nx, Ny, Nz = shape
+    s = m3d.Solver(m3d.KIND_MECH, Nx, Ny, Nz, {"e": 0, "ep": 1, "ed": 2}[behav], precision, 1)
+    s.set_material_mech(mat, rve, force)
+    s.set_load(E, X0)
+    s.run(tol, tol, nInc, criterion)
+    o = O.MechOracle(Nx, Ny, Nz, behav)
+    o.material(mat, rve, force_scheme=force)
+    o.set_load(E, X0)
+    o.run(tol, tol, nInc, criterion=criterion)
+    return s, o
+
+
+@pytest.mark.parametrize("shape,force", [((16, 16, 16), 0), ((16, 16, 16), 1), ((12, 16, 20), 0),
+                                         ((15, 15, 15), 0), ((13, 13, 13), 1)])
+def test_elastic_reference_rule(shape, force):
+    rve = sphere_rve(shape, 3.4)
+    E = np.array([1e-3, 0, 0, 0, 2e-4, 0.0])
+    s, o = mech_pair(shape, MAT_SOFT_MATRIX, rve, E, force=force)
+    st = s.stats()
+    assert st["scheme"] == (1 if o.strain_based else 2)
+    assert abs(st["iters"] - o.iters_per_inc[-1]) <= 1
+    assert rel(s.field(m3d.FIELD_STRAIN), o.eps.reshape(6, -1)) < 1e-9
+    assert rel(s.field(m3d.FIELD_STRESS), o.sig.reshape(6, -1)) < 1e-9
+
+
+def test_elastic_stress_based_stiff_matrix():
+    shape = (16, 16, 16)
+    rve = sphere_rve(shape, 4.0)
+    E = np.array([0, 1e6, 0, 0, 0, 3e5])
+    s, o = mech_pair(shape, MAT_STIFF_MATRIX, rve, E)
+    assert rel(s.field(m3d.FIELD_STRAIN), o.eps.reshape(6, -1)) < 1e-9
+    assert rel(s.field(m3d.FIELD_STRESS), o.sig.reshape(6, -1)) < 1e-9
+
+
+@pytest.mark.parametrize("km,ki,shape", [(1.0, 100.0, (16, 16, 16)), (30.0, 25.0, (16, 16, 16)),
+                                         (1.0, 10.0, (15, 15, 15))])
+def test_thermal_reference_rule(km, ki, shape):
+    Nx, Ny, Nz = shape
+    rve = sphere_rve(shape, 4.0)
+    E = np.array([0.0, 0.3, 1.0])
+    s = m3d.Solver(m3d.KIND_THERMAL, Nx, Ny, Nz, 0, "fp64", 1)
+    s.set_material_thermal(km, ki, rve)
+    s.set_load(E)
+    s.run(1e-10, 1e-10, 1, m3d.CRIT_REFERENCE)
+    o = O.ThermOracle(Nx, Ny, Nz)
+    o.material(km, ki, rve)
+    o.set_load(E)
+    o.run(1e-10, 1e-10)
+    assert abs(s.stats()["iters"] - o.iters) <= 1
+    assert rel(s.field(m3d.FIELD_STRAIN), o.grad.reshape(3, -1)) < 1e-9
+    assert rel(s.field(m3d.FIELD_STRESS), o.flux.reshape(3, -1)) < 1e-9
+
+
+def test_elastic_homogenization_fp64():
+    shape = (12, 12, 12)
+    rve = sphere_rve(shape, 3.0)
+    s = m3d.Solver(m3d.KIND_MECH, *shape, 0, "fp64", 6)
+    s.set_material_mech(MAT_SOFT_MATRIX, rve)
+    Ce, Se, ep, sg, _ = s.homogenize(1e-10, 1e-10, m3d.CRIT_REFERENCE)
+    o = O.MechOracle(*shape, "e")
+    o.material(MAT_SOFT_MATRIX, rve)
+    CH, SH = o.homogenization(1e-10, 1e-10)
+    assert np.abs(Ce - CH).max() / np.abs(CH).max() < 1e-9
+    assert np.abs(Se - SH).max() / np.abs(SH).max() < 1e-9
+
+
+def test_thermal_homogenization_fp64():
+    shape = (12, 12, 12)
+    rve = sphere_rve(shape, 3.0)
+    s = m3d.Solver(m3d.KIND_THERMAL, *shape, 0, "fp64", 3)
+    s.set_material_thermal(1.0, 100.0, rve)
+    K, R, g, q, _ = s.homogenize(1e-10, 1e-10, m3d.CRIT_REFERENCE)
+    o = O.ThermOracle(*shape)
+    o.material(1.0, 100.0, rve)
+    KH, RH = o.homogenization(1e-10, 1e-10)
+    assert np.abs(K - KH).max() / np.abs(KH).max() < 1e-9
+
+
+def test_residual_rule_fp64_and_fp32():
+    shape = (16, 16, 16)
+    rve = sphere_rve(shape, 3.4)
+    E = np.array([1e-3, 0, 0, 0, 0, 0.0])
+    o = O.MechOracle(*shape, "e")
+    o.material(MAT_SOFT_MATRIX, rve)
+    o.set_load(E)
+    o.run(1e-12, 0, criterion=O.CRIT_RESIDUAL)
+    for prec, tol, bound in (("fp64", 1e-10, 1e-8), ("fp32", 1e-5, 2e-4), ("fp32_refine", 1e-10, 1e-7)):
+        s = m3d.Solver(m3d.KIND_MECH, *shape, 0, prec, 1)
+        s.set_material_mech(MAT_SOFT_MATRIX, rve)
+        s.set_load(E)
+        s.run(tol, 0, 1, m3d.CRIT_RESIDUAL)
+        err = rel(s.field(m3d.FIELD_STRAIN), o.eps.reshape(6, -1))
+        assert err < bound, (prec, err)
+        st = s.stats()
+        assert st["residual"] < tol
+        if prec == "fp32_refine":
+            assert st["sweeps_fp64"] >= 1 and st["sweeps_fp32"] >= 1
+
+
+def test_refine_homogenization_gate():
+    shape = (16, 16, 16)
+    rve = sphere_rve(shape, 4.0)
+    o = O.MechOracle(*shape, "e")
+    o.material(MAT_SOFT_MATRIX, rve)
+    CH, _ = o.homogenization(1e-12, 0, criterion=O.CRIT_RESIDUAL)
+    s = m3d.Solver(m3d.KIND_MECH, *shape, 0, "fp32_refine", 6)
+    s.set_material_mech(MAT_SOFT_MATRIX, rve)
+    Ce, *_ = s.homogenize(1e-9, 0, m3d.CRIT_RESIDUAL)
+    assert np.abs(Ce - CH).max() / np.abs(CH).max() < 1e-5
+
+
+def test_thermal_refine():
+    shape = (16, 16, 16)
+    rve = sphere_rve(shape, 4.0)
+    o = O.ThermOracle(*shape)
+    o.material(1.0, 100.0, rve)
+    o.set_load(np.array([0, 0, 1.0]))
+    o.run(1e-12, 0, criterion=O.CRIT_RESIDUAL)
+    s = m3d.Solver(m3d.KIND_THERMAL, *shape, 0, "fp32_refine", 1)
+    s.set_material_thermal(1.0, 100.0, rve)
+    s.set_load(np.array([0, 0, 1.0]))
+    s.run(1e-9, 0, 1, m3d.CRIT_RESIDUAL)
+    assert rel(s.field(m3d.FIELD_STRAIN), o.grad.reshape(3, -1)) < 1e-7
+
+
+@pytest.mark.parametrize("behav,mat,ninc", [("ep", np.array([[400e9, .2, 1e30, 0, 1, 0, 1e30],
+                                                              [70e9, .33, 100e6, 1e9, 1, 0, 1e30]]), 3),
+                                             ("ep", MAT_SOFT_MATRIX, 3),
+                                             ("ed", MAT_SOFT_MATRIX, 3)])
+def test_inelastic_reference_rule(behav, mat, ninc):
+    shape = (12, 12, 12)
+    rve = sphere_rve(shape, 3.2, center=(6, 6, 6))
+    E = np.array([0.02, 0, 0, 0, 0, 0.0])
+    X0 = np.array([1.0, 0, 0, 0, 0, 0])
+    s, o = mech_pair(shape, mat, rve, E, X0, behav=behav, tol=1e-8, nInc=ninc)
+    assert rel(s.field(m3d.FIELD_STRAIN), o.eps.reshape(6, -1)) < 1e-8
+    assert rel(s.field(m3d.FIELD_STRESS), o.sig.reshape(6, -1)) < 1e-8
+    prop = s.increments()
+    assert prop.shape[0] == o.ninc_done
+    assert np.abs(prop - o.prop[: o.ninc_done]).max() / np.abs(o.prop).max() < 1e-8
+    if behav == "ep":
+        assert np.abs(s.field(m3d.FIELD_EPS_P) - o.ep_eff.ravel()).max() < 1e-12 + 1e-8 * o.ep_eff.max()
+
+
+def test_batch_equals_single():
+    """Each load case of a batched solve equals the same case solved alone (bitwise)."""
+    shape = (16, 16, 16)
+    rve = sphere_rve(shape, 3.4)
+    Es = [np.eye(6)[w] * 5e-4 for w in range(3)]
+    sb = m3d.Solver(m3d.KIND_MECH, *shape, 0, "fp64", 3)
+    sb.set_material_mech(MAT_SOFT_MATRIX, rve)
+    for w in range(3):
+        sb.set_load(Es[w], None, b=w)
+    sb.run(1e-9, 0, 1, m3d.CRIT_RESIDUAL)
+    for w in range(3):
+        s1 = m3d.Solver(m3d.KIND_MECH, *shape, 0, "fp64", 1)
+        s1.set_material_mech(MAT_SOFT_MATRIX, rve)
+        s1.set_load(Es[w])
+        s1.run(1e-9, 0, 1, m3d.CRIT_RESIDUAL)
+        assert np.array_equal(sb.field(m3d.FIELD_STRAIN, w), s1.field(m3d.FIELD_STRAIN, 0))
