@@ -129,6 +129,19 @@ int m3d_get_stats(const m3d_solver* h, m3d_stats* out);
 /* Per-increment averages of the ep/ed path (prop_homogenized, nInc x 9). */
 int m3d_get_increments(const m3d_solver* h, double* out, int max_rows);
 
+/* Device time of the sweeps, from CUDA events recorded on the handle's stream
+   around every sweep while profiling is enabled (off by default).  Sweeps that
+   only found converged entries are not counted.  No counterpart in the
+   reference, which has no timers. */
+typedef struct {
+    double ms_fp64;      /* summed device time of FP64 sweeps */
+    long long n_fp64;    /* FP64 sweeps timed */
+    double ms_fp32;      /* summed device time of FP32 sweeps */
+    long long n_fp32;    /* FP32 sweeps timed */
+} m3d_profile;
+int m3d_set_profiling(m3d_solver* h, int enable);  /* enabling also resets the counters */
+int m3d_get_profile(const m3d_solver* h, m3d_profile* out);
+
 /* The CUDA stream (cudaStream_t) all work of the handle is ordered on.
    m3d_set_stream replaces it with a caller-owned stream (NULL: the handle's own). */
 void* m3d_get_stream(const m3d_solver* h);

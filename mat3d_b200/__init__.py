@@ -61,6 +61,11 @@ class Stats(ctypes.Structure):
         return d
 
 
+class Profile(ctypes.Structure):
+    _fields_ = [("ms_fp64", ctypes.c_double), ("n_fp64", ctypes.c_longlong),
+                ("ms_fp32", ctypes.c_double), ("n_fp32", ctypes.c_longlong)]
+
+
 _lib = None
 
 # every symbol the C ABI header declares
@@ -68,6 +73,7 @@ EXPORTS = [
     "m3d_create", "m3d_destroy", "m3d_set_material_mech", "m3d_set_material_thermal", "m3d_set_load", "m3d_run",
     "m3d_homogenize", "m3d_get_field", "m3d_get_means", "m3d_get_stats", "m3d_get_increments",
     "m3d_status_string", "m3d_last_error", "m3d_abi_version", "m3d_get_stream", "m3d_set_stream",
+    "m3d_set_profiling", "m3d_get_profile",
 ]
 
 
@@ -102,6 +108,8 @@ def load_library(path: str | None = None):
     L.m3d_get_stream.restype = vp
     L.m3d_get_stream.argtypes = [vp]
     L.m3d_set_stream.argtypes = [vp, vp]
+    L.m3d_set_profiling.argtypes = [vp, i]
+    L.m3d_get_profile.argtypes = [vp, ctypes.POINTER(Profile)]
     if path is None:
         _lib = L
     return L
@@ -182,6 +190,14 @@ class Solver:
         st = Stats()
         _check(self.L, self.L.m3d_get_stats(self.h, ctypes.byref(st)), "get_stats")
         return st.as_dict()
+
+    def set_profiling(self, enable=True):
+        _check(self.L, self.L.m3d_set_profiling(self.h, 1 if enable else 0), "set_profiling")
+
+    def profile(self):
+        p = Profile()
+        _check(self.L, self.L.m3d_get_profile(self.h, ctypes.byref(p)), "get_profile")
+        return {k: getattr(p, k) for k, _ in p._fields_}
 
     def stream_ptr(self):
         """cudaStream_t of the handle (for timing with events on the launching stream)."""

@@ -194,6 +194,29 @@ struct m3d_solver {
     // launch geometry
     int G64 = 2, G32 = 2, TZy64 = 8, TZy32 = 16, TZx64 = 4, TZx32 = 8;
 
+    // per-sweep event timing (m3d_set_profiling)
+    static constexpr int kChunk = 8;
+    bool prof = false;
+    cudaEvent_t pev[kChunk + 1] = {};
+    m3d_profile pr{};
+    void prof_mark(int k) {
+        if (prof) cudaEventRecord(pev[k], stream);
+    }
+    // add the first `executed` sweep intervals of the last chunk (host has synced)
+    void prof_collect(int executed, bool fp64) {
+        if (!prof) return;
+        for (int k = 0; k < executed && k < kChunk; ++k) {
+            float ms = 0;
+            if (cudaEventElapsedTime(&ms, pev[k], pev[k + 1]) != cudaSuccess) continue;
+            if (fp64) { pr.ms_fp64 += ms; pr.n_fp64 += 1; } else { pr.ms_fp32 += ms; pr.n_fp32 += 1; }
+        }
+    }
+    int max_iters() const {
+        int m = 0;
+        for (int b = 0; b < B; ++b) m = std::max(m, h_ctl[b].iters);
+        return m;
+    }
+
     ~m3d_solver();
     int alloc(int batch);
     void free_all();
@@ -444,9 +467,11 @@ int m3d_solver::run_linear(double tol_field, double tol_eq, int criterion, int m
     k_fill_load<T><<<dim3(256, B * CC), 256, 0, stream>>>(x, d_ctl, CC, g.V);
     st.kernel_launches += 1;
     C2* sp = (C2*)d_spec;
-    const int chunk = 8;
+    const int chunk = kChunk;
+    int before = 0;
     for (;;) {
         for (int k = 0; k < chunk; ++k) {
+            prof_mark(k);
             if (criterion == M3D_CRIT_RESIDUAL) {
                 rc = launch_em<T, CC>(d_ctl, x, nullptr, sp, 0, POL_RESIDUAL, nullptr);
             } else {
@@ -455,8 +480,11 @@ int m3d_solver::run_linear(double tol_field, double tol_eq, int criterion, int m
             }
             if (rc) return rc;
         }
+        prof_mark(chunk);
         rc = sync_ctl(d_ctl);
         if (rc) return rc;
+        prof_collect(max_iters() - before, sizeof(T) == 8);
+        before = max_iters();
         bool all = true;
         for (int b = 0; b < B; ++b) all = all && h_ctl[b].done;
         if (all) break;
@@ -497,11 +525,14 @@ int m3d_solver::run_refine(double tol_field, int max_iter) {
     for (;;) {
         ProRefine64<CC> pro{d_phase, x, first ? nullptr : d_delta, g.V, dm(off_P), nph, nullptr};
         EpiDefect<CC> epi{d_phase, x, d_r32, g.V, dm(off_Os), nph, nullptr};
+        prof_mark(0);
         rc = launch_sweep<double, CC>(pro, green<double, CC>(0), epi, d_ctl, sp64, POL_REFINE_OUTER, nullptr);
         if (rc) return rc;
+        prof_mark(1);
         first = false;
         rc = sync_ctl(d_ctl);
         if (rc) return rc;
+        prof_collect(1, true);
         bool all = true;
         for (int b = 0; b < B; ++b) all = all && h_ctl[b].done;
         if (all) break;
@@ -517,13 +548,18 @@ int m3d_solver::run_refine(double tol_field, int max_iter) {
         }
         M3D_CUDA(cudaMemcpyAsync(d_ctl_in, h_ctl, B * sizeof(Ctl), cudaMemcpyHostToDevice, stream));
         M3D_CUDA(cudaMemsetAsync(d_delta, 0, (size_t)B * CC * g.V * sizeof(float), stream));
+        int before = 0;
         for (;;) {
             for (int k = 0; k < chunk; ++k) {
+                prof_mark(k);
                 rc = launch_em<float, CC>(d_ctl_in, d_delta, d_r32, sp32, 1, POL_REFINE_INNER, d_ctl);
                 if (rc) return rc;
             }
+            prof_mark(chunk);
             rc = sync_ctl(d_ctl_in);
             if (rc) return rc;
+            prof_collect(max_iters() - before, false);
+            before = max_iters();
             bool alli = true;
             for (int b = 0; b < B; ++b) alli = alli && h_ctl[b].done;
             if (alli) break;
@@ -708,6 +744,8 @@ int m3d_create(int kind, int Nx, int Ny, int Nz, int behav, int precision, int b
 int m3d_destroy(m3d_solver* h) {
     if (!h) return M3D_OK;
     if (h->stream) cudaStreamSynchronize(h->stream);
+    for (int k = 0; k <= m3d_solver::kChunk; ++k)
+        if (h->pev[k]) cudaEventDestroy(h->pev[k]);
     h->free_all();
     if (h->own_stream) cudaStreamDestroy(h->own_stream);
     delete h;
@@ -813,7 +851,8 @@ int m3d_set_material_mech(m3d_solver* h, const double* mat, int nph, const int32
     h->den_ref = (h->scheme == 1) ? 0.5 * h->Cp[0][0] + 0.5 * h->Cp[p1][0] : 0.5 * h->Sp[0][0] + 0.5 * h->Sp[p1][0];
     int rc = upload_tables(h);
     if (rc) return rc;
-    M3D_CUDA(cudaMemcpy(h->d_phase, ph8.data(), (size_t)V, cudaMemcpyHostToDevice));
+    M3D_CUDA(cudaMemcpyAsync(h->d_phase, ph8.data(), (size_t)V, cudaMemcpyHostToDevice, h->stream));
+    M3D_CUDA(cudaStreamSynchronize(h->stream));
     h->material_set = true;
     h->st.scheme = h->scheme;
     h->st.la0 = h->la0;
@@ -874,7 +913,8 @@ int m3d_set_material_thermal(m3d_solver* h, double km, double ki, const int32_t*
     h->den_ref = (h->scheme == 1) ? 0.5 * ki + 0.5 * km : 0.5 / ki + 0.5 / km;  // (:346, :356)
     int rc = upload_tables(h);
     if (rc) return rc;
-    M3D_CUDA(cudaMemcpy(h->d_phase, ph8.data(), (size_t)V, cudaMemcpyHostToDevice));
+    M3D_CUDA(cudaMemcpyAsync(h->d_phase, ph8.data(), (size_t)V, cudaMemcpyHostToDevice, h->stream));
+    M3D_CUDA(cudaStreamSynchronize(h->stream));
     h->material_set = true;
     h->st.scheme = h->scheme;
     h->st.k0 = h->k0;
@@ -1061,6 +1101,21 @@ int m3d_get_field(m3d_solver* h, int which, int b, double* out) {
     if (h->C == 6)
         return h->prec == M3D_PREC_FP32 ? export_field<float, 6>(h, h->d_x, M, b, out) : export_field<double, 6>(h, h->d_x, M, b, out);
     return h->prec == M3D_PREC_FP32 ? export_field<float, 3>(h, h->d_x, M, b, out) : export_field<double, 3>(h, h->d_x, M, b, out);
+}
+
+int m3d_set_profiling(m3d_solver* h, int enable) {
+    if (!h) return fail(M3D_ERR_ARG, "NULL handle");
+    if (enable && !h->pev[0])
+        for (int k = 0; k <= m3d_solver::kChunk; ++k) M3D_CUDA(cudaEventCreate(&h->pev[k]));
+    h->prof = enable != 0;
+    std::memset(&h->pr, 0, sizeof(h->pr));
+    return M3D_OK;
+}
+
+int m3d_get_profile(const m3d_solver* h, m3d_profile* out) {
+    if (!h || !out) return fail(M3D_ERR_ARG, "NULL argument");
+    *out = h->pr;
+    return M3D_OK;
 }
 
 void* m3d_get_stream(const m3d_solver* h) { return h ? (void*)h->stream : nullptr; }

@@ -211,8 +211,10 @@ int m3d_solver::run_inelastic(double tol_field, double tol_eq, int nInc, int cri
         k_constitutive<T><<<dim3(cblk, B), 256, csmem, stream>>>(cons, d_ctl, d_part);
         k_finalize_j2<<<B, 256, 0, stream>>>(d_ctl, d_part, 13, cblk, POLJ2_START, (double)V, in.d_S0);
         st.kernel_launches += 2;
+        int before = 0;
         for (;;) {
             for (int k = 0; k < chunk; ++k) {
+                prof_mark(k);
                 k_zfwd<T, 6, ProStress<T>><<<dim3(zblk, B), 256, zsmem, stream>>>(g, pz, tw<T>(2), sp, pro, d_ctl, Gl, d_part);
                 k_ypass<T><<<dim3(Nx * ntzy, 6 * B), 256, ysmem, stream>>>(g, py, tw<T>(1), sp, tzy, 6, -1, d_ctl);
                 k_xturn<T, 6, SpecBasic<T>><<<dim3(xblk, B), 256, xsmem, stream>>>(g, px, tw<T>(0), sp, tzx, spec, d_ctl, d_part);
@@ -224,8 +226,11 @@ int m3d_solver::run_inelastic(double tol_field, double tol_eq, int nInc, int cri
                 st.kernel_launches += (criterion == M3D_CRIT_REFERENCE) ? 7 : 6;
             }
             M3D_CUDA(cudaGetLastError());
+            prof_mark(chunk);
             int rc = sync_ctl(d_ctl);
             if (rc) return rc;
+            prof_collect(max_iters() - before, sizeof(T) == 8);
+            before = max_iters();
             bool all = true;
             for (int b = 0; b < B; ++b) all = all && h_ctl[b].done;
             if (all) break;
