@@ -13,6 +13,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <cstdlib>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -20,6 +21,7 @@
 #include "../../include/mat3d_b200.h"
 #include "physics.cuh"
 #include "inelastic.cuh"
+#include "passes_fast.cuh"
 
 using namespace m3d;
 
@@ -235,6 +237,12 @@ struct m3d_solver {
     int launch_sweep(Pro pro, Spec spec, Epi epi, Ctl* ctl, typename Cx<T>::t* sp, int policy, const Ctl* outer);
     template <typename T, int CC>
     int launch_check(Ctl* ctl, const void* x, typename Cx<T>::t* sp);
+    template <typename T, int CC> size_t op_smem() const;
+    template <typename T, int CC, class Pro> void pass_zfwd(Pro pro, Ctl* ctl, typename Cx<T>::t* sp);
+    template <typename T> void pass_y(int sign, int CC, Ctl* ctl, typename Cx<T>::t* sp);
+    template <typename T, int CC, class Spec> int pass_x(Spec op, Ctl* ctl, typename Cx<T>::t* sp);
+    template <typename T, int CC, class Epi> int pass_zinv(Epi epi, Ctl* ctl, typename Cx<T>::t* sp);
+    bool use_fast = true;
     template <typename T, int CC>
     int run_linear(double tol_field, double tol_eq, int criterion, int max_iter);
     template <int CC>
@@ -293,8 +301,12 @@ int m3d_solver::alloc(int batch) {
     const size_t zblk = (size_t)((g.NL + Gmin - 1) / Gmin);
     const int TZmin = std::min(TZx32, TZx64);
     const size_t xblk = (size_t)Ny * ((g.Hzp + TZmin - 1) / TZmin);
-    // (the pointwise kernels launch up to 592 blocks with up to 13 sums each)
-    part_cap = std::max(std::max(zblk, xblk), (size_t)1024) * (size_t)batch * 16;
+    // (the pointwise kernels launch up to 592 blocks with up to 13 sums each;
+    // the fast z passes use at least 2 lines per block, the x passes at least
+    // one column per block)
+    (void)zblk; (void)xblk;
+    const size_t blk_max = std::max(std::max((size_t)(g.NL / 2 + 1), (size_t)Ny * g.Hzp), (size_t)1024);
+    part_cap = blk_max * (size_t)batch * 16;
     M3D_CUDA(cudaMalloc(&d_part, part_cap * sizeof(double)));
     M3D_CUDA(cudaMalloc(&d_ctl, batch * sizeof(Ctl)));
     M3D_CUDA(cudaMalloc(&d_ctl_in, batch * sizeof(Ctl)));
@@ -379,32 +391,142 @@ SpecGreen<T, CC> m3d_solver::green(int zero_k0) const {
     return s;
 }
 
+template <int NN> struct IntC { static constexpr int value = NN; };
+// Calls f(IntC<n>) when n has a compile-time specialised FFT.
+template <class F> bool with_fast_n(int n, F&& f) {
+    switch (n) {
+        case 32: f(IntC<32>{}); return true;
+        case 48: f(IntC<48>{}); return true;
+        case 64: f(IntC<64>{}); return true;
+        case 96: f(IntC<96>{}); return true;
+        case 128: f(IntC<128>{}); return true;
+        case 256: f(IntC<256>{}); return true;
+        default: return false;
+    }
+}
+
+template <typename T, int CC>
+size_t m3d_solver::op_smem() const {
+    return (size_t)nph * std::max(sizeof(PhaseMech), (size_t)(CC * CC + CC) * sizeof(double)) + 64;
+}
+
+template <typename T, int CC, class Pro>
+void m3d_solver::pass_zfwd(Pro pro, Ctl* ctl, typename Cx<T>::t* sp) {
+    typedef typename Cx<T>::t C2;
+    const size_t extra = op_smem<T, CC>();
+    const bool done = use_fast && with_fast_n(Nz, [&](auto nc) {
+        constexpr int NN = decltype(nc)::value;
+        typedef ZTile<T, NN, CC> Z;
+        static bool init = false;
+        if (!init) { allow_smem(k_zfwd_fast<T, NN, CC, Pro>); init = true; }
+        const int blk = (int)((g.NL + Z::G - 1) / Z::G);
+        k_zfwd_fast<T, NN, CC, Pro><<<dim3(blk, B), kFastThreads, z_fast_smem<T, NN, CC>(extra), stream>>>(
+            g, tw<T>(2), sp, pro, ctl);
+    });
+    if (!done) {
+        const int Gl = G<T>();
+        const int zblk = (int)((g.NL + Gl - 1) / Gl);
+        const size_t zsmem = (size_t)Nz * sizeof(C2) + 2 * (size_t)(Gl / 2) * CC * Nz * sizeof(C2) + 16 + 32 * 32 * 8 + extra;
+        static bool init = false;
+        if (!init) { allow_smem(k_zfwd<T, CC, Pro>); init = true; }
+        k_zfwd<T, CC, Pro><<<dim3(zblk, B), 256, zsmem, stream>>>(g, pz, tw<T>(2), sp, pro, ctl, Gl, d_part);
+    }
+    st.kernel_launches += 1;
+}
+
+template <typename T>
+void m3d_solver::pass_y(int sign, int CC, Ctl* ctl, typename Cx<T>::t* sp) {
+    typedef typename Cx<T>::t C2;
+    const bool done = use_fast && with_fast_n(Ny, [&](auto nc) {
+        constexpr int NN = decltype(nc)::value;
+        constexpr int CPW = 32 / LineSplit<T, NN>::Tl;
+        const int ntz = (g.Hzp + 4 * CPW - 1) / (4 * CPW);
+        const dim3 grid(Nx * ntz, CC * B);
+        const size_t sm = ypass_fast_smem<T, NN>();
+        static bool init = false;
+        if (!init) {
+            allow_smem(k_ypass_fast<T, NN, -1>);
+            allow_smem(k_ypass_fast<T, NN, +1>);
+            init = true;
+        }
+        if (sign < 0) k_ypass_fast<T, NN, -1><<<grid, kFastThreads, sm, stream>>>(g, tw<T>(1), sp, CC, ctl);
+        else k_ypass_fast<T, NN, +1><<<grid, kFastThreads, sm, stream>>>(g, tw<T>(1), sp, CC, ctl);
+    });
+    if (!done) {
+        const int tzy = TZy<T>();
+        const size_t ysmem = (size_t)Ny * sizeof(C2) + 2 * (size_t)Ny * tzy * sizeof(C2);
+        const int ntzy = (g.Hzp + tzy - 1) / tzy;
+        static bool init = false;
+        if (!init) { allow_smem(k_ypass<T>); init = true; }
+        k_ypass<T><<<dim3(Nx * ntzy, CC * B), 256, ysmem, stream>>>(g, py, tw<T>(1), sp, tzy, CC, sign, ctl);
+    }
+    st.kernel_launches += 1;
+}
+
+template <typename T, int CC, class Spec>
+int m3d_solver::pass_x(Spec op, Ctl* ctl, typename Cx<T>::t* sp) {
+    typedef typename Cx<T>::t C2;
+    int nblk = 0;
+    const bool done = use_fast && with_fast_n(Nx, [&](auto nc) {
+        constexpr int NN = decltype(nc)::value;
+        constexpr int WPC = XWarps<T, NN, CC>::value;
+        constexpr int CPW = 32 / LineSplit<T, NN>::Tl;
+        const int ntz = (g.Hzp + WPC * CPW - 1) / (WPC * CPW);
+        nblk = Ny * ntz;
+        static bool init = false;
+        if (!init) { allow_smem(k_xturn_fast<T, NN, CC, Spec>); init = true; }
+        k_xturn_fast<T, NN, CC, Spec><<<dim3(nblk, B), WPC * 32, xturn_fast_smem<T, NN, CC>(), stream>>>(
+            g, tw<T>(0), sp, op, ctl, d_part);
+    });
+    if (!done) {
+        const int tzx = TZx<T>();
+        const size_t xsmem = (size_t)Nx * sizeof(C2) + 2 * (size_t)CC * Nx * tzx * sizeof(C2) + 16 + 32 * 32 * 8;
+        const int ntzx = (g.Hzp + tzx - 1) / tzx;
+        nblk = Ny * ntzx;
+        static bool init = false;
+        if (!init) { allow_smem(k_xturn<T, CC, Spec>); init = true; }
+        k_xturn<T, CC, Spec><<<dim3(nblk, B), 256, xsmem, stream>>>(g, px, tw<T>(0), sp, tzx, op, ctl, d_part);
+    }
+    st.kernel_launches += 1;
+    return nblk;
+}
+
+template <typename T, int CC, class Epi>
+int m3d_solver::pass_zinv(Epi epi, Ctl* ctl, typename Cx<T>::t* sp) {
+    typedef typename Cx<T>::t C2;
+    const size_t extra = op_smem<T, CC>();
+    int nblk = 0;
+    const bool done = use_fast && with_fast_n(Nz, [&](auto nc) {
+        constexpr int NN = decltype(nc)::value;
+        typedef ZTile<T, NN, CC> Z;
+        nblk = (int)((g.NL + Z::G - 1) / Z::G);
+        static bool init = false;
+        if (!init) { allow_smem(k_zinv_fast<T, NN, CC, Epi>); init = true; }
+        k_zinv_fast<T, NN, CC, Epi><<<dim3(nblk, B), kFastThreads, z_fast_smem<T, NN, CC>(extra), stream>>>(
+            g, tw<T>(2), sp, epi, ctl, d_part);
+    });
+    if (!done) {
+        const int Gl = G<T>();
+        nblk = (int)((g.NL + Gl - 1) / Gl);
+        const size_t zsmem = (size_t)Nz * sizeof(C2) + 2 * (size_t)(Gl / 2) * CC * Nz * sizeof(C2) + 16 + 32 * 32 * 8 + extra;
+        static bool init = false;
+        if (!init) { allow_smem(k_zinv<T, CC, Epi>); init = true; }
+        k_zinv<T, CC, Epi><<<dim3(nblk, B), 256, zsmem, stream>>>(g, pz, tw<T>(2), sp, epi, ctl, Gl, d_part);
+    }
+    st.kernel_launches += 1;
+    return nblk;
+}
+
 template <typename T, int CC, class Pro, class Spec, class Epi>
 int m3d_solver::launch_sweep(Pro pro, Spec spec, Epi epi, Ctl* ctl, typename Cx<T>::t* sp, int policy,
                              const Ctl* outer) {
-    typedef typename Cx<T>::t C2;
-    const int Gl = G<T>(), tzy = TZy<T>(), tzx = TZx<T>();
-    const int zblk = (int)((g.NL + Gl - 1) / Gl);
-    const size_t mats_bytes = (size_t)nph * (CC * CC + CC) * sizeof(double) + 64;
-    const size_t zsmem = (size_t)Nz * sizeof(C2) + 2 * (size_t)(Gl / 2) * CC * Nz * sizeof(C2) + 16 + 32 * 32 * 8 + mats_bytes;
-    const size_t ysmem = (size_t)Ny * sizeof(C2) + 2 * (size_t)Ny * tzy * sizeof(C2);
-    const size_t xsmem = (size_t)Nx * sizeof(C2) + 2 * (size_t)CC * Nx * tzx * sizeof(C2) + 16 + 32 * 32 * 8;
-    const int ntzy = (g.Hzp + tzy - 1) / tzy, ntzx = (g.Hzp + tzx - 1) / tzx;
-    static bool init = false;
-    if (!init) {
-        allow_smem(k_zfwd<T, CC, Pro>);
-        allow_smem(k_ypass<T>);
-        allow_smem(k_xturn<T, CC, Spec>);
-        allow_smem(k_zinv<T, CC, Epi>);
-        init = true;
-    }
-    k_zfwd<T, CC, Pro><<<dim3(zblk, B), 256, zsmem, stream>>>(g, pz, tw<T>(2), sp, pro, ctl, Gl, d_part);
-    k_ypass<T><<<dim3(Nx * ntzy, CC * B), 256, ysmem, stream>>>(g, py, tw<T>(1), sp, tzy, CC, -1, ctl);
-    k_xturn<T, CC, Spec><<<dim3(Ny * ntzx, B), 256, xsmem, stream>>>(g, px, tw<T>(0), sp, tzx, spec, ctl, d_part);
-    k_ypass<T><<<dim3(Nx * ntzy, CC * B), 256, ysmem, stream>>>(g, py, tw<T>(1), sp, tzy, CC, +1, ctl);
-    k_zinv<T, CC, Epi><<<dim3(zblk, B), 256, zsmem, stream>>>(g, pz, tw<T>(2), sp, epi, ctl, Gl, d_part);
+    pass_zfwd<T, CC>(pro, ctl, sp);
+    pass_y<T>(-1, CC, ctl, sp);
+    pass_x<T, CC>(spec, ctl, sp);
+    pass_y<T>(+1, CC, ctl, sp);
+    const int zblk = pass_zinv<T, CC>(epi, ctl, sp);
     k_finalize<<<B, 256, 0, stream>>>(ctl, d_part, Epi::NSUM, zblk, policy, (double)g.V, outer);
-    st.kernel_launches += 6;
+    st.kernel_launches += 1;
     M3D_CUDA(cudaGetLastError());
     return M3D_OK;
 }
@@ -413,29 +535,13 @@ int m3d_solver::launch_sweep(Pro pro, Spec spec, Epi epi, Ctl* ctl, typename Cx<
 // convergenceCheck reductions (src/3d/FFT_analysis3D.cpp:351-416).
 template <typename T, int CC>
 int m3d_solver::launch_check(Ctl* ctl, const void* x, typename Cx<T>::t* sp) {
-    typedef typename Cx<T>::t C2;
-    const int Gl = G<T>(), tzy = TZy<T>(), tzx = TZx<T>();
-    const int zblk = (int)((g.NL + Gl - 1) / Gl);
-    const size_t mats_bytes = (size_t)nph * (CC * CC + CC) * sizeof(double) + 64;
-    const size_t zsmem = (size_t)Nz * sizeof(C2) + 2 * (size_t)(Gl / 2) * CC * Nz * sizeof(C2) + 16 + 32 * 32 * 8 + mats_bytes;
-    const size_t ysmem = (size_t)Ny * sizeof(C2) + 2 * (size_t)Ny * tzy * sizeof(C2);
-    const size_t xsmem = (size_t)Nx * sizeof(C2) + 2 * (size_t)CC * Nx * tzx * sizeof(C2) + 16 + 32 * 32 * 8;
-    const int ntzy = (g.Hzp + tzy - 1) / tzy, ntzx = (g.Hzp + tzx - 1) / tzx;
     ProMat<T, CC> pro{d_phase, (const T*)x, g.V, dm(off_Q), nph, nullptr};
     SpecEqVar<T, CC> sv{g};
-    static bool init = false;
-    if (!init) {
-        allow_smem(k_zfwd<T, CC, ProMat<T, CC>>);
-        allow_smem(k_xturn<T, CC, SpecEqVar<T, CC>>);
-        allow_smem(k_ypass<T>);
-        init = true;
-    }
-    k_zfwd<T, CC, ProMat<T, CC>><<<dim3(zblk, B), 256, zsmem, stream>>>(g, pz, tw<T>(2), sp, pro, ctl, Gl, d_part);
-    k_ypass<T><<<dim3(Nx * ntzy, CC * B), 256, ysmem, stream>>>(g, py, tw<T>(1), sp, tzy, CC, -1, ctl);
-    const int xblk = Ny * ntzx;
-    k_xturn<T, CC, SpecEqVar<T, CC>><<<dim3(xblk, B), 256, xsmem, stream>>>(g, px, tw<T>(0), sp, tzx, sv, ctl, d_part);
+    pass_zfwd<T, CC>(pro, ctl, sp);
+    pass_y<T>(-1, CC, ctl, sp);
+    const int xblk = pass_x<T, CC>(sv, ctl, sp);
     k_finalize<<<B, 256, 0, stream>>>(ctl, d_part, 2, xblk, POL_REF_CHECK, (double)g.V, nullptr);
-    st.kernel_launches += 4;
+    st.kernel_launches += 1;
     M3D_CUDA(cudaGetLastError());
     return M3D_OK;
 }
@@ -713,6 +819,10 @@ int m3d_create(int kind, int Nx, int Ny, int Nz, int behav, int precision, int b
     cudaError_t e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
     if (e != cudaSuccess) { delete h; return fail(M3D_ERR_CUDA, cudaGetErrorString(e)); }
     h->own_stream = h->stream;
+    {
+        const char* e2 = std::getenv("M3D_GENERIC_FFT");
+        h->use_fast = !(e2 && e2[0] == '1');
+    }
     int rc = h->alloc(batch);
     if (rc) { cudaStreamDestroy(h->stream); delete h; return rc; }
     // twiddles

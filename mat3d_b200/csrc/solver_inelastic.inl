@@ -175,22 +175,11 @@ int m3d_solver::run_inelastic(double tol_field, double tol_eq, int nInc, int cri
     EpiBasic<T> epi{cons};
     ProStress<T> pro{sig, V};
     SpecBasic<T> spec{green<T, 6>(0), SpecEqVar<T, 6>{g}};
-    const int Gl = G<T>(), tzy = TZy<T>(), tzx = TZx<T>();
-    const int zblk = (int)((g.NL + Gl - 1) / Gl);
     const size_t phb = (size_t)nph * sizeof(PhaseMech) + 64;
-    const size_t zsmem = (size_t)Nz * sizeof(C2) + 2 * (size_t)(Gl / 2) * 6 * Nz * sizeof(C2) + 16 + 32 * 32 * 8 + phb;
-    const size_t ysmem = (size_t)Ny * sizeof(C2) + 2 * (size_t)Ny * tzy * sizeof(C2);
-    const size_t xsmem = (size_t)Nx * sizeof(C2) + 2 * (size_t)6 * Nx * tzx * sizeof(C2) + 16 + 32 * 32 * 8;
-    const int ntzy = (g.Hzp + tzy - 1) / tzy, ntzx = (g.Hzp + tzx - 1) / tzx;
-    const int xblk = Ny * ntzx;
     const int cblk = 592;
     const size_t csmem = 32 * 32 * 8 + phb;
     static bool init = false;
     if (!init) {
-        allow_smem(k_zfwd<T, 6, ProStress<T>>);
-        allow_smem(k_ypass<T>);
-        allow_smem(k_xturn<T, 6, SpecBasic<T>>);
-        allow_smem(k_zinv<T, 6, EpiBasic<T>>);
         allow_smem(k_constitutive<T>);
         allow_smem(k_commit<T>);
         init = true;
@@ -215,15 +204,17 @@ int m3d_solver::run_inelastic(double tol_field, double tol_eq, int nInc, int cri
         for (;;) {
             for (int k = 0; k < chunk; ++k) {
                 prof_mark(k);
-                k_zfwd<T, 6, ProStress<T>><<<dim3(zblk, B), 256, zsmem, stream>>>(g, pz, tw<T>(2), sp, pro, d_ctl, Gl, d_part);
-                k_ypass<T><<<dim3(Nx * ntzy, 6 * B), 256, ysmem, stream>>>(g, py, tw<T>(1), sp, tzy, 6, -1, d_ctl);
-                k_xturn<T, 6, SpecBasic<T>><<<dim3(xblk, B), 256, xsmem, stream>>>(g, px, tw<T>(0), sp, tzx, spec, d_ctl, d_part);
-                if (criterion == M3D_CRIT_REFERENCE)
+                pass_zfwd<T, 6>(pro, d_ctl, sp);
+                pass_y<T>(-1, 6, d_ctl, sp);
+                const int xblk = pass_x<T, 6>(spec, d_ctl, sp);
+                if (criterion == M3D_CRIT_REFERENCE) {
                     k_finalize_j2<<<B, 256, 0, stream>>>(d_ctl, d_part, 2, xblk, POLJ2_CHECK, (double)V, in.d_S0);
-                k_ypass<T><<<dim3(Nx * ntzy, 6 * B), 256, ysmem, stream>>>(g, py, tw<T>(1), sp, tzy, 6, +1, d_ctl);
-                k_zinv<T, 6, EpiBasic<T>><<<dim3(zblk, B), 256, zsmem, stream>>>(g, pz, tw<T>(2), sp, epi, d_ctl, Gl, d_part);
+                    st.kernel_launches += 1;
+                }
+                pass_y<T>(+1, 6, d_ctl, sp);
+                const int zblk = pass_zinv<T, 6>(epi, d_ctl, sp);
                 k_finalize_j2<<<B, 256, 0, stream>>>(d_ctl, d_part, 13, zblk, POLJ2_SWEEP, (double)V, in.d_S0);
-                st.kernel_launches += (criterion == M3D_CRIT_REFERENCE) ? 7 : 6;
+                st.kernel_launches += 1;
             }
             M3D_CUDA(cudaGetLastError());
             prof_mark(chunk);

@@ -198,3 +198,74 @@ def test_batch_equals_single():
         s1.set_load(Es[w])
         s1.run(1e-9, 0, 1, m3d.CRIT_RESIDUAL)
         assert np.array_equal(sb.field(m3d.FIELD_STRAIN, w), s1.field(m3d.FIELD_STRAIN, 0))
+
+
+# ---- compile-time specialised FFT sizes (32, 48, 64, 96, 128, 256) ---------
+@pytest.mark.parametrize("shape,force", [((32, 32, 32), 1), ((32, 48, 64), 0), ((64, 32, 48), 2),
+                                         ((96, 32, 32), 1), ((32, 32, 128), 0)])
+def test_elastic_fast_sizes(shape, force):
+    rve = sphere_rve(shape, min(shape) / 4)
+    E = np.array([1e-3, 0, 2e-4, 0, 2e-4, 1e-4])
+    s, o = mech_pair(shape, MAT_SOFT_MATRIX, rve, E, force=force, tol=1e-9)
+    assert abs(s.stats()["iters"] - o.iters_per_inc[-1]) <= 1
+    assert rel(s.field(m3d.FIELD_STRAIN), o.eps.reshape(6, -1)) < 1e-9
+    assert rel(s.field(m3d.FIELD_STRESS), o.sig.reshape(6, -1)) < 1e-9
+
+
+@pytest.mark.parametrize("km,ki,shape", [(1.0, 100.0, (32, 32, 32)), (30.0, 25.0, (48, 48, 48)),
+                                         (1.0, 10.0, (64, 64, 64))])
+def test_thermal_fast_sizes(km, ki, shape):
+    rve = sphere_rve(shape, min(shape) / 4)
+    E = np.array([0.2, 0.3, 1.0])
+    s = m3d.Solver(m3d.KIND_THERMAL, *shape, 0, "fp64", 1)
+    s.set_material_thermal(km, ki, rve)
+    s.set_load(E)
+    s.run(1e-9, 1e-9, 1, m3d.CRIT_REFERENCE)
+    o = O.ThermOracle(*shape)
+    o.material(km, ki, rve)
+    o.set_load(E)
+    o.run(1e-9, 1e-9)
+    assert abs(s.stats()["iters"] - o.iters) <= 1
+    assert rel(s.field(m3d.FIELD_STRAIN), o.grad.reshape(3, -1)) < 1e-9
+
+
+@pytest.mark.parametrize("prec,bound", [("fp32", 2e-4), ("fp32_refine", 1e-7)])
+def test_fast_fp32_paths(prec, bound):
+    shape = (64, 64, 64)
+    rve = sphere_rve(shape, 14)
+    E = np.array([0, 0, 1.0])
+    o = O.ThermOracle(*shape)
+    o.material(1.0, 100.0, rve)
+    o.set_load(E)
+    o.run(1e-12, 0, criterion=O.CRIT_RESIDUAL)
+    s = m3d.Solver(m3d.KIND_THERMAL, *shape, 0, prec, 1)
+    s.set_material_thermal(1.0, 100.0, rve)
+    s.set_load(E)
+    s.run(1e-9 if prec == "fp32_refine" else 1e-5, 0, 1, m3d.CRIT_RESIDUAL)
+    assert rel(s.field(m3d.FIELD_STRAIN), o.grad.reshape(3, -1)) < bound
+
+
+def test_fast_j2():
+    shape = (32, 32, 32)
+    rve = sphere_rve(shape, 7.0)
+    mat = np.array([[400e9, .2, 1e30, 0, 1, 0, 1e30], [70e9, .33, 100e6, 1e9, 1, 0, 1e30]])
+    E = np.array([0.02, 0, 0, 0, 0, 0.0])
+    X0 = np.array([1.0, 0, 0, 0, 0, 0])
+    s, o = mech_pair(shape, mat, rve, E, X0, behav="ep", tol=1e-8, nInc=2)
+    assert rel(s.field(m3d.FIELD_STRESS), o.sig.reshape(6, -1)) < 1e-8
+
+
+def test_fast_matches_generic(monkeypatch):
+    shape = (64, 64, 64)
+    rve = sphere_rve(shape, 12)
+    E = np.array([1e-3, 0, 0, 0, 0, 0.0])
+    out = []
+    for generic in ("0", "1"):
+        monkeypatch.setenv("M3D_GENERIC_FFT", generic)
+        s = m3d.Solver(m3d.KIND_MECH, *shape, 0, "fp64", 1)
+        s.set_material_mech(MAT_SOFT_MATRIX, rve)
+        s.set_load(E)
+        s.run(1e-9, 0, 1, m3d.CRIT_RESIDUAL)
+        out.append((s.field(m3d.FIELD_STRAIN), s.stats()["iters"]))
+    assert out[0][1] == out[1][1]
+    assert rel(out[0][0], out[1][0]) < 1e-12
