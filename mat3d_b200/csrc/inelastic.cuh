@@ -173,11 +173,21 @@ struct ProStress {
     static constexpr int NSUM = 0;
     const T* sig;
     long long V;
+    struct Pre {
+        T s[6];
+    };
     __device__ __forceinline__ void load_smem(char*) {}
-    __device__ __forceinline__ void eval(int b, long long v, T (&out)[6], double*) const {
+    __device__ __forceinline__ Pre load(int b, long long v) const {
+        Pre q;
 #pragma unroll
-        for (int c = 0; c < 6; ++c) out[c] = sig[((long long)b * 6 + c) * V + v];
+        for (int c = 0; c < 6; ++c) q.s[c] = sig[((long long)b * 6 + c) * V + v];
+        return q;
     }
+    __device__ __forceinline__ void eval_pre(const Pre& q, int, long long, T (&out)[6]) const {
+#pragma unroll
+        for (int c = 0; c < 6; ++c) out[c] = q.s[c];
+    }
+    __device__ __forceinline__ void eval(int b, long long v, T (&out)[6], double*) const { eval_pre(load(b, v), b, v, out); }
 };
 
 // spectral op of the basic scheme: reductions of sig^ for the reference stop
@@ -199,7 +209,13 @@ struct SpecBasic {
 template <typename T>
 struct EpiBasic {
     static constexpr int NSUM = 13;
+    static constexpr bool kPrefetch = false;  // 19 values per voxel: loaded at use
     EpiConstitutive<T> c;
+    struct Pre {};
+    __device__ __forceinline__ Pre load(int, long long) const { return Pre{}; }
+    __device__ __forceinline__ void apply_pre(const Pre&, int b, long long v, T (&xc)[6], double* acc) const {
+        c.apply(b, v, xc, acc);
+    }
     __device__ __forceinline__ void load_smem(char* s) { c.load_smem(s); }
     __device__ __forceinline__ void apply(int b, long long v, T (&xc)[6], double* acc) const { c.apply(b, v, xc, acc); }
 };
@@ -304,27 +320,31 @@ __device__ __forceinline__ double prodv(const double* a, const double* b) {
 
 // updateE (:583-594): x = S0 <sig> - <eps>; k = (sum(dE) incNo + prod(x,X0)) / prod(S0 X0, X0);
 // E = k S0 X0 - S0 <sig> + <eps>.  S0 is isotropic: passed as its 6x6 in aux2.
+__device__ __forceinline__ void policy_j2(Ctl& c, const double* tot, int policy, double V, const double* S0m);
+
 __global__ void k_finalize_j2(Ctl* ctl, const double* __restrict__ partials, int NS, int nblk, int policy, double V,
                               const double* __restrict__ S0m) {
     const int b = blockIdx.x;
-    Ctl& c = ctl[b];
-    if (c.done) return;
+    if (ctl[b].done) return;
     __shared__ double red[256];
     __shared__ double tot[16];
-    for (int s = 0; s < NS; ++s) {
-        double t = 0;
-        const double* p = partials + ((long long)b * NS + s) * nblk;
-        for (int i = threadIdx.x; i < nblk; i += blockDim.x) t += p[i];
-        red[threadIdx.x] = t;
-        __syncthreads();
-        for (int o = blockDim.x / 2; o > 0; o >>= 1) {
-            if (threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
-            __syncthreads();
-        }
-        if (threadIdx.x == 0) tot[s] = red[0];
-        __syncthreads();
+    sum_partials(partials, NS, nblk, b, red, tot);
+    if (threadIdx.x == 0) policy_j2(ctl[b], tot, policy, V, S0m);
+}
+
+struct FinJ2 {
+    int policy;
+    double V;
+    const double* S0m;
+    int* counter;
+    __device__ __forceinline__ void run(Ctl* ctl, const double* partials, int NS, int nblk, int b, double* red,
+                                        double* tot) const {
+        sum_partials(partials, NS, nblk, b, red, tot);
+        if (threadIdx.x == 0) policy_j2(ctl[b], tot, policy, V, S0m);
     }
-    if (threadIdx.x != 0) return;
+};
+
+__device__ __forceinline__ void policy_j2(Ctl& c, const double* tot, int policy, double V, const double* S0m) {
     if (policy == POLJ2_CHECK) {
         // convergenceCheck of the state produced by the previous sweep (itNo = iters)
         if (c.iters < 1) return;

@@ -72,6 +72,31 @@ __device__ __forceinline__ void block_reduce_store(double (&acc)[NS], double* re
     }
 }
 
+// No fused finalize.
+struct FinNone {
+    int* counter = nullptr;
+    __device__ __forceinline__ void run(Ctl*, const double*, int, int, int, double*, double*) const {}
+};
+
+// The last block of a pass (per batch entry) to finish runs the finalize on
+// all blocks' partials: threadfence + completion counter, the counter reset
+// by that block for the next launch.  All threads of the block must call it.
+template <class Fin>
+__device__ __forceinline__ void fused_finalize(const Fin& fin, Ctl* ctl, const double* partials, int NS, int b) {
+    if (fin.counter == nullptr) return;
+    __shared__ int last;
+    __shared__ double red[256];
+    __shared__ double tot[16];
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) last = (atomicAdd(&fin.counter[b], 1) == (int)gridDim.x - 1);
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    fin.run(ctl, partials, NS, gridDim.x, b, red, tot);
+    if (threadIdx.x == 0) fin.counter[b] = 0;
+}
+
 // ---- shared-memory carve-up helper -----------------------------------------
 __device__ __forceinline__ char* align_up(char* p, int a) {
     return (char*)(((uintptr_t)p + (a - 1)) & ~(uintptr_t)(a - 1));
@@ -245,10 +270,10 @@ __global__ void __launch_bounds__(256) k_xturn(GridDims g, LinePlan px, const ty
 // Nyquist imaginary parts dropped, which is FFTW's c2r rule) -> inverse FFT ->
 // real parts / imaginary parts are the two real lines -> epilogue per voxel.
 // ============================================================================
-template <typename T, int C, class Epi>
+template <typename T, int C, class Epi, class Fin>
 __global__ void __launch_bounds__(256) k_zinv(GridDims g, LinePlan pz, const typename Cx<T>::t* __restrict__ twz,
-                                              const typename Cx<T>::t* __restrict__ spec, Epi epi,
-                                              const Ctl* __restrict__ ctl, int G, double* partials) {
+                                              const typename Cx<T>::t* __restrict__ spec, Epi epi, Ctl* ctl, int G,
+                                              double* partials, Fin fin) {
     typedef typename Cx<T>::t C2;
     const int b = blockIdx.y;
     if (ctl[b].done) return;
@@ -300,6 +325,7 @@ __global__ void __launch_bounds__(256) k_zinv(GridDims g, LinePlan pz, const typ
     }
     if constexpr (Epi::NSUM > 0) {
         block_reduce_store<Epi::NSUM>(acc, red, partials, b, gridDim.x, blockIdx.x);
+        fused_finalize(fin, ctl, partials, Epi::NSUM, b);
     }
 }
 

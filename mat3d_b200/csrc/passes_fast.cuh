@@ -1,16 +1,22 @@
 // passes_fast.cuh -- the five sweep passes for compile-time line lengths
-// (16, 32, 48, 64, 96, 128, 256), built on the warp-split line FFT of
+// (32, 48, 64, 96, 128, 256), built on the warp-split line FFT of
 // fft_reg.cuh.  Same data layout, operators and reductions as the generic
 // kernels in passes.cuh, which remain the path for any other length.
 //
 // Column passes (y, x): lane = col + CPW*t with CPW = 32/T columns per warp,
 // so one load instruction touches CPW consecutive complex words of T rows
-// (whole 32-byte sectors); data goes from global memory straight into
-// registers, one warp-local exchange per transform, and back.
+// (whole 32-byte sectors).  The y pass goes global -> registers -> one
+// warp-local exchange -> global.  The x turnaround first issues cp.async
+// copies of all C components of its columns into a per-warp staging area
+// (all loads in flight together), transforms each component there (the
+// staging rows double as the exchange buffer), applies the spectral op to
+// every mode with all components at hand, and transforms back.
 // z passes: a tile of G voxel lines is staged in shared memory (the
 // prologue/epilogue need all components of a voxel); components are packed
-// two per complex line (c0 + i c1, ...), transformed by warps in registers and
-// split into half spectra.
+// two per complex line (c0 + i c1, ...) and each line is transformed by T
+// lanes in registers, exchanging through its own padded tile row.  The
+// epilogue's global loads are issued before the tile FFT so their latency
+// overlaps it.
 #pragma once
 #include "fft_reg.cuh"
 #include "passes.cuh"
@@ -19,9 +25,27 @@ namespace m3d {
 
 constexpr int kFastThreads = 128;
 
+// Row length (complex elements) of a line that is also its exchange buffer:
+// at least max(N, E*(T+1)), padded so that consecutive rows start 16 banks
+// apart (FP32: rows of 8 mod 16 complex; FP64: 4 mod 8).
+template <typename T, int N>
+struct RowLen {
+    static constexpr int E = LineSplit<T, N>::E, TL = LineSplit<T, N>::Tl;
+    static constexpr int base = (N > E * (TL + 1)) ? N : E * (TL + 1);
+    static constexpr int mod = sizeof(T) == 4 ? 16 : 8, tgt = sizeof(T) == 4 ? 8 : 4;
+    static constexpr int value = base + ((tgt - base % mod) + mod) % mod;
+};
+
 // ---------------------------------------------------------------------------
 // y pass: CTA = 4 warps = 4*CPW consecutive kz columns of one (batch*comp, x)
 // ---------------------------------------------------------------------------
+template <typename T, int N>
+constexpr size_t ypass_fast_smem() {
+    typedef typename Cx<T>::t C2;
+    constexpr int E = LineSplit<T, N>::E, TL = LineSplit<T, N>::Tl, CPW = 32 / TL;
+    return (size_t)N * sizeof(C2) + (size_t)4 * CPW * Xch<E, TL>::size * sizeof(C2);
+}
+
 template <typename T, int N, int SIGN>
 __global__ void __launch_bounds__(kFastThreads) k_ypass_fast(GridDims g, const typename Cx<T>::t* __restrict__ twy,
                                                             typename Cx<T>::t* __restrict__ spec, int C,
@@ -66,23 +90,36 @@ __global__ void __launch_bounds__(kFastThreads) k_ypass_fast(GridDims g, const t
 }
 
 // ---------------------------------------------------------------------------
-// x turnaround: CTA = 4 warps = 4*CPW kz columns of one (batch, y); each lane
-// transforms all C components of its column, staging the spectra in shared
-// memory so the spectral op sees all components of a mode.
+// x turnaround
 // ---------------------------------------------------------------------------
-template <typename T, int N>
-constexpr size_t ypass_fast_smem() {
-    typedef typename Cx<T>::t C2;
-    constexpr int E = LineSplit<T, N>::E, TL = LineSplit<T, N>::Tl, CPW = 32 / TL;
-    return (size_t)N * sizeof(C2) + (size_t)4 * CPW * Xch<E, TL>::size * sizeof(C2);
+// 8- or 16-byte asynchronous global->shared copy; src_bytes = 0 writes zeros
+__device__ __forceinline__ void cp_async(void* smem_dst, const void* gmem_src, int bytes, int src_bytes) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(smem_dst);
+    if (bytes == 8)
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(d), "l"(gmem_src), "r"(src_bytes));
+    else
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(d), "l"(gmem_src), "r"(src_bytes));
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+    asm volatile("cp.async.commit_group;\n" ::);
+    asm volatile("cp.async.wait_group 0;\n" ::);
 }
 
-// warps per CTA of the x turnaround: as many as keep the staging <= 64 KB
+// warps per CTA of the x turnaround: as many as keep the staging <= 24 KB
+// (small CTAs: many resident per SM and a fine-grained tail)
 template <typename T, int N, int C>
 struct XWarps {
-    static constexpr size_t per_warp = (size_t)C * N * (32 / LineSplit<T, N>::Tl) * sizeof(typename Cx<T>::t);
-    static constexpr int value = (4 * per_warp <= 64 * 1024) ? 4 : ((2 * per_warp <= 64 * 1024) ? 2 : 1);
+    static constexpr size_t per_warp =
+        (size_t)C * (32 / LineSplit<T, N>::Tl) * RowLen<T, N>::value * sizeof(typename Cx<T>::t);
+    static constexpr int value = (4 * per_warp <= 24 * 1024) ? 4 : ((2 * per_warp <= 24 * 1024) ? 2 : 1);
 };
+
+template <typename T, int N, int C, int NSUM>
+constexpr size_t xturn_fast_smem() {
+    typedef typename Cx<T>::t C2;
+    return (size_t)N * sizeof(C2) + (size_t)XWarps<T, N, C>::value * XWarps<T, N, C>::per_warp + 16 +
+           (size_t)32 * NSUM * sizeof(double);
+}
 
 template <typename T, int N, int C, class Spec>
 __global__ void __launch_bounds__(kFastThreads) k_xturn_fast(GridDims g, const typename Cx<T>::t* __restrict__ twx,
@@ -90,17 +127,14 @@ __global__ void __launch_bounds__(kFastThreads) k_xturn_fast(GridDims g, const t
                                                             const Ctl* __restrict__ ctl, double* partials) {
     typedef typename Cx<T>::t C2;
     constexpr int E = LineSplit<T, N>::E, TL = LineSplit<T, N>::Tl, CPW = 32 / TL;
-    constexpr int XS = Xch<E, TL>::size;
     constexpr int WPC = XWarps<T, N, C>::value;
+    constexpr int RL = RowLen<T, N>::value;
     const int b = blockIdx.y;
     if (ctl[b].done) return;
     extern __shared__ __align__(16) char smem_raw[];
     C2* tw = (C2*)smem_raw;
-    C2* xch = tw + N;
-    C2* stage = xch + WPC * CPW * XS;                    // [warp][c][r][lane]
-    double* red = (double*)align_up((char*)(stage + WPC * C * E * 32), 16);
-    for (int i = threadIdx.x; i < N; i += blockDim.x) tw[i] = twx[i];
-    __syncthreads();
+    C2* stage = tw + N;  // [warp][c][col][RL]
+    double* red = (double*)align_up((char*)(stage + WPC * C * CPW * RL), 16);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int col = lane % CPW, t = lane / CPW;
     const int ncol_cta = WPC * CPW;
@@ -108,58 +142,66 @@ __global__ void __launch_bounds__(kFastThreads) k_xturn_fast(GridDims g, const t
     const int y = blockIdx.x / ntz;
     const int kz = (blockIdx.x - y * ntz) * ncol_cta + warp * CPW + col;
     const bool ok = kz < g.Hzp;
-    const long long cstride = g.NL * g.Hzp;  // component stride
-    C2* base = spec + ((long long)b * C * g.NL + y) * g.Hzp + (ok ? kz : 0);
-    const long long xstride = (long long)g.Ny * g.Hzp;
-    C2* xl = xch + (warp * CPW + col) * XS;
-    C2* st = stage + warp * C * E * 32;
+    const long long cstride = g.NL * g.Hzp;            // component stride
+    const long long xstride = (long long)g.Ny * g.Hzp;  // x stride
+    const C2* base = spec + ((long long)b * C * g.NL + y) * g.Hzp + (ok ? kz : 0);
+    C2* wst = stage + warp * C * CPW * RL;
+    // issue every load of the warp's columns (all components) at once
 #pragma unroll 1
     for (int c = 0; c < C; ++c) {
+        C2* row = wst + (c * CPW + col) * RL;
+#pragma unroll
+        for (int j = 0; j < E; ++j)
+            cp_async(row + t + TL * j, base + c * cstride + (long long)(t + TL * j) * xstride, (int)sizeof(C2),
+                     ok ? (int)sizeof(C2) : 0);
+    }
+    for (int i = threadIdx.x; i < N; i += blockDim.x) tw[i] = twx[i];
+    cp_async_wait_all();
+    __syncthreads();
+#pragma unroll 1
+    for (int c = 0; c < C; ++c) {
+        C2* row = wst + (c * CPW + col) * RL;
         C2 v[E];
 #pragma unroll
-        for (int j = 0; j < E; ++j) v[j] = ok ? base[c * cstride + (t + TL * j) * xstride] : mk<C2>(0, 0);
-        line_fwd<C2, E, TL>(v, t, xl, tw);
+        for (int j = 0; j < E; ++j) v[j] = row[t + TL * j];
+        __syncwarp();
+        line_fwd<C2, E, TL>(v, t, row, tw);
 #pragma unroll
-        for (int r = 0; r < E; ++r) st[(c * E + r) * 32 + lane] = v[r];
+        for (int r = 0; r < E; ++r) row[spec_mode<E, TL>(t, r)] = v[r];
     }
     double acc[Spec::NSUM > 0 ? Spec::NSUM : 1] = {};
     const bool live = ok && kz < g.Hz;
 #pragma unroll 1
     for (int r = 0; r < E; ++r) {
+        const int mode = spec_mode<E, TL>(t, r);
         C2 m[C];
 #pragma unroll
-        for (int c = 0; c < C; ++c) m[c] = st[(c * E + r) * 32 + lane];
-        if (live) op.apply(b, spec_mode<E, TL>(t, r), y, kz, m, acc, ctl);
+        for (int c = 0; c < C; ++c) m[c] = wst[(c * CPW + col) * RL + mode];
+        if (live) op.apply(b, mode, y, kz, m, acc, ctl);
         if constexpr (Spec::kInverse) {
 #pragma unroll
-            for (int c = 0; c < C; ++c) st[(c * E + r) * 32 + lane] = m[c];
+            for (int c = 0; c < C; ++c) wst[(c * CPW + col) * RL + mode] = m[c];
         }
     }
     if constexpr (Spec::NSUM > 0) {
         block_reduce_store<Spec::NSUM>(acc, red, partials, b, gridDim.x, blockIdx.x);
     }
     if constexpr (Spec::kInverse) {
+        C2* out = spec + ((long long)b * C * g.NL + y) * g.Hzp + (ok ? kz : 0);
 #pragma unroll 1
         for (int c = 0; c < C; ++c) {
+            C2* row = wst + (c * CPW + col) * RL;
             C2 v[E];
 #pragma unroll
-            for (int r = 0; r < E; ++r) v[r] = st[(c * E + r) * 32 + lane];
-            line_inv<C2, E, TL>(v, t, xl, tw);
+            for (int r = 0; r < E; ++r) v[r] = row[spec_mode<E, TL>(t, r)];
+            __syncwarp();
+            line_inv<C2, E, TL>(v, t, row, tw);
             if (ok) {
 #pragma unroll
-                for (int j = 0; j < E; ++j) base[c * cstride + (t + TL * j) * xstride] = v[j];
+                for (int j = 0; j < E; ++j) out[c * cstride + (long long)(t + TL * j) * xstride] = v[j];
             }
         }
     }
-}
-
-template <typename T, int N, int C>
-constexpr size_t xturn_fast_smem() {
-    typedef typename Cx<T>::t C2;
-    constexpr int E = LineSplit<T, N>::E, TL = LineSplit<T, N>::Tl, CPW = 32 / TL;
-    constexpr int WPC = XWarps<T, N, C>::value;
-    return (size_t)N * sizeof(C2) + (size_t)WPC * CPW * Xch<E, TL>::size * sizeof(C2) +
-           (size_t)WPC * C * E * 32 * sizeof(C2) + 16 + 32 * 32 * sizeof(double);
 }
 
 // ---------------------------------------------------------------------------
@@ -167,56 +209,57 @@ constexpr size_t xturn_fast_smem() {
 // ---------------------------------------------------------------------------
 template <int C> struct NclOf { static constexpr int value = (C + 1) / 2; };
 
-// G: voxel lines per CTA; chosen so that G * NCL lines keep 4 warps busy
 template <typename T, int N, int C>
 struct ZTile {
     static constexpr int E = LineSplit<T, N>::E, TL = LineSplit<T, N>::Tl, LPW = 32 / TL;
     static constexpr int NCL = NclOf<C>::value;
     static constexpr int G = (4 * LPW) / NCL > 0 ? (4 * LPW) / NCL : 1;  // voxel lines per CTA
     static constexpr int LINES = G * NCL;
-    // padded tile row: consecutive lines start 16 banks apart
-    static constexpr int ROW = N + (sizeof(T) == 4 ? 8 : 4);
+    static constexpr int SLOTS = ((LINES + 4 * LPW - 1) / (4 * LPW)) * 4 * LPW;  // rows incl. idle-lane rows
+    static constexpr int ROW = RowLen<T, N>::value;
+    static constexpr int TOT = G * N;  // voxels per CTA
+    static constexpr int PER = (TOT + kFastThreads - 1) / kFastThreads;
 };
 
 template <typename T, int N, int C>
 constexpr size_t z_fast_smem(size_t extra) {
     typedef typename Cx<T>::t C2;
     typedef ZTile<T, N, C> Z;
-    return (size_t)N * sizeof(C2) + (size_t)Z::LINES * Z::ROW * sizeof(C2) +
-           (size_t)4 * Z::LPW * Xch<Z::E, Z::TL>::size * sizeof(C2) + 16 + 32 * 32 * sizeof(double) + extra;
+    return (size_t)N * sizeof(C2) + (size_t)Z::SLOTS * Z::ROW * sizeof(C2) + 16 + 32 * 16 * sizeof(double) + extra;
 }
 
-// transform the tile's complex lines in place: fwd (natural -> natural order
-// spectrum) or inv
-template <typename C2, int N, int E, int TL, int LINES, int ROW, bool FWD>
-__device__ __forceinline__ void z_tile_fft(C2* tile, C2* xch, const C2* tw) {
+template <typename T, int N, int C>
+constexpr size_t zinv_fast_smem(size_t extra) {
+    return z_fast_smem<T, N, C>(extra) + (size_t)ZTile<T, N, C>::G * C * (N / 2 + 1) * sizeof(typename Cx<T>::t);
+}
+
+// transform the tile's complex lines in place (FWD: natural order in,
+// natural-order spectrum out; !FWD: the inverse), each line's row doubling as
+// its exchange buffer
+template <typename C2, int N, int E, int TL, int SLOTS, int ROW, bool FWD>
+__device__ __forceinline__ void z_tile_fft(C2* tile, const C2* tw) {
     constexpr int LPW = 32 / TL;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int t = lane % TL, lw = lane / TL;
-    C2* xl = xch + (warp * LPW + lw) * Xch<E, TL>::size;
-    const int nw = blockDim.x >> 5;
+    constexpr int NW = kFastThreads / 32;
 #pragma unroll 1
-    for (int l0 = warp * LPW; l0 < LINES; l0 += nw * LPW) {
-        const int line = l0 + lw;
-        const bool ok = line < LINES;
-        C2* row = tile + (ok ? line : 0) * ROW;
+    for (int l0 = warp * LPW; l0 < SLOTS; l0 += NW * LPW) {
+        C2* row = tile + (l0 + lw) * ROW;
         C2 v[E];
         if constexpr (FWD) {
 #pragma unroll
             for (int j = 0; j < E; ++j) v[j] = row[t + TL * j];
-            line_fwd<C2, E, TL>(v, t, xl, tw);
-            if (ok) {
+            __syncwarp();
+            line_fwd<C2, E, TL>(v, t, row, tw);
 #pragma unroll
-                for (int r = 0; r < E; ++r) row[spec_mode<E, TL>(t, r)] = v[r];
-            }
+            for (int r = 0; r < E; ++r) row[spec_mode<E, TL>(t, r)] = v[r];
         } else {
 #pragma unroll
             for (int r = 0; r < E; ++r) v[r] = row[spec_mode<E, TL>(t, r)];
-            line_inv<C2, E, TL>(v, t, xl, tw);
-            if (ok) {
+            __syncwarp();
+            line_inv<C2, E, TL>(v, t, row, tw);
 #pragma unroll
-                for (int j = 0; j < E; ++j) row[t + TL * j] = v[j];
-            }
+            for (int j = 0; j < E; ++j) row[t + TL * j] = v[j];
         }
     }
 }
@@ -232,19 +275,28 @@ __global__ void __launch_bounds__(kFastThreads) k_zfwd_fast(GridDims g, const ty
     extern __shared__ __align__(16) char smem_raw[];
     C2* tw = (C2*)smem_raw;
     C2* tile = tw + N;
-    C2* xch = tile + Z::LINES * Z::ROW;
-    char* extra = align_up((char*)(xch + 4 * Z::LPW * Xch<Z::E, Z::TL>::size), 16) + 32 * 32 * sizeof(double);
+    char* extra = align_up((char*)(tile + Z::SLOTS * Z::ROW), 16) + 32 * 16 * sizeof(double);
+    const long long l0 = (long long)blockIdx.x * Z::G;
+    // all prologue loads first
+    typename Pro::Pre pre[Z::PER];
+#pragma unroll
+    for (int k = 0; k < Z::PER; ++k) {
+        const int i = threadIdx.x + k * kFastThreads;
+        const int gi = i / N, z = i - gi * N;
+        if (i < Z::TOT && l0 + gi < g.NL) pre[k] = pro.load(b, (l0 + gi) * N + z);
+    }
     for (int i = threadIdx.x; i < N; i += blockDim.x) tw[i] = twz[i];
     pro.load_smem(extra);
     __syncthreads();
-    const long long l0 = (long long)blockIdx.x * Z::G;
-    double dummy[1];
-    for (int i = threadIdx.x; i < Z::G * N; i += blockDim.x) {
+#pragma unroll
+    for (int k = 0; k < Z::PER; ++k) {
+        const int i = threadIdx.x + k * kFastThreads;
+        if (i >= Z::TOT) break;
         const int gi = i / N, z = i - gi * N;
         const long long l = l0 + gi;
         T val[C];
         if (l < g.NL) {
-            pro.eval(b, l * N + z, val, dummy);
+            pro.eval_pre(pre[k], b, l * N + z, val);
         } else {
 #pragma unroll
             for (int c = 0; c < C; ++c) val[c] = (T)0;
@@ -254,7 +306,7 @@ __global__ void __launch_bounds__(kFastThreads) k_zfwd_fast(GridDims g, const ty
             tile[(gi * Z::NCL + cl) * Z::ROW + z] = mk<C2>(val[2 * cl], (2 * cl + 1 < C) ? val[2 * cl + 1] : (T)0);
     }
     __syncthreads();
-    z_tile_fft<C2, N, Z::E, Z::TL, Z::LINES, Z::ROW, true>(tile, xch, tw);
+    z_tile_fft<C2, N, Z::E, Z::TL, Z::SLOTS, Z::ROW, true>(tile, tw);
     __syncthreads();
     const int Hz = g.Hz, Hzp = g.Hzp;
     for (int i = threadIdx.x; i < Z::G * C * Hzp; i += blockDim.x) {
@@ -274,10 +326,10 @@ __global__ void __launch_bounds__(kFastThreads) k_zfwd_fast(GridDims g, const ty
     }
 }
 
-template <typename T, int N, int C, class Epi>
+template <typename T, int N, int C, class Epi, class Fin>
 __global__ void __launch_bounds__(kFastThreads) k_zinv_fast(GridDims g, const typename Cx<T>::t* __restrict__ twz,
                                                            const typename Cx<T>::t* __restrict__ spec, Epi epi,
-                                                           const Ctl* __restrict__ ctl, double* partials) {
+                                                           Ctl* ctl, double* partials, Fin fin) {
     typedef typename Cx<T>::t C2;
     typedef ZTile<T, N, C> Z;
     const int b = blockIdx.y;
@@ -285,22 +337,40 @@ __global__ void __launch_bounds__(kFastThreads) k_zinv_fast(GridDims g, const ty
     extern __shared__ __align__(16) char smem_raw[];
     C2* tw = (C2*)smem_raw;
     C2* tile = tw + N;
-    C2* xch = tile + Z::LINES * Z::ROW;
-    double* red = (double*)align_up((char*)(xch + 4 * Z::LPW * Xch<Z::E, Z::TL>::size), 16);
-    char* extra = (char*)red + 32 * 32 * sizeof(double);
+    C2* raw = tile + Z::SLOTS * Z::ROW;  // [gi][c][k] half spectra as stored
+    double* red = (double*)align_up((char*)(raw + Z::G * C * (N / 2 + 1)), 16);
+    char* extra = (char*)red + 32 * 16 * sizeof(double);
+    const long long l0 = (long long)blockIdx.x * Z::G;
+    constexpr int Hz = N / 2 + 1;
+    const int Hzp = g.Hzp;
+    // asynchronous copies of the G x C half-spectrum rows (coalesced along kz)
+    for (int i = threadIdx.x; i < Z::G * C * Hz; i += kFastThreads) {
+        const int k = i % Hz, gc = i / Hz;
+        const int gi = gc / C, c = gc - gi * C;
+        const long long l = l0 + gi;
+        const bool okl = l < g.NL;
+        cp_async(raw + i, spec + (((long long)b * C + c) * g.NL + (okl ? l : 0)) * Hzp + k, (int)sizeof(C2),
+                 okl ? (int)sizeof(C2) : 0);
+    }
+    // epilogue loads do not depend on the transform: issue them meanwhile
+    typename Epi::Pre pre[Epi::kPrefetch ? Z::PER : 1];
+    if constexpr (Epi::kPrefetch) {
+#pragma unroll
+        for (int k = 0; k < Z::PER; ++k) {
+            const int i = threadIdx.x + k * kFastThreads;
+            const int gi = i / N, z = i - gi * N;
+            if (i < Z::TOT && l0 + gi < g.NL) pre[k] = epi.load(b, (l0 + gi) * N + z);
+        }
+    }
     for (int i = threadIdx.x; i < N; i += blockDim.x) tw[i] = twz[i];
     epi.load_smem(extra);
-    const long long l0 = (long long)blockIdx.x * Z::G;
-    const int Hz = g.Hz, Hzp = g.Hzp;
-    for (int i = threadIdx.x; i < Z::G * Z::NCL * Hz; i += blockDim.x) {
+    cp_async_wait_all();
+    __syncthreads();
+    for (int i = threadIdx.x; i < Z::G * Z::NCL * Hz; i += kFastThreads) {
         const int k = i % Hz, gl = i / Hz;
         const int gi = gl / Z::NCL, cl = gl - gi * Z::NCL;
-        const long long l = l0 + gi;
-        C2 a = mk<C2>(0, 0), bb = mk<C2>(0, 0);
-        if (l < g.NL) {
-            a = spec[(((long long)b * C + 2 * cl) * g.NL + l) * Hzp + k];
-            if (2 * cl + 1 < C) bb = spec[(((long long)b * C + 2 * cl + 1) * g.NL + l) * Hzp + k];
-        }
+        const C2 a = raw[(gi * C + 2 * cl) * Hz + k];
+        const C2 bb = (2 * cl + 1 < C) ? raw[(gi * C + 2 * cl + 1) * Hz + k] : mk<C2>(0, 0);
         C2* row = tile + gl * Z::ROW;
         if (k == 0 || 2 * k == N) {
             row[k] = mk<C2>(a.x, bb.x);
@@ -310,11 +380,14 @@ __global__ void __launch_bounds__(kFastThreads) k_zinv_fast(GridDims g, const ty
         }
     }
     __syncthreads();
-    z_tile_fft<C2, N, Z::E, Z::TL, Z::LINES, Z::ROW, false>(tile, xch, tw);
+    z_tile_fft<C2, N, Z::E, Z::TL, Z::SLOTS, Z::ROW, false>(tile, tw);
     __syncthreads();
     const T invV = (T)(1.0 / (double)g.V);
     double acc[Epi::NSUM > 0 ? Epi::NSUM : 1] = {};
-    for (int i = threadIdx.x; i < Z::G * N; i += blockDim.x) {
+#pragma unroll
+    for (int k = 0; k < Z::PER; ++k) {
+        const int i = threadIdx.x + k * kFastThreads;
+        if (i >= Z::TOT) break;
         const int gi = i / N, z = i - gi * N;
         const long long l = l0 + gi;
         if (l >= g.NL) continue;
@@ -325,10 +398,12 @@ __global__ void __launch_bounds__(kFastThreads) k_zinv_fast(GridDims g, const ty
             xc[2 * cl] = w.x * invV;
             if (2 * cl + 1 < C) xc[2 * cl + 1] = w.y * invV;
         }
-        epi.apply(b, l * N + z, xc, acc);
+        if constexpr (Epi::kPrefetch) epi.apply_pre(pre[k], b, l * N + z, xc, acc);
+        else epi.apply(b, l * N + z, xc, acc);
     }
     if constexpr (Epi::NSUM > 0) {
         block_reduce_store<Epi::NSUM>(acc, red, partials, b, gridDim.x, blockIdx.x);
+        fused_finalize(fin, ctl, partials, Epi::NSUM, b);
     }
 }
 

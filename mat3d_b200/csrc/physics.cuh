@@ -166,6 +166,10 @@ struct SpecEqVar {
 // ----------------------------------------------------------------------------
 // Prologues
 // ----------------------------------------------------------------------------
+// Every prologue/epilogue splits into load() -- the global reads of one voxel
+// -- and a compute step, so a pass can issue the loads of all its voxels
+// before the first compute and keep them in flight together.
+// ----------------------------------------------------------------------------
 // out = M[ph] x  (M: per phase CxC, row-major, double in global -> T in smem)
 template <typename T, int C, typename TX = T>
 struct ProMat {
@@ -176,24 +180,32 @@ struct ProMat {
     const double* mats;
     int nph;
     T* sm;
+    struct Pre {
+        int p;
+        T xv[C];
+    };
     __device__ __forceinline__ void load_smem(char* s) {
         sm = (T*)s;
         for (int i = threadIdx.x; i < nph * C * C; i += blockDim.x) sm[i] = (T)mats[i];
     }
-    __device__ __forceinline__ void eval(int b, long long v, T (&out)[C], double*) const {
-        const int p = phase[v];
-        const T* M = sm + p * C * C;
-        T xv[C];
+    __device__ __forceinline__ Pre load(int b, long long v) const {
+        Pre q;
+        q.p = phase[v];
 #pragma unroll
-        for (int c = 0; c < C; ++c) xv[c] = (T)x[((long long)b * C + c) * V + v];
+        for (int c = 0; c < C; ++c) q.xv[c] = (T)x[((long long)b * C + c) * V + v];
+        return q;
+    }
+    __device__ __forceinline__ void eval_pre(const Pre& q, int, long long, T (&out)[C]) const {
+        const T* M = sm + q.p * C * C;
 #pragma unroll
         for (int i = 0; i < C; ++i) {
             T s = 0;
 #pragma unroll
-            for (int j = 0; j < C; ++j) s += M[i * C + j] * xv[j];
+            for (int j = 0; j < C; ++j) s += M[i * C + j] * q.xv[j];
             out[i] = s;
         }
     }
+    __device__ __forceinline__ void eval(int b, long long v, T (&out)[C], double*) const { eval_pre(load(b, v), b, v, out); }
 };
 
 // FP64 defect pass of the refinement: x += delta (FP32 correction of the
@@ -208,30 +220,41 @@ struct ProRefine64 {
     const double* mats;
     int nph;
     double* sm;
+    struct Pre {
+        int p;
+        double xv[C];
+    };
     __device__ __forceinline__ void load_smem(char* s) {
         sm = (double*)s;
         for (int i = threadIdx.x; i < nph * C * C; i += blockDim.x) sm[i] = mats[i];
     }
-    __device__ __forceinline__ void eval(int b, long long v, double (&out)[C], double*) const {
-        const int p = phase[v];
-        const double* M = sm + p * C * C;
-        double xv[C];
+    __device__ __forceinline__ Pre load(int b, long long v) const {
+        Pre q;
+        q.p = phase[v];
 #pragma unroll
         for (int c = 0; c < C; ++c) {
             const long long idx = ((long long)b * C + c) * V + v;
-            xv[c] = x[idx];
-            if (delta) {
-                xv[c] += (double)delta[idx];
-                x[idx] = xv[c];
-            }
+            q.xv[c] = x[idx];
+            if (delta) q.xv[c] += (double)delta[idx];
+        }
+        return q;
+    }
+    __device__ __forceinline__ void eval_pre(const Pre& q, int b, long long v, double (&out)[C]) const {
+        const double* M = sm + q.p * C * C;
+        if (delta) {
+#pragma unroll
+            for (int c = 0; c < C; ++c) x[((long long)b * C + c) * V + v] = q.xv[c];
         }
 #pragma unroll
         for (int i = 0; i < C; ++i) {
             double s = 0;
 #pragma unroll
-            for (int j = 0; j < C; ++j) s += M[i * C + j] * xv[j];
+            for (int j = 0; j < C; ++j) s += M[i * C + j] * q.xv[j];
             out[i] = s;
         }
+    }
+    __device__ __forceinline__ void eval(int b, long long v, double (&out)[C], double*) const {
+        eval_pre(load(b, v), b, v, out);
     }
 };
 
@@ -242,6 +265,7 @@ struct ProRefine64 {
 template <typename T, int C>
 struct EpiEM {
     static constexpr int NSUM = 2;
+    static constexpr bool kPrefetch = true;
     const uint8_t* phase;
     T* x;
     const float* r;  // defect forcing of the correction solve, may be null
@@ -250,24 +274,33 @@ struct EpiEM {
     const double* osum;   // [nph][C]: column sums of the "other field" matrix
     int nph;
     T* sm;
+    struct Pre {
+        int p;
+        T xv[C];
+        T rv[C];
+    };
     __device__ __forceinline__ void load_smem(char* s) {
         sm = (T*)s;
         for (int i = threadIdx.x; i < nph * C * C; i += blockDim.x) sm[i] = (T)amats[i];
         for (int i = threadIdx.x; i < nph * C; i += blockDim.x) sm[nph * C * C + i] = (T)osum[i];
     }
-    __device__ __forceinline__ void apply(int b, long long v, T (&xc)[C], double* acc) const {
-        const int p = phase[v];
-        const T* Am = sm + p * C * C;
-        const T* os = sm + nph * C * C + p * C;
-        T xv[C], d[C];
+    __device__ __forceinline__ Pre load(int b, long long v) const {
+        Pre q;
+        q.p = phase[v];
 #pragma unroll
         for (int c = 0; c < C; ++c) {
             const long long idx = ((long long)b * C + c) * V + v;
-            xv[c] = x[idx];
-            T xcv = xc[c];
-            if (r) xcv += (T)r[idx];
-            d[c] = xcv - xv[c];
+            q.xv[c] = x[idx];
+            q.rv[c] = r ? (T)r[idx] : (T)0;
         }
+        return q;
+    }
+    __device__ __forceinline__ void apply_pre(const Pre& q, int b, long long v, T (&xc)[C], double* acc) const {
+        const T* Am = sm + q.p * C * C;
+        const T* os = sm + nph * C * C + q.p * C;
+        T d[C], xn[C];
+#pragma unroll
+        for (int c = 0; c < C; ++c) d[c] = (xc[c] + q.rv[c]) - q.xv[c];
         double rs = 0, ot = 0;
 #pragma unroll
         for (int i = 0; i < C; ++i) {
@@ -276,14 +309,16 @@ struct EpiEM {
             T s = 0;
 #pragma unroll
             for (int j = 0; j < C; ++j) s += Am[i * C + j] * d[j];
-            const T xn = xv[i] + s;
-            x[((long long)b * C + i) * V + v] = xn;
-            xv[i] = xn;
+            xn[i] = q.xv[i] + s;
+            x[((long long)b * C + i) * V + v] = xn[i];
         }
 #pragma unroll
-        for (int c = 0; c < C; ++c) ot += (double)os[c] * (double)xv[c];
+        for (int c = 0; c < C; ++c) ot += (double)os[c] * (double)xn[c];
         acc[0] += rs;
         acc[1] += ot;
+    }
+    __device__ __forceinline__ void apply(int b, long long v, T (&xc)[C], double* acc) const {
+        apply_pre(load(b, v), b, v, xc, acc);
     }
 };
 
@@ -292,6 +327,7 @@ struct EpiEM {
 template <int C>
 struct EpiDefect {
     static constexpr int NSUM = 2;
+    static constexpr bool kPrefetch = true;
     const uint8_t* phase;
     const double* x;
     float* r;
@@ -299,25 +335,36 @@ struct EpiDefect {
     const double* osum;
     int nph;
     double* sm;
+    struct Pre {
+        int p;
+        double xv[C];
+    };
     __device__ __forceinline__ void load_smem(char* s) {
         sm = (double*)s;
         for (int i = threadIdx.x; i < nph * C; i += blockDim.x) sm[i] = osum[i];
     }
-    __device__ __forceinline__ void apply(int b, long long v, double (&xc)[C], double* acc) const {
-        const int p = phase[v];
+    __device__ __forceinline__ Pre load(int b, long long v) const {
+        Pre q;
+        q.p = phase[v];
+#pragma unroll
+        for (int c = 0; c < C; ++c) q.xv[c] = x[((long long)b * C + c) * V + v];
+        return q;
+    }
+    __device__ __forceinline__ void apply_pre(const Pre& q, int b, long long v, double (&xc)[C], double* acc) const {
         double rs = 0, ot = 0;
 #pragma unroll
         for (int c = 0; c < C; ++c) {
-            const long long idx = ((long long)b * C + c) * V + v;
-            const double xv = x[idx];
-            const double d = xc[c] - xv;
-            r[idx] = (float)d;
+            const double d = xc[c] - q.xv[c];
+            r[((long long)b * C + c) * V + v] = (float)d;
             const double w = (C == 6 && c >= 3) ? 2.0 : 1.0;
             rs += w * d * d;
-            ot += sm[p * C + c] * xv;
+            ot += sm[q.p * C + c] * q.xv[c];
         }
         acc[0] += rs;
         acc[1] += ot;
+    }
+    __device__ __forceinline__ void apply(int b, long long v, double (&xc)[C], double* acc) const {
+        apply_pre(load(b, v), b, v, xc, acc);
     }
 };
 
@@ -332,17 +379,15 @@ enum Policy {
     POL_REFINE_INNER = 4, // FP32 correction sweep
 };
 
-__global__ void k_finalize(Ctl* ctl, const double* __restrict__ partials, int NS, int nblk, int policy, double V,
-                           const Ctl* outer) {
-    const int b = blockIdx.x;
-    Ctl& c = ctl[b];
-    if (c.done) return;
-    __shared__ double red[256];
-    __shared__ double tot[8];
+// tot[s] = sum over the nblk block partials of sum s, in a fixed order (every
+// thread strides the same blocks, then a fixed tree) -> bit-reproducible.
+// Called by all threads of a block of at most 256 threads (power of two).
+__device__ __forceinline__ void sum_partials(const double* partials, int NS, int nblk, int b, double* red,
+                                             double* tot) {
     for (int s = 0; s < NS; ++s) {
         double t = 0;
         const double* p = partials + ((long long)b * NS + s) * nblk;
-        for (int i = threadIdx.x; i < nblk; i += blockDim.x) t += p[i];
+        for (int i = threadIdx.x; i < nblk; i += blockDim.x) t += __ldcg(p + i);
         red[threadIdx.x] = t;
         __syncthreads();
         for (int o = blockDim.x / 2; o > 0; o >>= 1) {
@@ -352,7 +397,36 @@ __global__ void k_finalize(Ctl* ctl, const double* __restrict__ partials, int NS
         if (threadIdx.x == 0) tot[s] = red[0];
         __syncthreads();
     }
-    if (threadIdx.x != 0) return;
+}
+
+__device__ __forceinline__ void policy_linear(Ctl& c, const double* tot, int policy, double V, const Ctl* outer,
+                                              int b);
+
+__global__ void k_finalize(Ctl* ctl, const double* __restrict__ partials, int NS, int nblk, int policy, double V,
+                           const Ctl* outer) {
+    const int b = blockIdx.x;
+    if (ctl[b].done) return;
+    __shared__ double red[256];
+    __shared__ double tot[16];
+    sum_partials(partials, NS, nblk, b, red, tot);
+    if (threadIdx.x == 0) policy_linear(ctl[b], tot, policy, V, outer, b);
+}
+
+// Finalize run by the last block of the pass that produced the partials.
+struct FinLinear {
+    int policy;
+    double V;
+    const Ctl* outer;
+    int* counter;
+    __device__ __forceinline__ void run(Ctl* ctl, const double* partials, int NS, int nblk, int b, double* red,
+                                        double* tot) const {
+        sum_partials(partials, NS, nblk, b, red, tot);
+        if (threadIdx.x == 0) policy_linear(ctl[b], tot, policy, V, outer, b);
+    }
+};
+
+__device__ __forceinline__ void policy_linear(Ctl& c, const double* tot, int policy, double V, const Ctl* outer,
+                                              int b) {
     switch (policy) {
         case POL_RESIDUAL: {
             c.iters += 1;

@@ -132,9 +132,16 @@ std::vector<typename Cx<T>::t> twiddles(int n) {
     return t;
 }
 
+// Let a kernel use all dynamic shared memory left next to its static arrays
+// (227 KB per block on sm_100 in total).
 template <class K>
 void allow_smem(K kernel) {
-    cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+    cudaFuncAttributes a;
+    if (cudaFuncGetAttributes(&a, kernel) == cudaSuccess) {
+        const int maxdyn = 227 * 1024 - (int)a.sharedSizeBytes;
+        cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, maxdyn);
+    }
+    (void)cudaGetLastError();  // an unsupported request must not surface at the next launch check
 }
 
 int even_up(int v) { return (v + 1) & ~1; }
@@ -241,7 +248,8 @@ struct m3d_solver {
     template <typename T, int CC, class Pro> void pass_zfwd(Pro pro, Ctl* ctl, typename Cx<T>::t* sp);
     template <typename T> void pass_y(int sign, int CC, Ctl* ctl, typename Cx<T>::t* sp);
     template <typename T, int CC, class Spec> int pass_x(Spec op, Ctl* ctl, typename Cx<T>::t* sp);
-    template <typename T, int CC, class Epi> int pass_zinv(Epi epi, Ctl* ctl, typename Cx<T>::t* sp);
+    template <typename T, int CC, class Epi, class Fin> int pass_zinv(Epi epi, Ctl* ctl, typename Cx<T>::t* sp, Fin fin);
+    int* d_counter = nullptr;  // completion counters of the fused finalize, one per batch entry
     bool use_fast = true;
     template <typename T, int CC>
     int run_linear(double tol_field, double tol_eq, int criterion, int max_iter);
@@ -268,6 +276,7 @@ void m3d_solver::free_all() {
     cudaFree(d_part); d_part = nullptr;
     cudaFree(d_ctl); d_ctl = nullptr;
     cudaFree(d_ctl_in); d_ctl_in = nullptr;
+    cudaFree(d_counter); d_counter = nullptr;
     if (h_ctl) cudaFreeHost(h_ctl);
     h_ctl = nullptr;
     cudaFree(d_mats); d_mats = nullptr;
@@ -310,6 +319,10 @@ int m3d_solver::alloc(int batch) {
     M3D_CUDA(cudaMalloc(&d_part, part_cap * sizeof(double)));
     M3D_CUDA(cudaMalloc(&d_ctl, batch * sizeof(Ctl)));
     M3D_CUDA(cudaMalloc(&d_ctl_in, batch * sizeof(Ctl)));
+    cudaFree(d_counter);
+    d_counter = nullptr;
+    M3D_CUDA(cudaMalloc(&d_counter, batch * sizeof(int)));
+    M3D_CUDA(cudaMemsetAsync(d_counter, 0, batch * sizeof(int), stream));
     M3D_CUDA(cudaMemsetAsync(d_ctl, 0, batch * sizeof(Ctl), stream));
     M3D_CUDA(cudaMemsetAsync(d_ctl_in, 0, batch * sizeof(Ctl), stream));
     M3D_CUDA(cudaMallocHost(&h_ctl, batch * sizeof(Ctl)));
@@ -475,7 +488,7 @@ int m3d_solver::pass_x(Spec op, Ctl* ctl, typename Cx<T>::t* sp) {
         nblk = Ny * ntz;
         static bool init = false;
         if (!init) { allow_smem(k_xturn_fast<T, NN, CC, Spec>); init = true; }
-        k_xturn_fast<T, NN, CC, Spec><<<dim3(nblk, B), WPC * 32, xturn_fast_smem<T, NN, CC>(), stream>>>(
+        k_xturn_fast<T, NN, CC, Spec><<<dim3(nblk, B), WPC * 32, xturn_fast_smem<T, NN, CC, Spec::NSUM>(), stream>>>(
             g, tw<T>(0), sp, op, ctl, d_part);
     });
     if (!done) {
@@ -491,8 +504,8 @@ int m3d_solver::pass_x(Spec op, Ctl* ctl, typename Cx<T>::t* sp) {
     return nblk;
 }
 
-template <typename T, int CC, class Epi>
-int m3d_solver::pass_zinv(Epi epi, Ctl* ctl, typename Cx<T>::t* sp) {
+template <typename T, int CC, class Epi, class Fin>
+int m3d_solver::pass_zinv(Epi epi, Ctl* ctl, typename Cx<T>::t* sp, Fin fin) {
     typedef typename Cx<T>::t C2;
     const size_t extra = op_smem<T, CC>();
     int nblk = 0;
@@ -501,22 +514,24 @@ int m3d_solver::pass_zinv(Epi epi, Ctl* ctl, typename Cx<T>::t* sp) {
         typedef ZTile<T, NN, CC> Z;
         nblk = (int)((g.NL + Z::G - 1) / Z::G);
         static bool init = false;
-        if (!init) { allow_smem(k_zinv_fast<T, NN, CC, Epi>); init = true; }
-        k_zinv_fast<T, NN, CC, Epi><<<dim3(nblk, B), kFastThreads, z_fast_smem<T, NN, CC>(extra), stream>>>(
-            g, tw<T>(2), sp, epi, ctl, d_part);
+        if (!init) { allow_smem(k_zinv_fast<T, NN, CC, Epi, Fin>); init = true; }
+        k_zinv_fast<T, NN, CC, Epi, Fin><<<dim3(nblk, B), kFastThreads, zinv_fast_smem<T, NN, CC>(extra), stream>>>(
+            g, tw<T>(2), sp, epi, ctl, d_part, fin);
     });
     if (!done) {
         const int Gl = G<T>();
         nblk = (int)((g.NL + Gl - 1) / Gl);
         const size_t zsmem = (size_t)Nz * sizeof(C2) + 2 * (size_t)(Gl / 2) * CC * Nz * sizeof(C2) + 16 + 32 * 32 * 8 + extra;
         static bool init = false;
-        if (!init) { allow_smem(k_zinv<T, CC, Epi>); init = true; }
-        k_zinv<T, CC, Epi><<<dim3(nblk, B), 256, zsmem, stream>>>(g, pz, tw<T>(2), sp, epi, ctl, Gl, d_part);
+        if (!init) { allow_smem(k_zinv<T, CC, Epi, Fin>); init = true; }
+        k_zinv<T, CC, Epi, Fin><<<dim3(nblk, B), 256, zsmem, stream>>>(g, pz, tw<T>(2), sp, epi, ctl, Gl, d_part, fin);
     }
     st.kernel_launches += 1;
     return nblk;
 }
 
+// One sweep; the finalize (sum of partials + stop rule) runs in the last
+// block of the z-inverse pass.
 template <typename T, int CC, class Pro, class Spec, class Epi>
 int m3d_solver::launch_sweep(Pro pro, Spec spec, Epi epi, Ctl* ctl, typename Cx<T>::t* sp, int policy,
                              const Ctl* outer) {
@@ -524,9 +539,7 @@ int m3d_solver::launch_sweep(Pro pro, Spec spec, Epi epi, Ctl* ctl, typename Cx<
     pass_y<T>(-1, CC, ctl, sp);
     pass_x<T, CC>(spec, ctl, sp);
     pass_y<T>(+1, CC, ctl, sp);
-    const int zblk = pass_zinv<T, CC>(epi, ctl, sp);
-    k_finalize<<<B, 256, 0, stream>>>(ctl, d_part, Epi::NSUM, zblk, policy, (double)g.V, outer);
-    st.kernel_launches += 1;
+    pass_zinv<T, CC>(epi, ctl, sp, FinLinear{policy, (double)g.V, outer, d_counter});
     M3D_CUDA(cudaGetLastError());
     return M3D_OK;
 }

@@ -212,9 +212,7 @@ int m3d_solver::run_inelastic(double tol_field, double tol_eq, int nInc, int cri
                     st.kernel_launches += 1;
                 }
                 pass_y<T>(+1, 6, d_ctl, sp);
-                const int zblk = pass_zinv<T, 6>(epi, d_ctl, sp);
-                k_finalize_j2<<<B, 256, 0, stream>>>(d_ctl, d_part, 13, zblk, POLJ2_SWEEP, (double)V, in.d_S0);
-                st.kernel_launches += 1;
+                pass_zinv<T, 6>(epi, d_ctl, sp, FinJ2{POLJ2_SWEEP, (double)V, in.d_S0, d_counter});
             }
             M3D_CUDA(cudaGetLastError());
             prof_mark(chunk);
