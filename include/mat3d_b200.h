@@ -142,6 +142,27 @@ typedef struct {
 int m3d_set_profiling(m3d_solver* h, int enable);  /* enabling also resets the counters */
 int m3d_get_profile(const m3d_solver* h, m3d_profile* out);
 
+/* Thermal solve for callers that cannot allocate device memory (they run
+   inside another framework's memory pool, or on a serving path that must not
+   block on the allocator or fail with out-of-memory half-way).  No
+   counterpart in the reference.  Steady conduction on an Nx x Ny x Nz grid,
+   FP64, rms-residual stop rule |x_c - x| / |E| < tol, scheme chosen as by
+   m3d_set_material_thermal; E is the macroscopic temperature gradient
+   (gradient-based scheme) or heat flux (flux-based), as for m3d_set_load.
+   The caller passes device pointers: d_phase (V bytes, 0 = inclusion with
+   conductivity ki, nonzero = matrix with km) and d_grad (3*V doubles, output,
+   component-major: d_grad[c*V + v]).  All working memory is a fixed 32 MiB
+   device array inside the library (held by every GPU that loads it until
+   exit); grids that need more (beyond about 96^3) are rejected with
+   M3D_ERR_ARG.  The first call on a device looks up that array's address, so
+   make it before any stream capture.  Calls share the array: calls that
+   overlap on the GPU race, serialise them.  stream: cudaStream_t (NULL = the
+   legacy default stream).  Calls no cudaMalloc, cudaFree or allocating
+   library routine. */
+int m3d_thermal_solve_noalloc(int Nx, int Ny, int Nz, double km, double ki, const uint8_t* d_phase,
+                              const double* E, double tol, int max_iter, double* d_grad, int* iters_out,
+                              double* residual_out, void* stream);
+
 /* The CUDA stream (cudaStream_t) all work of the handle is ordered on.
    m3d_set_stream replaces it with a caller-owned stream (NULL: the handle's own). */
 void* m3d_get_stream(const m3d_solver* h);

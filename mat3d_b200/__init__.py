@@ -73,7 +73,7 @@ EXPORTS = [
     "m3d_create", "m3d_destroy", "m3d_set_material_mech", "m3d_set_material_thermal", "m3d_set_load", "m3d_run",
     "m3d_homogenize", "m3d_get_field", "m3d_get_means", "m3d_get_stats", "m3d_get_increments",
     "m3d_status_string", "m3d_last_error", "m3d_abi_version", "m3d_get_stream", "m3d_set_stream",
-    "m3d_set_profiling", "m3d_get_profile",
+    "m3d_set_profiling", "m3d_get_profile", "m3d_thermal_solve_noalloc",
 ]
 
 
@@ -108,6 +108,8 @@ def load_library(path: str | None = None):
     L.m3d_get_stream.restype = vp
     L.m3d_get_stream.argtypes = [vp]
     L.m3d_set_stream.argtypes = [vp, vp]
+    L.m3d_thermal_solve_noalloc.argtypes = [i, i, i, d, d, vp, vp, d, i, vp, ctypes.POINTER(ctypes.c_int),
+                                            ctypes.POINTER(ctypes.c_double), vp]
     L.m3d_set_profiling.argtypes = [vp, i]
     L.m3d_get_profile.argtypes = [vp, ctypes.POINTER(Profile)]
     if path is None:

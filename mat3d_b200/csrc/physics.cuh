@@ -402,8 +402,8 @@ __device__ __forceinline__ void sum_partials(const double* partials, int NS, int
 __device__ __forceinline__ void policy_linear(Ctl& c, const double* tot, int policy, double V, const Ctl* outer,
                                               int b);
 
-__global__ void k_finalize(Ctl* ctl, const double* __restrict__ partials, int NS, int nblk, int policy, double V,
-                           const Ctl* outer) {
+static __global__ void k_finalize(Ctl* ctl, const double* __restrict__ partials, int NS, int nblk, int policy, double V,
+                                  const Ctl* outer) {
     const int b = blockIdx.x;
     if (ctl[b].done) return;
     __shared__ double red[256];

@@ -761,6 +761,9 @@ static int export_field(m3d_solver* h, const void* x, const double* mats, int b,
 
 #include "solver_inelastic.inl"
 
+// Lets the allocation-free entry point (noalloc.cu) report through m3d_last_error().
+void m3d_internal_set_error(const std::string& msg) { g_last_error = msg; }
+
 // ============================================================================
 // C ABI
 // ============================================================================
