@@ -81,20 +81,25 @@ constexpr bool fast_size(int n) {
 // exchange buffer of one line: element (k1, t) at k1*(T+1) + t
 template <int E, int T> struct Xch { static constexpr int size = E * (T + 1) + 1; };
 
+// Exchange element (k1, t) lives at k1*(T+1) + (t ^ sw); `sw` (0 or 1) is a
+// per-line bank swizzle chosen with the row padding (BankCfg in
+// passes_fast.cuh) so that the natural, spectral and both exchange access
+// patterns of a warp are conflict-free.
 template <typename C2, int E, int T>
-__device__ __forceinline__ void line_fwd(C2 (&v)[E], int t, C2* xch, const C2* tw) {
+__device__ __forceinline__ void line_fwd(C2 (&v)[E], int t, C2* xch, const C2* tw, int sw = 0) {
     constexpr int N = E * T, Q = E / T;
     dft_reg<C2, E, N>(v, tw, -1);
 #pragma unroll
     for (int k1 = 1; k1 < E; ++k1) v[k1] = cmul(v[k1], twid(tw, t * k1, -1));
+    const int ts = t ^ sw;
 #pragma unroll
-    for (int k1 = 0; k1 < E; ++k1) xch[k1 * (T + 1) + t] = v[k1];
+    for (int k1 = 0; k1 < E; ++k1) xch[k1 * (T + 1) + ts] = v[k1];
     __syncwarp();
 #pragma unroll
     for (int q = 0; q < Q; ++q) {
         C2 u[T];
 #pragma unroll
-        for (int t2 = 0; t2 < T; ++t2) u[t2] = xch[(t * Q + q) * (T + 1) + t2];
+        for (int t2 = 0; t2 < T; ++t2) u[t2] = xch[(t * Q + q) * (T + 1) + (t2 ^ sw)];
         dft_reg<C2, T, N>(u, tw, -1);
 #pragma unroll
         for (int k2 = 0; k2 < T; ++k2) v[q * T + k2] = u[k2];
@@ -103,7 +108,7 @@ __device__ __forceinline__ void line_fwd(C2 (&v)[E], int t, C2* xch, const C2* t
 }
 
 template <typename C2, int E, int T>
-__device__ __forceinline__ void line_inv(C2 (&v)[E], int t, C2* xch, const C2* tw) {
+__device__ __forceinline__ void line_inv(C2 (&v)[E], int t, C2* xch, const C2* tw, int sw = 0) {
     constexpr int N = E * T, Q = E / T;
 #pragma unroll
     for (int q = 0; q < Q; ++q) {
@@ -115,12 +120,13 @@ __device__ __forceinline__ void line_inv(C2 (&v)[E], int t, C2* xch, const C2* t
 #pragma unroll
         for (int t2 = 0; t2 < T; ++t2) {
             const C2 w = (t2 == 0) ? u[t2] : cmul(u[t2], twid(tw, t2 * k1, +1));
-            xch[k1 * (T + 1) + t2] = w;
+            xch[k1 * (T + 1) + (t2 ^ sw)] = w;
         }
     }
     __syncwarp();
+    const int ts = t ^ sw;
 #pragma unroll
-    for (int k1 = 0; k1 < E; ++k1) v[k1] = xch[k1 * (T + 1) + t];
+    for (int k1 = 0; k1 < E; ++k1) v[k1] = xch[k1 * (T + 1) + ts];
     __syncwarp();
     dft_reg<C2, E, N>(v, tw, +1);
 }

@@ -25,15 +25,41 @@ namespace m3d {
 
 constexpr int kFastThreads = 128;
 
-// Row length (complex elements) of a line that is also its exchange buffer:
-// at least max(N, E*(T+1)), padded so that consecutive rows start 16 banks
-// apart (FP32: rows of 8 mod 16 complex; FP64: 4 mod 8).
-template <typename T, int N>
+// Shared-memory bank layout of a line's row (which is also its exchange
+// buffer).  Rows hold at least max(N, E*(T+1)) complex elements, padded so
+// that row length == `tgt` modulo the number of complex elements per
+// wavefront slot cycle (16 for 8-byte FP32 complex, 8 for 16-byte FP64), and
+// lines with odd index XOR-swizzle bit 0 when `sw`.  The (tgt, sw) pairs are
+// the conflict-free choices for the four access patterns of a warp
+// (natural, spectral, exchange write, exchange read), found by enumerating
+// all paddings and both swizzles under half-warp (8-byte) / quarter-warp
+// (16-byte) servicing, separately for the column layout of the x/y passes
+// (lane = col + CPW*t) and the line layout of the z tiles (lane = t + T*line).
+constexpr int bank_tgt(bool fp32, int E, int T, bool col) {
+    if (fp32) {
+        if (col) return (E == 16 && T == 8) ? 4 : (E == 8 && T == 8) ? 4 : (E == 32) ? 3 : (T == 4) ? 2 : 8;
+        return (T == 4) ? 4 : 8;
+    }
+    if (col) return (T == 16) ? 4 : (T == 8) ? 2 : 1;
+    return (T == 4) ? 4 : 0;
+}
+constexpr int bank_sw(bool fp32, int E, int T, bool col) {
+    if (fp32) {
+        if (col) return (E == 16 && T == 8) || (E == 8 && T == 4) || (E == 24 && T == 4);
+        return (E == 16 && T == 8) || (E == 32) || (E == 8 && T == 4) || (E == 24 && T == 4);
+    }
+    if (col) return (E == 16 && T == 8);
+    return (E == 8 && T == 4) || (E == 24 && T == 4);
+}
+
+template <typename T, int N, bool COL>
 struct RowLen {
     static constexpr int E = LineSplit<T, N>::E, TL = LineSplit<T, N>::Tl;
+    static constexpr bool fp32 = sizeof(T) == 4;
     static constexpr int base = (N > E * (TL + 1)) ? N : E * (TL + 1);
-    static constexpr int mod = sizeof(T) == 4 ? 16 : 8, tgt = sizeof(T) == 4 ? 8 : 4;
+    static constexpr int mod = fp32 ? 16 : 8, tgt = bank_tgt(fp32, E, TL, COL);
     static constexpr int value = base + ((tgt - base % mod) + mod) % mod;
+    static constexpr int sw = bank_sw(fp32, E, TL, COL);
 };
 
 // ---------------------------------------------------------------------------
@@ -43,7 +69,8 @@ template <typename T, int N>
 constexpr size_t ypass_fast_smem() {
     typedef typename Cx<T>::t C2;
     constexpr int E = LineSplit<T, N>::E, TL = LineSplit<T, N>::Tl, CPW = 32 / TL;
-    return (size_t)N * sizeof(C2) + (size_t)4 * CPW * Xch<E, TL>::size * sizeof(C2);
+    (void)E;
+    return (size_t)N * sizeof(C2) + (size_t)4 * CPW * RowLen<T, N, true>::value * sizeof(C2);
 }
 
 template <typename T, int N, int SIGN>
@@ -52,7 +79,7 @@ __global__ void __launch_bounds__(kFastThreads) k_ypass_fast(GridDims g, const t
                                                             const Ctl* __restrict__ ctl) {
     typedef typename Cx<T>::t C2;
     constexpr int E = LineSplit<T, N>::E, TL = LineSplit<T, N>::Tl, CPW = 32 / TL;
-    constexpr int XS = Xch<E, TL>::size;
+    constexpr int XS = RowLen<T, N, true>::value;
     const int cb = blockIdx.y;
     if (ctl[cb / C].done) return;
     extern __shared__ __align__(16) char smem_raw[];
@@ -69,11 +96,12 @@ __global__ void __launch_bounds__(kFastThreads) k_ypass_fast(GridDims g, const t
     const bool ok = kz < g.Hzp;
     C2* base = spec + ((long long)cb * g.NL + (long long)x * g.Ny) * g.Hzp + (ok ? kz : 0);
     C2* xl = xch + (warp * CPW + col) * XS;
+    const int sw = RowLen<T, N, true>::sw ? (col & 1) : 0;
     C2 v[E];
     if constexpr (SIGN < 0) {
 #pragma unroll
         for (int j = 0; j < E; ++j) v[j] = ok ? base[(long long)(t + TL * j) * g.Hzp] : mk<C2>(0, 0);
-        line_fwd<C2, E, TL>(v, t, xl, tw);
+        line_fwd<C2, E, TL>(v, t, xl, tw, sw);
         if (ok) {
 #pragma unroll
             for (int r = 0; r < E; ++r) base[(long long)spec_mode<E, TL>(t, r) * g.Hzp] = v[r];
@@ -81,7 +109,7 @@ __global__ void __launch_bounds__(kFastThreads) k_ypass_fast(GridDims g, const t
     } else {
 #pragma unroll
         for (int r = 0; r < E; ++r) v[r] = ok ? base[(long long)spec_mode<E, TL>(t, r) * g.Hzp] : mk<C2>(0, 0);
-        line_inv<C2, E, TL>(v, t, xl, tw);
+        line_inv<C2, E, TL>(v, t, xl, tw, sw);
         if (ok) {
 #pragma unroll
             for (int j = 0; j < E; ++j) base[(long long)(t + TL * j) * g.Hzp] = v[j];
@@ -110,7 +138,7 @@ __device__ __forceinline__ void cp_async_wait_all() {
 template <typename T, int N, int C>
 struct XWarps {
     static constexpr size_t per_warp =
-        (size_t)C * (32 / LineSplit<T, N>::Tl) * RowLen<T, N>::value * sizeof(typename Cx<T>::t);
+        (size_t)C * (32 / LineSplit<T, N>::Tl) * RowLen<T, N, true>::value * sizeof(typename Cx<T>::t);
     static constexpr int value = (4 * per_warp <= 24 * 1024) ? 4 : ((2 * per_warp <= 24 * 1024) ? 2 : 1);
 };
 
@@ -128,7 +156,7 @@ __global__ void __launch_bounds__(kFastThreads) k_xturn_fast(GridDims g, const t
     typedef typename Cx<T>::t C2;
     constexpr int E = LineSplit<T, N>::E, TL = LineSplit<T, N>::Tl, CPW = 32 / TL;
     constexpr int WPC = XWarps<T, N, C>::value;
-    constexpr int RL = RowLen<T, N>::value;
+    constexpr int RL = RowLen<T, N, true>::value;
     const int b = blockIdx.y;
     if (ctl[b].done) return;
     extern __shared__ __align__(16) char smem_raw[];
@@ -146,14 +174,15 @@ __global__ void __launch_bounds__(kFastThreads) k_xturn_fast(GridDims g, const t
     const long long xstride = (long long)g.Ny * g.Hzp;  // x stride
     const C2* base = spec + ((long long)b * C * g.NL + y) * g.Hzp + (ok ? kz : 0);
     C2* wst = stage + warp * C * CPW * RL;
+    const int sw = RowLen<T, N, true>::sw ? (col & 1) : 0;  // bank swizzle of this column's rows
     // issue every load of the warp's columns (all components) at once
 #pragma unroll 1
     for (int c = 0; c < C; ++c) {
         C2* row = wst + (c * CPW + col) * RL;
 #pragma unroll
         for (int j = 0; j < E; ++j)
-            cp_async(row + t + TL * j, base + c * cstride + (long long)(t + TL * j) * xstride, (int)sizeof(C2),
-                     ok ? (int)sizeof(C2) : 0);
+            cp_async(row + ((t + TL * j) ^ sw), base + c * cstride + (long long)(t + TL * j) * xstride,
+                     (int)sizeof(C2), ok ? (int)sizeof(C2) : 0);
     }
     for (int i = threadIdx.x; i < N; i += blockDim.x) tw[i] = twx[i];
     cp_async_wait_all();
@@ -163,11 +192,11 @@ __global__ void __launch_bounds__(kFastThreads) k_xturn_fast(GridDims g, const t
         C2* row = wst + (c * CPW + col) * RL;
         C2 v[E];
 #pragma unroll
-        for (int j = 0; j < E; ++j) v[j] = row[t + TL * j];
+        for (int j = 0; j < E; ++j) v[j] = row[(t + TL * j) ^ sw];
         __syncwarp();
-        line_fwd<C2, E, TL>(v, t, row, tw);
+        line_fwd<C2, E, TL>(v, t, row, tw, sw);
 #pragma unroll
-        for (int r = 0; r < E; ++r) row[spec_mode<E, TL>(t, r)] = v[r];
+        for (int r = 0; r < E; ++r) row[spec_mode<E, TL>(t, r) ^ sw] = v[r];
     }
     double acc[Spec::NSUM > 0 ? Spec::NSUM : 1] = {};
     const bool live = ok && kz < g.Hz;
@@ -176,11 +205,11 @@ __global__ void __launch_bounds__(kFastThreads) k_xturn_fast(GridDims g, const t
         const int mode = spec_mode<E, TL>(t, r);
         C2 m[C];
 #pragma unroll
-        for (int c = 0; c < C; ++c) m[c] = wst[(c * CPW + col) * RL + mode];
+        for (int c = 0; c < C; ++c) m[c] = wst[(c * CPW + col) * RL + (mode ^ sw)];
         if (live) op.apply(b, mode, y, kz, m, acc, ctl);
         if constexpr (Spec::kInverse) {
 #pragma unroll
-            for (int c = 0; c < C; ++c) wst[(c * CPW + col) * RL + mode] = m[c];
+            for (int c = 0; c < C; ++c) wst[(c * CPW + col) * RL + (mode ^ sw)] = m[c];
         }
     }
     if constexpr (Spec::NSUM > 0) {
@@ -193,9 +222,9 @@ __global__ void __launch_bounds__(kFastThreads) k_xturn_fast(GridDims g, const t
             C2* row = wst + (c * CPW + col) * RL;
             C2 v[E];
 #pragma unroll
-            for (int r = 0; r < E; ++r) v[r] = row[spec_mode<E, TL>(t, r)];
+            for (int r = 0; r < E; ++r) v[r] = row[spec_mode<E, TL>(t, r) ^ sw];
             __syncwarp();
-            line_inv<C2, E, TL>(v, t, row, tw);
+            line_inv<C2, E, TL>(v, t, row, tw, sw);
             if (ok) {
 #pragma unroll
                 for (int j = 0; j < E; ++j) out[c * cstride + (long long)(t + TL * j) * xstride] = v[j];
@@ -216,7 +245,8 @@ struct ZTile {
     static constexpr int G = (4 * LPW) / NCL > 0 ? (4 * LPW) / NCL : 1;  // voxel lines per CTA
     static constexpr int LINES = G * NCL;
     static constexpr int SLOTS = ((LINES + 4 * LPW - 1) / (4 * LPW)) * 4 * LPW;  // rows incl. idle-lane rows
-    static constexpr int ROW = RowLen<T, N>::value;
+    static constexpr int ROW = RowLen<T, N, false>::value;
+    static constexpr int SW = RowLen<T, N, false>::sw;
     static constexpr int TOT = G * N;  // voxels per CTA
     static constexpr int PER = (TOT + kFastThreads - 1) / kFastThreads;
 };
@@ -236,7 +266,7 @@ constexpr size_t zinv_fast_smem(size_t extra) {
 // transform the tile's complex lines in place (FWD: natural order in,
 // natural-order spectrum out; !FWD: the inverse), each line's row doubling as
 // its exchange buffer
-template <typename C2, int N, int E, int TL, int SLOTS, int ROW, bool FWD>
+template <typename C2, int N, int E, int TL, int SLOTS, int ROW, int SW, bool FWD>
 __device__ __forceinline__ void z_tile_fft(C2* tile, const C2* tw) {
     constexpr int LPW = 32 / TL;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -245,21 +275,22 @@ __device__ __forceinline__ void z_tile_fft(C2* tile, const C2* tw) {
 #pragma unroll 1
     for (int l0 = warp * LPW; l0 < SLOTS; l0 += NW * LPW) {
         C2* row = tile + (l0 + lw) * ROW;
+        const int sw = ((l0 + lw) & 1) * SW;  // odd tile rows are swizzled when SW
         C2 v[E];
         if constexpr (FWD) {
 #pragma unroll
-            for (int j = 0; j < E; ++j) v[j] = row[t + TL * j];
+            for (int j = 0; j < E; ++j) v[j] = row[(t + TL * j) ^ sw];
             __syncwarp();
-            line_fwd<C2, E, TL>(v, t, row, tw);
+            line_fwd<C2, E, TL>(v, t, row, tw, sw);
 #pragma unroll
-            for (int r = 0; r < E; ++r) row[spec_mode<E, TL>(t, r)] = v[r];
+            for (int r = 0; r < E; ++r) row[spec_mode<E, TL>(t, r) ^ sw] = v[r];
         } else {
 #pragma unroll
-            for (int r = 0; r < E; ++r) v[r] = row[spec_mode<E, TL>(t, r)];
+            for (int r = 0; r < E; ++r) v[r] = row[spec_mode<E, TL>(t, r) ^ sw];
             __syncwarp();
-            line_inv<C2, E, TL>(v, t, row, tw);
+            line_inv<C2, E, TL>(v, t, row, tw, sw);
 #pragma unroll
-            for (int j = 0; j < E; ++j) row[t + TL * j] = v[j];
+            for (int j = 0; j < E; ++j) row[(t + TL * j) ^ sw] = v[j];
         }
     }
 }
@@ -302,11 +333,13 @@ __global__ void __launch_bounds__(kFastThreads) k_zfwd_fast(GridDims g, const ty
             for (int c = 0; c < C; ++c) val[c] = (T)0;
         }
 #pragma unroll
-        for (int cl = 0; cl < Z::NCL; ++cl)
-            tile[(gi * Z::NCL + cl) * Z::ROW + z] = mk<C2>(val[2 * cl], (2 * cl + 1 < C) ? val[2 * cl + 1] : (T)0);
+        for (int cl = 0; cl < Z::NCL; ++cl) {
+            const int rw = gi * Z::NCL + cl;
+            tile[rw * Z::ROW + (z ^ ((rw & 1) * Z::SW))] = mk<C2>(val[2 * cl], (2 * cl + 1 < C) ? val[2 * cl + 1] : (T)0);
+        }
     }
     __syncthreads();
-    z_tile_fft<C2, N, Z::E, Z::TL, Z::SLOTS, Z::ROW, true>(tile, tw);
+    z_tile_fft<C2, N, Z::E, Z::TL, Z::SLOTS, Z::ROW, Z::SW, true>(tile, tw);
     __syncthreads();
     const int Hz = g.Hz, Hzp = g.Hzp;
     for (int i = threadIdx.x; i < Z::G * C * Hzp; i += blockDim.x) {
@@ -316,9 +349,10 @@ __global__ void __launch_bounds__(kFastThreads) k_zfwd_fast(GridDims g, const ty
         if (l >= g.NL) continue;
         C2 out = mk<C2>(0, 0);
         if (k < Hz) {
-            const C2* row = tile + (gi * Z::NCL + c / 2) * Z::ROW;
-            const C2 Zk = row[k];
-            const C2 Zm = row[k == 0 ? 0 : N - k];
+            const int rw = gi * Z::NCL + c / 2, sw = (rw & 1) * Z::SW;
+            const C2* row = tile + rw * Z::ROW;
+            const C2 Zk = row[k ^ sw];
+            const C2 Zm = row[(k == 0 ? 0 : N - k) ^ sw];
             out = (c & 1) ? mk<C2>((T)0.5 * (Zk.y + Zm.y), (T)-0.5 * (Zk.x - Zm.x))
                           : mk<C2>((T)0.5 * (Zk.x + Zm.x), (T)0.5 * (Zk.y - Zm.y));
         }
@@ -372,15 +406,16 @@ __global__ void __launch_bounds__(kFastThreads) k_zinv_fast(GridDims g, const ty
         const C2 a = raw[(gi * C + 2 * cl) * Hz + k];
         const C2 bb = (2 * cl + 1 < C) ? raw[(gi * C + 2 * cl + 1) * Hz + k] : mk<C2>(0, 0);
         C2* row = tile + gl * Z::ROW;
+        const int sw = (gl & 1) * Z::SW;
         if (k == 0 || 2 * k == N) {
-            row[k] = mk<C2>(a.x, bb.x);
+            row[k ^ sw] = mk<C2>(a.x, bb.x);
         } else {
-            row[k] = mk<C2>(a.x - bb.y, a.y + bb.x);
-            row[N - k] = mk<C2>(a.x + bb.y, bb.x - a.y);
+            row[k ^ sw] = mk<C2>(a.x - bb.y, a.y + bb.x);
+            row[(N - k) ^ sw] = mk<C2>(a.x + bb.y, bb.x - a.y);
         }
     }
     __syncthreads();
-    z_tile_fft<C2, N, Z::E, Z::TL, Z::SLOTS, Z::ROW, false>(tile, tw);
+    z_tile_fft<C2, N, Z::E, Z::TL, Z::SLOTS, Z::ROW, Z::SW, false>(tile, tw);
     __syncthreads();
     const T invV = (T)(1.0 / (double)g.V);
     double acc[Epi::NSUM > 0 ? Epi::NSUM : 1] = {};
@@ -394,7 +429,8 @@ __global__ void __launch_bounds__(kFastThreads) k_zinv_fast(GridDims g, const ty
         T xc[C];
 #pragma unroll
         for (int cl = 0; cl < Z::NCL; ++cl) {
-            const C2 w = tile[(gi * Z::NCL + cl) * Z::ROW + z];
+            const int rw = gi * Z::NCL + cl;
+            const C2 w = tile[rw * Z::ROW + (z ^ ((rw & 1) * Z::SW))];
             xc[2 * cl] = w.x * invV;
             if (2 * cl + 1 < C) xc[2 * cl + 1] = w.y * invV;
         }
