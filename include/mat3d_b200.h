@@ -25,6 +25,11 @@
  *   m3d_get_stream / m3d_set_stream
  *                              no counterpart (the reference is CPU-only); lets a
  *                              caller order the solve on its own CUDA stream
+ *   m3d_create_multi / m3d_set_material_mech_rve / m3d_set_material_thermal_rve
+ *                              no counterpart: the reference solves one RVE per
+ *                              object; these run many RVEs of one grid size in
+ *                              one batch, each with the reference's per-RVE
+ *                              material() setup (own scheme and reference medium)
  *
  * Layout conventions (as the reference): grid Nx x Ny x Nz, voxel index
  * v = z + Nz*(y + Ny*x); fields exchanged as AoS doubles out[v*c + comp]
@@ -97,6 +102,12 @@ typedef struct {
 /* Create a solver for an Nx x Ny x Nz grid.  `batch` independent solves
    (load cases) share the phase map and run together. */
 int m3d_create(int kind, int Nx, int Ny, int Nz, int behav, int precision, int batch, m3d_solver** out);
+/* A linear (elastic or thermal) solver whose batch holds nrve RVEs of one
+   grid size with nload load cases each: entry b = r * nload + l solves RVE r.
+   Each RVE takes its phase map and properties from the _rve setters below;
+   m3d_set_material_mech / _thermal set RVE 0.  m3d_homogenize then runs all
+   RVEs (6 or 3 load cases each) and writes nrve consecutive tensors. */
+int m3d_create_multi(int kind, int Nx, int Ny, int Nz, int precision, int nrve, int nload, m3d_solver** out);
 int m3d_destroy(m3d_solver* h);
 
 /* Phase properties, rows [E, nu, sigma_y, H, n, P, Y0] (row-major nph x 7), and
@@ -104,6 +115,9 @@ int m3d_destroy(m3d_solver* h);
 int m3d_set_material_mech(m3d_solver* h, const double* mat, int nph, const int32_t* phase, int scheme);
 /* km: matrix (id != 0), ki: inclusion (id == 0). */
 int m3d_set_material_thermal(m3d_solver* h, double km, double ki, const int32_t* phase, int scheme);
+/* The same for RVE r of a multi-RVE solver (0 <= r < nrve). */
+int m3d_set_material_mech_rve(m3d_solver* h, int r, const double* mat, int nph, const int32_t* phase, int scheme);
+int m3d_set_material_thermal_rve(m3d_solver* h, int r, double km, double ki, const int32_t* phase, int scheme);
 
 /* Load of batch entry b (b = -1: all entries): E has 6 (mech) or 3 (thermal)
    values; X0 (mech, may be NULL) is the stress direction of mixed control. */
@@ -116,7 +130,8 @@ int m3d_run(m3d_solver* h, double tol_field, double tol_eq, int nInc, int criter
 
 /* Effective tensor from 6 (mech) / 3 (thermal) load cases run as one batch
    (homogenization).  Ceff, Seff: 36 or 9 doubles, row-major.  ep_means,
-   sig_means (optional): the reference's epHomo / sigHomo matrices. */
+   sig_means (optional): the reference's epHomo / sigHomo matrices.  On a
+   multi-RVE solver every array holds nrve such blocks, RVE r at r*36 (r*9). */
 int m3d_homogenize(m3d_solver* h, double tol_field, double tol_eq, int criterion, int max_iter, double* Ceff,
                    double* Seff, double* ep_means, double* sig_means);
 

@@ -74,6 +74,7 @@ EXPORTS = [
     "m3d_homogenize", "m3d_get_field", "m3d_get_means", "m3d_get_stats", "m3d_get_increments",
     "m3d_status_string", "m3d_last_error", "m3d_abi_version", "m3d_get_stream", "m3d_set_stream",
     "m3d_set_profiling", "m3d_get_profile", "m3d_thermal_solve_noalloc",
+    "m3d_create_multi", "m3d_set_material_mech_rve", "m3d_set_material_thermal_rve",
 ]
 
 
@@ -110,6 +111,9 @@ def load_library(path: str | None = None):
     L.m3d_set_stream.argtypes = [vp, vp]
     L.m3d_thermal_solve_noalloc.argtypes = [i, i, i, d, d, vp, vp, d, i, vp, ctypes.POINTER(ctypes.c_int),
                                             ctypes.POINTER(ctypes.c_double), vp]
+    L.m3d_create_multi.argtypes = [i, i, i, i, i, i, i, ctypes.POINTER(vp)]
+    L.m3d_set_material_mech_rve.argtypes = [vp, i, vp, i, vp, i]
+    L.m3d_set_material_thermal_rve.argtypes = [vp, i, d, d, vp, i]
     L.m3d_set_profiling.argtypes = [vp, i]
     L.m3d_get_profile.argtypes = [vp, ctypes.POINTER(Profile)]
     if path is None:
@@ -130,15 +134,22 @@ def _check(L, rc, what, allow_not_converged=True):
 class Solver:
     """Thin handle over the C ABI (one CUDA stream, `batch` solves at once)."""
 
-    def __init__(self, kind, Nx, Ny, Nz, behav=ELASTIC, precision=FP64, batch=1):
+    def __init__(self, kind, Nx, Ny, Nz, behav=ELASTIC, precision=FP64, batch=1, nrve=None, nload=None):
         self.L = load_library()
-        self.kind, self.shape, self.batch = kind, (Nx, Ny, Nz), batch
+        self.kind, self.shape = kind, (Nx, Ny, Nz)
         self.V = Nx * Ny * Nz
         self.C = 6 if kind == KIND_MECH else 3
         self.behav = behav
         h = ctypes.c_void_p()
-        _check(self.L, self.L.m3d_create(kind, Nx, Ny, Nz, behav, _PRECISIONS[precision], batch, ctypes.byref(h)),
-               "m3d_create")
+        if nrve is None:
+            self.nrve, self.batch = 1, batch
+            rc = self.L.m3d_create(kind, Nx, Ny, Nz, behav, _PRECISIONS[precision], batch, ctypes.byref(h))
+        else:
+            # many RVEs of one grid size, nload load cases each (linear solves only)
+            nload = self.C if nload is None else nload
+            self.nrve, self.batch = nrve, nrve * nload
+            rc = self.L.m3d_create_multi(kind, Nx, Ny, Nz, _PRECISIONS[precision], nrve, nload, ctypes.byref(h))
+        _check(self.L, rc, "m3d_create")
         self.h = h
 
     def close(self):
@@ -152,14 +163,16 @@ class Solver:
         except Exception:
             pass
 
-    def set_material_mech(self, mat, phase, scheme=SCHEME_AUTO):
+    def set_material_mech(self, mat, phase, scheme=SCHEME_AUTO, rve=0):
         mat = np.ascontiguousarray(mat, np.float64)
         ph = np.ascontiguousarray(np.asarray(phase).ravel(), np.int32)
-        _check(self.L, self.L.m3d_set_material_mech(self.h, _ptr(mat), mat.shape[0], _ptr(ph), scheme), "material")
+        _check(self.L, self.L.m3d_set_material_mech_rve(self.h, rve, _ptr(mat), mat.shape[0], _ptr(ph), scheme),
+               "material")
 
-    def set_material_thermal(self, km, ki, phase, scheme=SCHEME_AUTO):
+    def set_material_thermal(self, km, ki, phase, scheme=SCHEME_AUTO, rve=0):
         ph = np.ascontiguousarray(np.asarray(phase).ravel(), np.int32)
-        _check(self.L, self.L.m3d_set_material_thermal(self.h, float(km), float(ki), _ptr(ph), scheme), "material")
+        _check(self.L, self.L.m3d_set_material_thermal_rve(self.h, rve, float(km), float(ki), _ptr(ph), scheme),
+               "material")
 
     def set_load(self, E, X0=None, b=-1):
         E = np.ascontiguousarray(E, np.float64)
@@ -170,10 +183,13 @@ class Solver:
         return _check(self.L, self.L.m3d_run(self.h, tol_field, tol_eq, nInc, criterion, max_iter), "run")
 
     def homogenize(self, tol_field, tol_eq=0.0, criterion=CRIT_RESIDUAL, max_iter=0):
+        """Effective tensors; on a multi-RVE solver each array is (nrve, C, C)."""
         C = self.C
-        Ce, Se, ep, sg = (np.zeros((C, C)) for _ in range(4))
+        Ce, Se, ep, sg = (np.zeros((self.nrve, C, C)) for _ in range(4))
         rc = _check(self.L, self.L.m3d_homogenize(self.h, tol_field, tol_eq, criterion, max_iter,
                                                   _ptr(Ce), _ptr(Se), _ptr(ep), _ptr(sg)), "homogenize")
+        if self.nrve == 1:
+            Ce, Se, ep, sg = Ce[0], Se[0], ep[0], sg[0]
         return Ce, Se, ep, sg, rc
 
     def field(self, which=FIELD_STRAIN, b=0):

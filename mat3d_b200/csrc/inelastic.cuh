@@ -120,7 +120,7 @@ struct EpiConstitutive {
     static constexpr int NSUM = 13;
     InelasticPtrs<T> p;
     PhaseMech* sm;
-    __device__ __forceinline__ void load_smem(char* s) {
+    __device__ __forceinline__ void load_smem(char* s, int = 0) {
         sm = (PhaseMech*)s;
         const double* src = (const double*)p.ph;
         double* dst = (double*)s;
@@ -176,7 +176,7 @@ struct ProStress {
     struct Pre {
         T s[6];
     };
-    __device__ __forceinline__ void load_smem(char*) {}
+    __device__ __forceinline__ void load_smem(char*, int = 0) {}
     __device__ __forceinline__ Pre load(int b, long long v) const {
         Pre q;
 #pragma unroll
@@ -198,6 +198,7 @@ struct SpecBasic {
     static constexpr int NSUM = 2;
     SpecGreen<T, 6> green;
     SpecEqVar<T, 6> eq;
+    __device__ __forceinline__ void prepare(const Ctl* ctl, int b) { green.prepare(ctl, b); }
     __device__ __forceinline__ void apply(int b, int x, int y, int kz, typename Cx<T>::t (&v)[6], double* acc,
                                           const Ctl* ctl) const {
         eq.apply(b, x, y, kz, v, acc, ctl);
@@ -216,7 +217,7 @@ struct EpiBasic {
     __device__ __forceinline__ void apply_pre(const Pre&, int b, long long v, T (&xc)[6], double* acc) const {
         c.apply(b, v, xc, acc);
     }
-    __device__ __forceinline__ void load_smem(char* s) { c.load_smem(s); }
+    __device__ __forceinline__ void load_smem(char* s, int b = 0) { c.load_smem(s, b); }
     __device__ __forceinline__ void apply(int b, long long v, T (&xc)[6], double* acc) const { c.apply(b, v, xc, acc); }
 };
 

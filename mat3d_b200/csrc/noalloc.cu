@@ -237,6 +237,9 @@ extern "C" int m3d_thermal_solve_noalloc(int Nx, int Ny, int Nz, double km, doub
         en += E[i] * E[i];
     }
     hc.enorm = en > 0 ? std::sqrt(en) : 1.0;
+    hc.gxw = Nx;
+    if (scheme == 1) { hc.gkind = GREEN_TGRAD; hc.gnyq = 1; hc.gp1 = 1.0 / k0; }
+    else { hc.gkind = GREEN_TFLUX; hc.gxw = Ny; hc.gp1 = k0; }
     NA_CUDA(cudaMemcpyAsync(mats, hm, sizeof(hm), cudaMemcpyHostToDevice, stream));
     NA_CUDA(cudaMemcpyAsync(tw, htw.data(), htw.size() * sizeof(double2), cudaMemcpyHostToDevice, stream));
     NA_CUDA(cudaMemcpyAsync(ctl, &hc, sizeof(hc), cudaMemcpyHostToDevice, stream));

@@ -32,7 +32,10 @@ struct Ctl {
     int status;     // 0 ok, 1 iteration cap, 2 non-finite residual
     int max_iter;
     int crit_residual;    // 1: residual stop rule, 0: the reference's rule
-    int pad_;
+    int gkind;            // Green operator of this entry's RVE (GreenKind)
+    int gnyq;             // 1: index <= N/2 is a positive frequency
+    int gxw;              // wrap length of the x index
+    double gp1, gp2;      // Green operator constants (see SpecGreen)
     double kzero[6];      // value of the k = 0 mode after the spectral op (already times V)
     double residual;      // last residual (criterion dependent)
     double tol_field, tol_eq;
@@ -124,7 +127,7 @@ __global__ void __launch_bounds__(256) k_zfwd(GridDims g, LinePlan pz, const typ
     double* red = (double*)extra;
     extra += 32 * 32 * sizeof(double);
     for (int i = threadIdx.x; i < Nz; i += blockDim.x) tw[i] = twz[i];
-    pro.load_smem(extra);
+    pro.load_smem(extra, b);
     __syncthreads();
 
     const long long l0 = (long long)blockIdx.x * G;
@@ -215,6 +218,7 @@ __global__ void __launch_bounds__(256) k_xturn(GridDims g, LinePlan px, const ty
     typedef typename Cx<T>::t C2;
     const int b = blockIdx.y;
     if (ctl[b].done) return;
+    op.prepare(ctl, b);
     extern __shared__ __align__(16) char smem_raw[];
     const int Nx = g.Nx, Ny = g.Ny, Hzp = g.Hzp;
     C2* tw = (C2*)smem_raw;
@@ -288,7 +292,7 @@ __global__ void __launch_bounds__(256) k_zinv(GridDims g, LinePlan pz, const typ
     double* red = (double*)extra;
     extra += 32 * 32 * sizeof(double);
     for (int i = threadIdx.x; i < Nz; i += blockDim.x) tw[i] = twz[i];
-    epi.load_smem(extra);
+    epi.load_smem(extra, b);
     const long long l0 = (long long)blockIdx.x * G;
     for (int i = threadIdx.x; i < nl * Hz; i += blockDim.x) {
         const int k = i % Hz, pc = i / Hz;

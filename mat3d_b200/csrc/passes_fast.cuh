@@ -159,6 +159,7 @@ __global__ void __launch_bounds__(kFastThreads) k_xturn_fast(GridDims g, const t
     constexpr int RL = RowLen<T, N, true>::value;
     const int b = blockIdx.y;
     if (ctl[b].done) return;
+    op.prepare(ctl, b);
     extern __shared__ __align__(16) char smem_raw[];
     C2* tw = (C2*)smem_raw;
     C2* stage = tw + N;  // [warp][c][col][RL]
@@ -317,7 +318,7 @@ __global__ void __launch_bounds__(kFastThreads) k_zfwd_fast(GridDims g, const ty
         if (i < Z::TOT && l0 + gi < g.NL) pre[k] = pro.load(b, (l0 + gi) * N + z);
     }
     for (int i = threadIdx.x; i < N; i += blockDim.x) tw[i] = twz[i];
-    pro.load_smem(extra);
+    pro.load_smem(extra, b);
     __syncthreads();
 #pragma unroll
     for (int k = 0; k < Z::PER; ++k) {
@@ -397,7 +398,7 @@ __global__ void __launch_bounds__(kFastThreads) k_zinv_fast(GridDims g, const ty
         }
     }
     for (int i = threadIdx.x; i < N; i += blockDim.x) tw[i] = twz[i];
-    epi.load_smem(extra);
+    epi.load_smem(extra, b);
     cp_async_wait_all();
     __syncthreads();
     for (int i = threadIdx.x; i < Z::G * Z::NCL * Hz; i += kFastThreads) {

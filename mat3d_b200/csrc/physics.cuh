@@ -80,6 +80,14 @@ struct SpecGreen {
     int xwrap;       // wrap length of the x index (Ny for the flux-based thermal quirk)
     int zero_k0;     // 1: k = 0 mode set to 0 (correction solves), else ctl.kzero
     T p1, p2;
+    // take the operator of batch entry b's RVE from its control block
+    __device__ __forceinline__ void prepare(const Ctl* ctl, int b) {
+        kind = ctl[b].gkind;
+        pos_nyq = ctl[b].gnyq;
+        xwrap = ctl[b].gxw;
+        p1 = (T)ctl[b].gp1;
+        p2 = (T)ctl[b].gp2;
+    }
     __device__ __forceinline__ void apply(int b, int x, int y, int kz, typename Cx<T>::t (&v)[C], double*,
                                           const Ctl* ctl) const {
         typedef typename Cx<T>::t C2;
@@ -132,6 +140,7 @@ struct SpecEqVar {
     static constexpr bool kInverse = false;
     static constexpr int NSUM = 2;
     GridDims g;
+    __device__ __forceinline__ void prepare(const Ctl*, int) {}
     __device__ __forceinline__ void apply(int, int x, int y, int kz, typename Cx<T>::t (&v)[C], double* acc,
                                           const Ctl*) const {
         if (x == 0 && y == 0 && kz == 0) {
@@ -180,17 +189,20 @@ struct ProMat {
     const double* mats;
     int nph;
     T* sm;
+    int lc = 0;             // batch entries per RVE (0: one RVE shared by all entries)
+    long long mstride = 0;  // stride of an RVE's table block in `mats`
     struct Pre {
         int p;
         T xv[C];
     };
-    __device__ __forceinline__ void load_smem(char* s) {
+    __device__ __forceinline__ void load_smem(char* s, int b) {
         sm = (T*)s;
-        for (int i = threadIdx.x; i < nph * C * C; i += blockDim.x) sm[i] = (T)mats[i];
+        const double* m = mats + (lc ? (long long)(b / lc) * mstride : 0);
+        for (int i = threadIdx.x; i < nph * C * C; i += blockDim.x) sm[i] = (T)m[i];
     }
     __device__ __forceinline__ Pre load(int b, long long v) const {
         Pre q;
-        q.p = phase[v];
+        q.p = phase[(lc ? (long long)(b / lc) * V : 0) + v];
 #pragma unroll
         for (int c = 0; c < C; ++c) q.xv[c] = (T)x[((long long)b * C + c) * V + v];
         return q;
@@ -220,17 +232,20 @@ struct ProRefine64 {
     const double* mats;
     int nph;
     double* sm;
+    int lc = 0;
+    long long mstride = 0;
     struct Pre {
         int p;
         double xv[C];
     };
-    __device__ __forceinline__ void load_smem(char* s) {
+    __device__ __forceinline__ void load_smem(char* s, int b) {
         sm = (double*)s;
-        for (int i = threadIdx.x; i < nph * C * C; i += blockDim.x) sm[i] = mats[i];
+        const double* m = mats + (lc ? (long long)(b / lc) * mstride : 0);
+        for (int i = threadIdx.x; i < nph * C * C; i += blockDim.x) sm[i] = m[i];
     }
     __device__ __forceinline__ Pre load(int b, long long v) const {
         Pre q;
-        q.p = phase[v];
+        q.p = phase[(lc ? (long long)(b / lc) * V : 0) + v];
 #pragma unroll
         for (int c = 0; c < C; ++c) {
             const long long idx = ((long long)b * C + c) * V + v;
@@ -274,19 +289,22 @@ struct EpiEM {
     const double* osum;   // [nph][C]: column sums of the "other field" matrix
     int nph;
     T* sm;
+    int lc = 0;
+    long long mstride = 0;
     struct Pre {
         int p;
         T xv[C];
         T rv[C];
     };
-    __device__ __forceinline__ void load_smem(char* s) {
+    __device__ __forceinline__ void load_smem(char* s, int b) {
         sm = (T*)s;
-        for (int i = threadIdx.x; i < nph * C * C; i += blockDim.x) sm[i] = (T)amats[i];
-        for (int i = threadIdx.x; i < nph * C; i += blockDim.x) sm[nph * C * C + i] = (T)osum[i];
+        const long long o = lc ? (long long)(b / lc) * mstride : 0;
+        for (int i = threadIdx.x; i < nph * C * C; i += blockDim.x) sm[i] = (T)amats[o + i];
+        for (int i = threadIdx.x; i < nph * C; i += blockDim.x) sm[nph * C * C + i] = (T)osum[o + i];
     }
     __device__ __forceinline__ Pre load(int b, long long v) const {
         Pre q;
-        q.p = phase[v];
+        q.p = phase[(lc ? (long long)(b / lc) * V : 0) + v];
 #pragma unroll
         for (int c = 0; c < C; ++c) {
             const long long idx = ((long long)b * C + c) * V + v;
@@ -335,17 +353,20 @@ struct EpiDefect {
     const double* osum;
     int nph;
     double* sm;
+    int lc = 0;
+    long long mstride = 0;
     struct Pre {
         int p;
         double xv[C];
     };
-    __device__ __forceinline__ void load_smem(char* s) {
+    __device__ __forceinline__ void load_smem(char* s, int b) {
         sm = (double*)s;
-        for (int i = threadIdx.x; i < nph * C; i += blockDim.x) sm[i] = osum[i];
+        const double* m = osum + (lc ? (long long)(b / lc) * mstride : 0);
+        for (int i = threadIdx.x; i < nph * C; i += blockDim.x) sm[i] = m[i];
     }
     __device__ __forceinline__ Pre load(int b, long long v) const {
         Pre q;
-        q.p = phase[v];
+        q.p = phase[(lc ? (long long)(b / lc) * V : 0) + v];
 #pragma unroll
         for (int c = 0; c < C; ++c) q.xv[c] = x[((long long)b * C + c) * V + v];
         return q;

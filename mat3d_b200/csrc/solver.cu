@@ -174,6 +174,46 @@ struct m3d_solver {
     std::vector<double> E;   // B x C
     std::vector<double> X0;  // B x 6
 
+    // RVEs of the batch: entry b solves RVE b / (B / nrve) (nrve == 1: one RVE
+    // shared by every entry).  Each RVE has its own phase map (V bytes at
+    // r * V in d_phase), its own table block (mstride doubles at r * mstride
+    // in d_mats) and its own reference medium, whose Green-operator constants
+    // travel in the entries' control blocks.
+    struct RveHost {
+        bool set = false;
+        int nph = 0, scheme = 0;
+        double den_ref = 0;
+        std::vector<long long> counts;
+        std::vector<double> hOsum;
+        int gkind = 0, gnyq = 0, gxw = 0;
+        double gp1 = 0, gp2 = 0;
+    };
+    int nrve = 1;
+    std::vector<RveHost> rv;
+    long long mstride = 0;  // doubles per RVE table block (kMaxPhases phase slots)
+    int entries_per_rve() const { return B / nrve; }
+    int rve_of(int b) const { return b / entries_per_rve(); }
+    void set_green(Ctl& c, int r) const {
+        const RveHost& m = rv[r];
+        c.gkind = m.gkind; c.gnyq = m.gnyq; c.gxw = m.gxw; c.gp1 = m.gp1; c.gp2 = m.gp2;
+    }
+    // per-RVE table and phase-map addressing of a pointwise operator
+    template <class Op> Op tab(Op o) const {
+        o.lc = entries_per_rve();
+        o.mstride = mstride;
+        return o;
+    }
+    void snapshot_rve(int r);
+    bool all_rves_set() const {
+        for (const RveHost& m : rv) if (!m.set) return false;
+        return true;
+    }
+    int nph_max() const {
+        int n = 1;
+        for (const RveHost& m : rv) n = std::max(n, m.nph);
+        return n;
+    }
+
     // device
     uint8_t* d_phase = nullptr;
     void* d_x = nullptr;       // state: T (FP32/FP64) or double (refine)
@@ -185,7 +225,7 @@ struct m3d_solver {
     Ctl* d_ctl = nullptr;
     Ctl* d_ctl_in = nullptr;
     Ctl* h_ctl = nullptr;  // pinned, B entries
-    double* d_mats = nullptr;  // [P | A | O | Osum | Q] blocks
+    double* d_mats = nullptr;  // per RVE: [P | A | O | Osum | Q] blocks
     size_t off_P = 0, off_A = 0, off_O = 0, off_Os = 0, off_Q = 0;
     void* d_tw64 = nullptr;  // double2: Nx | Ny | Nz
     void* d_tw32 = nullptr;  // float2
@@ -335,8 +375,10 @@ int m3d_solver::alloc(int batch) {
 
 int m3d_solver::init_ctl(Ctl* dctl, double tol_field, double tol_eq, int max_iter, bool inner) {
     for (int b = 0; b < B; ++b) {
+        const RveHost& m = rv[rve_of(b)];
         Ctl c;
         std::memset(&c, 0, sizeof(c));
+        set_green(c, rve_of(b));
         c.max_iter = max_iter;
         c.tol_field = tol_field;
         c.tol_eq = tol_eq;
@@ -350,13 +392,13 @@ int m3d_solver::init_ctl(Ctl* dctl, double tol_field, double tol_eq, int max_ite
         }
         c.enorm = std::sqrt(en);
         if (c.enorm == 0) c.enorm = 1;
-        c.den = (double)g.V * den_ref * es;
+        c.den = (double)g.V * m.den_ref * es;
         // sum of the "other" field at the initial uniform state (sum_field_old of the first sweep)
         double s0 = 0;
-        for (int p = 0; p < nph; ++p) {
+        for (int p = 0; p < m.nph; ++p) {
             double o = 0;
-            for (int i = 0; i < C; ++i) o += hOsum[p * C + i] * E[b * C + i];
-            s0 += (double)counts[p] * o;
+            for (int i = 0; i < C; ++i) o += m.hOsum[p * C + i] * E[b * C + i];
+            s0 += (double)m.counts[p] * o;
         }
         c.sum_prev = s0;
         c.inner_tol = inner ? 1e-3 : 0;
@@ -372,35 +414,55 @@ int m3d_solver::sync_ctl(Ctl* dctl) {
     return M3D_OK;
 }
 
+// Green-operator constants of the current reference medium, kept per RVE
+// (the kernels read them from each entry's control block).
+void m3d_solver::snapshot_rve(int r) {
+    RveHost& m = rv[r];
+    m.set = true;
+    m.nph = nph;
+    m.scheme = scheme;
+    m.den_ref = den_ref;
+    m.counts = counts;
+    m.hOsum = hOsum;
+    m.gxw = Nx;
+    m.gnyq = 0;
+    m.gp2 = 0;
+    if (kind == M3D_KIND_MECH) {
+        if (scheme == 1) {
+            m.gkind = GREEN_STRAIN;
+            m.gp1 = 1.0 / (2.0 * mu0);                      // 2*d1, d1 = 1/(4 mu0)   (src/3d/FFT_analysis3D.cpp:162)
+            m.gp2 = (la0 + mu0) / (mu0 * (la0 + 2 * mu0));  // d2                     (:163)
+        } else {
+            m.gkind = GREEN_STRESS;
+            const double c1 = 2 * mu0 * (3 * la0 + 2 * mu0) / (la0 + 2 * mu0), c2 = 2 * mu0;  // (:157-160)
+            m.gp1 = (c1 - c2) / 2.0;
+            m.gp2 = 2.0 * (c2 / 2.0);
+        }
+    } else {
+        if (scheme == 1) {
+            m.gkind = GREEN_TGRAD;
+            m.gnyq = 1;  // src/3dTherm/FFT_thermal3D.cpp:113-120
+            m.gp1 = 1.0 / k0;
+        } else {
+            m.gkind = GREEN_TFLUX;
+            m.gxw = Ny;  // :151 wraps x with Ny
+            m.gp1 = k0;
+        }
+    }
+}
+
+// The operator object; its kind and constants are taken from the control
+// block of each entry (SpecGreen::prepare).
 template <typename T, int CC>
 SpecGreen<T, CC> m3d_solver::green(int zero_k0) const {
     SpecGreen<T, CC> s;
     s.g = g;
     s.zero_k0 = zero_k0;
-    s.xwrap = Nx;
-    s.pos_nyq = 0;
-    if (kind == M3D_KIND_MECH) {
-        if (scheme == 1) {
-            s.kind = GREEN_STRAIN;
-            s.p1 = (T)(1.0 / (2.0 * mu0));                      // 2*d1, d1 = 1/(4 mu0)   (:162)
-            s.p2 = (T)((la0 + mu0) / (mu0 * (la0 + 2 * mu0)));  // d2                     (:163)
-        } else {
-            s.kind = GREEN_STRESS;
-            const double c1 = 2 * mu0 * (3 * la0 + 2 * mu0) / (la0 + 2 * mu0), c2 = 2 * mu0;  // (:157-160)
-            s.p1 = (T)((c1 - c2) / 2.0);
-            s.p2 = (T)(2.0 * (c2 / 2.0));
-        }
-    } else {
-        if (scheme == 1) {
-            s.kind = GREEN_TGRAD;
-            s.pos_nyq = 1;  // src/3dTherm/FFT_thermal3D.cpp:113-120
-            s.p1 = (T)(1.0 / k0);
-        } else {
-            s.kind = GREEN_TFLUX;
-            s.xwrap = Ny;   // :151 wraps x with Ny
-            s.p1 = (T)k0;
-        }
-    }
+    s.kind = rv[0].gkind;
+    s.pos_nyq = rv[0].gnyq;
+    s.xwrap = rv[0].gxw;
+    s.p1 = (T)rv[0].gp1;
+    s.p2 = (T)rv[0].gp2;
     return s;
 }
 
@@ -420,7 +482,7 @@ template <class F> bool with_fast_n(int n, F&& f) {
 
 template <typename T, int CC>
 size_t m3d_solver::op_smem() const {
-    return (size_t)nph * std::max(sizeof(PhaseMech), (size_t)(CC * CC + CC) * sizeof(double)) + 64;
+    return (size_t)nph_max() * std::max(sizeof(PhaseMech), (size_t)(CC * CC + CC) * sizeof(double)) + 64;
 }
 
 template <typename T, int CC, class Pro>
@@ -548,7 +610,7 @@ int m3d_solver::launch_sweep(Pro pro, Spec spec, Epi epi, Ctl* ctl, typename Cx<
 // convergenceCheck reductions (src/3d/FFT_analysis3D.cpp:351-416).
 template <typename T, int CC>
 int m3d_solver::launch_check(Ctl* ctl, const void* x, typename Cx<T>::t* sp) {
-    ProMat<T, CC> pro{d_phase, (const T*)x, g.V, dm(off_Q), nph, nullptr};
+    ProMat<T, CC> pro = tab(ProMat<T, CC>{d_phase, (const T*)x, g.V, dm(off_Q), nph_max(), nullptr});
     SpecEqVar<T, CC> sv{g};
     pass_zfwd<T, CC>(pro, ctl, sp);
     pass_y<T>(-1, CC, ctl, sp);
@@ -562,8 +624,8 @@ int m3d_solver::launch_check(Ctl* ctl, const void* x, typename Cx<T>::t* sp) {
 template <typename T, int CC>
 int m3d_solver::launch_em(Ctl* ctl, T* x, const float* r, typename Cx<T>::t* sp, int zero_k0, int policy,
                           const Ctl* outer) {
-    ProMat<T, CC> pro{d_phase, x, g.V, dm(off_P), nph, nullptr};
-    EpiEM<T, CC> epi{d_phase, x, r, g.V, dm(off_A), dm(off_Os), nph, nullptr};
+    ProMat<T, CC> pro = tab(ProMat<T, CC>{d_phase, x, g.V, dm(off_P), nph_max(), nullptr});
+    EpiEM<T, CC> epi = tab(EpiEM<T, CC>{d_phase, x, r, g.V, dm(off_A), dm(off_Os), nph_max(), nullptr});
     return launch_sweep<T, CC>(pro, green<T, CC>(zero_k0), epi, ctl, sp, policy, outer);
 }
 
@@ -642,8 +704,8 @@ int m3d_solver::run_refine(double tol_field, int max_iter) {
     bool first = true;
     const int chunk = 8;
     for (;;) {
-        ProRefine64<CC> pro{d_phase, x, first ? nullptr : d_delta, g.V, dm(off_P), nph, nullptr};
-        EpiDefect<CC> epi{d_phase, x, d_r32, g.V, dm(off_Os), nph, nullptr};
+        ProRefine64<CC> pro = tab(ProRefine64<CC>{d_phase, x, first ? nullptr : d_delta, g.V, dm(off_P), nph_max(), nullptr});
+        EpiDefect<CC> epi = tab(EpiDefect<CC>{d_phase, x, d_r32, g.V, dm(off_Os), nph_max(), nullptr});
         prof_mark(0);
         rc = launch_sweep<double, CC>(pro, green<double, CC>(0), epi, d_ctl, sp64, POL_REFINE_OUTER, nullptr);
         if (rc) return rc;
@@ -660,6 +722,7 @@ int m3d_solver::run_refine(double tol_field, int max_iter) {
         for (int b = 0; b < B; ++b) {
             Ctl c;
             std::memset(&c, 0, sizeof(c));
+            set_green(c, rve_of(b));
             c.done = outer[b].done;
             c.max_iter = max_iter;
             c.inner_tol = 2e-4;
@@ -751,7 +814,9 @@ static int export_field(m3d_solver* h, const void* x, const double* mats, int b,
         cudaError_t e = cudaMalloc(&h->d_out, (size_t)6 * V * sizeof(double));
         if (e != cudaSuccess) return fail(M3D_ERR_OOM, "export buffer allocation failed");
     }
-    k_export<TX, CC><<<592, 256, 0, h->stream>>>((const TX*)x, h->d_phase, mats, b, V, h->d_out);
+    const int r = h->rve_of(b);
+    const double* M = mats ? mats + (size_t)r * h->mstride : nullptr;
+    k_export<TX, CC><<<592, 256, 0, h->stream>>>((const TX*)x, h->d_phase + (size_t)r * V, M, b, V, h->d_out);
     h->st.kernel_launches += 1;
     M3D_CUDA(cudaGetLastError());
     M3D_CUDA(cudaMemcpyAsync(host_out, h->d_out, (size_t)CC * V * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
@@ -788,7 +853,10 @@ const char* m3d_status_string(int s) {
     }
 }
 
-int m3d_create(int kind, int Nx, int Ny, int Nz, int behav, int precision, int batch, m3d_solver** out) {
+static void table_layout(m3d_solver* h);
+
+static int create_impl(int kind, int Nx, int Ny, int Nz, int behav, int precision, int nrve, int batch,
+                       m3d_solver** out) {
     if (!out) return fail(M3D_ERR_ARG, "out is NULL");
     *out = nullptr;
     if (kind != M3D_KIND_MECH && kind != M3D_KIND_THERMAL) return fail(M3D_ERR_ARG, "kind must be MECH or THERMAL");
@@ -796,10 +864,11 @@ int m3d_create(int kind, int Nx, int Ny, int Nz, int behav, int precision, int b
         return fail(M3D_ERR_ARG, "grid sizes must be in [2, 1024]");
     if (behav < 0 || behav > 2 || (kind == M3D_KIND_THERMAL && behav != 0)) return fail(M3D_ERR_ARG, "invalid behaviour");
     if (precision < 0 || precision > 2) return fail(M3D_ERR_ARG, "invalid precision");
-    if (batch < 1 || batch > 64) return fail(M3D_ERR_ARG, "batch must be in [1, 64]");
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(M3D_ERR_CUDA, "no CUDA device");
     m3d_solver* h = new m3d_solver();
+    h->nrve = nrve;
+    h->rv.assign(nrve, m3d_solver::RveHost{});
     h->kind = kind;
     h->behav = behav;
     h->prec = precision;
@@ -859,12 +928,28 @@ int m3d_create(int kind, int Nx, int Ny, int Nz, int behav, int precision, int b
         cudaMemcpy(h->d_tw64, t64.data(), t64.size() * sizeof(double2), cudaMemcpyHostToDevice);
         cudaMemcpy(h->d_tw32, t32.data(), t32.size() * sizeof(float2), cudaMemcpyHostToDevice);
     }
-    if (cudaMalloc(&h->d_phase, (size_t)h->g.V) != cudaSuccess) {
+    table_layout(h);
+    if (cudaMalloc(&h->d_phase, (size_t)nrve * h->g.V) != cudaSuccess ||
+        cudaMalloc(&h->d_mats, (size_t)nrve * h->mstride * sizeof(double)) != cudaSuccess ||
+        cudaMemset(h->d_phase, 0, (size_t)nrve * h->g.V) != cudaSuccess ||
+        cudaMemset(h->d_mats, 0, (size_t)nrve * h->mstride * sizeof(double)) != cudaSuccess) {
         cudaStreamDestroy(h->stream); delete h;
-        return fail(M3D_ERR_OOM, "phase map allocation failed");
+        return fail(M3D_ERR_OOM, "phase map / table allocation failed");
     }
     *out = h;
     return M3D_OK;
+}
+
+int m3d_create(int kind, int Nx, int Ny, int Nz, int behav, int precision, int batch, m3d_solver** out) {
+    if (batch < 1 || batch > 64) return fail(M3D_ERR_ARG, "batch must be in [1, 64]");
+    return create_impl(kind, Nx, Ny, Nz, behav, precision, 1, batch, out);
+}
+
+int m3d_create_multi(int kind, int Nx, int Ny, int Nz, int precision, int nrve, int nload, m3d_solver** out) {
+    if (nrve < 1 || nrve > 4096) return fail(M3D_ERR_ARG, "nrve must be in [1, 4096]");
+    if (nload < 1 || nload > 6) return fail(M3D_ERR_ARG, "nload must be in [1, 6]");
+    if ((long long)nrve * nload > 8192) return fail(M3D_ERR_ARG, "nrve * nload must be <= 8192");
+    return create_impl(kind, Nx, Ny, Nz, M3D_BEHAV_ELASTIC, precision, nrve, nrve * nload, out);
 }
 
 int m3d_destroy(m3d_solver* h) {
@@ -878,31 +963,39 @@ int m3d_destroy(m3d_solver* h) {
     return M3D_OK;
 }
 
-static int upload_tables(m3d_solver* h) {
-    const int C = h->C, n = h->nph;
-    std::vector<double> all;
+// Table block of RVE r: P, A, O (C x C per phase slot), Osum (C per slot), Q
+// (C x C per slot), kMaxPhases slots each, at r * mstride in d_mats.
+static void table_layout(m3d_solver* h) {
+    const size_t C = h->C, S = kMaxPhases;
     h->off_P = 0;
-    all.insert(all.end(), h->hP.begin(), h->hP.end());
-    h->off_A = all.size();
-    all.insert(all.end(), h->hA.begin(), h->hA.end());
-    h->off_O = all.size();
-    all.insert(all.end(), h->hO.begin(), h->hO.end());
-    h->off_Os = all.size();
-    all.insert(all.end(), h->hOsum.begin(), h->hOsum.end());
-    h->off_Q = all.size();
-    all.insert(all.end(), h->hQ.begin(), h->hQ.end());
-    (void)C; (void)n;
-    cudaFree(h->d_mats);
-    h->d_mats = nullptr;
-    M3D_CUDA(cudaMalloc(&h->d_mats, all.size() * sizeof(double)));
-    M3D_CUDA(cudaMemcpy(h->d_mats, all.data(), all.size() * sizeof(double), cudaMemcpyHostToDevice));
+    h->off_A = S * C * C;
+    h->off_O = 2 * S * C * C;
+    h->off_Os = 3 * S * C * C;
+    h->off_Q = 3 * S * C * C + S * C;
+    h->mstride = (long long)(4 * S * C * C + S * C);
+}
+
+static int upload_tables(m3d_solver* h, int r) {
+    std::vector<double> blk((size_t)h->mstride, 0.0);
+    std::copy(h->hP.begin(), h->hP.end(), blk.begin() + h->off_P);
+    std::copy(h->hA.begin(), h->hA.end(), blk.begin() + h->off_A);
+    std::copy(h->hO.begin(), h->hO.end(), blk.begin() + h->off_O);
+    std::copy(h->hOsum.begin(), h->hOsum.end(), blk.begin() + h->off_Os);
+    std::copy(h->hQ.begin(), h->hQ.end(), blk.begin() + h->off_Q);
+    M3D_CUDA(cudaMemcpy(h->d_mats + (size_t)r * h->mstride, blk.data(), blk.size() * sizeof(double),
+                        cudaMemcpyHostToDevice));
     return M3D_OK;
 }
 
 static void push_mat(std::vector<double>& dst, const Mat& m) { dst.insert(dst.end(), m.begin(), m.end()); }
 
 int m3d_set_material_mech(m3d_solver* h, const double* mat, int nph, const int32_t* phase, int scheme) {
+    return m3d_set_material_mech_rve(h, 0, mat, nph, phase, scheme);
+}
+
+int m3d_set_material_mech_rve(m3d_solver* h, int r, const double* mat, int nph, const int32_t* phase, int scheme) {
     if (!h || !mat || !phase) return fail(M3D_ERR_ARG, "NULL argument");
+    if (r < 0 || r >= h->nrve) return fail(M3D_ERR_ARG, "RVE index out of range");
     if (h->kind != M3D_KIND_MECH) return fail(M3D_ERR_ARG, "not a mechanical solver");
     if (nph < 1 || nph > kMaxPhases) return fail(M3D_ERR_ARG, "nph must be in [1, 16]");
     if (scheme < 0 || scheme > 2) return fail(M3D_ERR_ARG, "invalid scheme");
@@ -975,11 +1068,12 @@ int m3d_set_material_mech(m3d_solver* h, const double* mat, int nph, const int32
     }
     const int p1 = nph > 1 ? 1 : 0;  // the reference reads phases 0 and 1 (:399, :408)
     h->den_ref = (h->scheme == 1) ? 0.5 * h->Cp[0][0] + 0.5 * h->Cp[p1][0] : 0.5 * h->Sp[0][0] + 0.5 * h->Sp[p1][0];
-    int rc = upload_tables(h);
+    int rc = upload_tables(h, r);
     if (rc) return rc;
-    M3D_CUDA(cudaMemcpyAsync(h->d_phase, ph8.data(), (size_t)V, cudaMemcpyHostToDevice, h->stream));
+    M3D_CUDA(cudaMemcpyAsync(h->d_phase + (size_t)r * V, ph8.data(), (size_t)V, cudaMemcpyHostToDevice, h->stream));
     M3D_CUDA(cudaStreamSynchronize(h->stream));
-    h->material_set = true;
+    h->snapshot_rve(r);
+    h->material_set = h->all_rves_set();
     h->st.scheme = h->scheme;
     h->st.la0 = h->la0;
     h->st.mu0 = h->mu0;
@@ -992,7 +1086,12 @@ int m3d_set_material_mech(m3d_solver* h, const double* mat, int nph, const int32
 }
 
 int m3d_set_material_thermal(m3d_solver* h, double km, double ki, const int32_t* phase, int scheme) {
+    return m3d_set_material_thermal_rve(h, 0, km, ki, phase, scheme);
+}
+
+int m3d_set_material_thermal_rve(m3d_solver* h, int r, double km, double ki, const int32_t* phase, int scheme) {
     if (!h || !phase) return fail(M3D_ERR_ARG, "NULL argument");
+    if (r < 0 || r >= h->nrve) return fail(M3D_ERR_ARG, "RVE index out of range");
     if (h->kind != M3D_KIND_THERMAL) return fail(M3D_ERR_ARG, "not a thermal solver");
     if (!(km > 0) || !(ki > 0)) return fail(M3D_ERR_ARG, "conductivities must be positive");
     if (scheme < 0 || scheme > 2) return fail(M3D_ERR_ARG, "invalid scheme");
@@ -1037,11 +1136,12 @@ int m3d_set_material_thermal(m3d_solver* h, double km, double ki, const int32_t*
         }
     }
     h->den_ref = (h->scheme == 1) ? 0.5 * ki + 0.5 * km : 0.5 / ki + 0.5 / km;  // (:346, :356)
-    int rc = upload_tables(h);
+    int rc = upload_tables(h, r);
     if (rc) return rc;
-    M3D_CUDA(cudaMemcpyAsync(h->d_phase, ph8.data(), (size_t)V, cudaMemcpyHostToDevice, h->stream));
+    M3D_CUDA(cudaMemcpyAsync(h->d_phase + (size_t)r * V, ph8.data(), (size_t)V, cudaMemcpyHostToDevice, h->stream));
     M3D_CUDA(cudaStreamSynchronize(h->stream));
-    h->material_set = true;
+    h->snapshot_rve(r);
+    h->material_set = h->all_rves_set();
     h->st.scheme = h->scheme;
     h->st.k0 = h->k0;
     h->st.vol_fraction[0] = h->vol[0];
@@ -1081,6 +1181,8 @@ int m3d_run(m3d_solver* h, double tol_field, double tol_eq, int nInc, int criter
 
 }  // extern "C"
 
+static int assemble_rve(m3d_solver* h, int r, double* Ceff, double* Seff, double* ep_means, double* sig_means);
+
 // means of the strain-like and stress-like fields of entry b
 template <typename TX, int CC>
 __global__ void k_means(const TX* __restrict__ x, const uint8_t* __restrict__ phase, const double* __restrict__ mats,
@@ -1116,13 +1218,15 @@ int m3d_get_means(m3d_solver* h, int b, double* strain_mean, double* stress_mean
     const int nblk = 296;
     double* part = h->d_part;
     if (h->part_cap < (size_t)nblk * 2 * C) return fail(M3D_ERR_STATE, "partials buffer too small");
-    const double* O = h->d_mats + h->off_O;
+    const int r = h->rve_of(b);
+    const double* O = h->d_mats + (size_t)r * h->mstride + h->off_O;
+    const uint8_t* ph = h->d_phase + (size_t)r * h->g.V;
     if (C == 6) {
-        if (h->prec == M3D_PREC_FP32) k_means<float, 6><<<nblk, 256, 0, h->stream>>>((const float*)h->d_x, h->d_phase, O, b, h->g.V, part);
-        else k_means<double, 6><<<nblk, 256, 0, h->stream>>>((const double*)h->d_x, h->d_phase, O, b, h->g.V, part);
+        if (h->prec == M3D_PREC_FP32) k_means<float, 6><<<nblk, 256, 0, h->stream>>>((const float*)h->d_x, ph, O, b, h->g.V, part);
+        else k_means<double, 6><<<nblk, 256, 0, h->stream>>>((const double*)h->d_x, ph, O, b, h->g.V, part);
     } else {
-        if (h->prec == M3D_PREC_FP32) k_means<float, 3><<<nblk, 256, 0, h->stream>>>((const float*)h->d_x, h->d_phase, O, b, h->g.V, part);
-        else k_means<double, 3><<<nblk, 256, 0, h->stream>>>((const double*)h->d_x, h->d_phase, O, b, h->g.V, part);
+        if (h->prec == M3D_PREC_FP32) k_means<float, 3><<<nblk, 256, 0, h->stream>>>((const float*)h->d_x, ph, O, b, h->g.V, part);
+        else k_means<double, 3><<<nblk, 256, 0, h->stream>>>((const double*)h->d_x, ph, O, b, h->g.V, part);
     }
     h->st.kernel_launches += 1;
     M3D_CUDA(cudaGetLastError());
@@ -1134,8 +1238,9 @@ int m3d_get_means(m3d_solver* h, int b, double* strain_mean, double* stress_mean
         for (int i = 0; i < nblk; ++i) s[k] += hp[(size_t)k * nblk + i];
     const double V = (double)h->g.V;
     // state = strain-like in the primal scheme, stress-like in the dual scheme
-    double* prim = (h->scheme == 1) ? strain_mean : stress_mean;
-    double* dual = (h->scheme == 1) ? stress_mean : strain_mean;
+    const bool primal = h->rv[r].scheme == 1;
+    double* prim = primal ? strain_mean : stress_mean;
+    double* dual = primal ? stress_mean : strain_mean;
     for (int c = 0; c < C; ++c) {
         if (prim) prim[c] = s[c] / V;
         if (dual) dual[c] = s[C + c] / V;
@@ -1149,28 +1254,47 @@ int m3d_homogenize(m3d_solver* h, double tol_field, double tol_eq, int criterion
     if (!h->material_set) return fail(M3D_ERR_STATE, "material not set");
     if (h->kind == M3D_KIND_MECH && h->behav != M3D_BEHAV_ELASTIC)
         return fail(M3D_ERR_ARG, "homogenization runs the elastic solver; create the solver with behaviour ELASTIC");
-    const int C = h->C;
-    if (h->B != C) {
-        int rc = h->alloc(C);
+    const int C = h->C, R = h->nrve;
+    if (h->B != C * R) {
+        int rc = h->alloc(C * R);
         if (rc) return rc;
     }
-    // load cases (src/3d/FFT_analysis3D.cpp:866-877; src/3dTherm/FFT_thermal3D.cpp:501-507, 544-549)
-    for (int w = 0; w < C; ++w) {
-        double E[6] = {0, 0, 0, 0, 0, 0};
-        if (h->kind == M3D_KIND_MECH) E[w] = (h->scheme == 1) ? 0.0005 : 1.e6;
-        else E[w] = 1.0;
-        int rc = m3d_set_load(h, w, E, h->kind == M3D_KIND_MECH ? E : nullptr);
-        if (rc) return rc;
-    }
+    // load cases (src/3d/FFT_analysis3D.cpp:866-877; src/3dTherm/FFT_thermal3D.cpp:501-507, 544-549);
+    // entry r * C + w is load case w of RVE r
+    for (int r = 0; r < R; ++r)
+        for (int w = 0; w < C; ++w) {
+            double E[6] = {0, 0, 0, 0, 0, 0};
+            if (h->kind == M3D_KIND_MECH) E[w] = (h->rv[r].scheme == 1) ? 0.0005 : 1.e6;
+            else E[w] = 1.0;
+            int rc = m3d_set_load(h, r * C + w, E, h->kind == M3D_KIND_MECH ? E : nullptr);
+            if (rc) return rc;
+        }
     const auto t0 = std::chrono::steady_clock::now();
     int rc = h->dispatch_run(tol_field, tol_eq, 1, criterion, max_iter);
     if (rc != M3D_OK && rc != M3D_NOT_CONVERGED) return rc;
     const int status = rc;
     h->run_done = true;
+    for (int r = 0; r < R; ++r) {
+        rc = assemble_rve(h, r, Ceff ? Ceff + (size_t)r * C * C : nullptr, Seff ? Seff + (size_t)r * C * C : nullptr,
+                          ep_means ? ep_means + (size_t)r * C * C : nullptr,
+                          sig_means ? sig_means + (size_t)r * C * C : nullptr);
+        if (rc) return rc;
+    }
+    h->st.solve_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    h->st.status = status;
+    return status;
+}
+
+}  // extern "C"
+
+// Effective tensor of RVE r from the means of its C load-case entries.
+static int assemble_rve(m3d_solver* h, int r, double* Ceff, double* Seff, double* ep_means, double* sig_means) {
+    const int C = h->C;
+    int rc;
     // strain-like means g[w][c], stress-like q[w][c] per load case w
     std::vector<double> gm(C * C), qm(C * C);
     for (int w = 0; w < C; ++w) {
-        rc = m3d_get_means(h, w, &gm[w * C], &qm[w * C]);
+        rc = m3d_get_means(h, r * C + w, &gm[w * C], &qm[w * C]);
         if (rc) return rc;
     }
     // Assembly exactly as the reference: one matrix stores the means with one
@@ -1183,7 +1307,7 @@ int m3d_homogenize(m3d_solver* h, double tol_field, double tol_eq, int criterion
     //      heatFluxHomo(j,w) (columns), KHomo = tempGradHomo^-1 heatFluxHomo
     //  thermal flux       (:567-578): heatFluxHomo(w,j) (rows), tempGradHomo(j,w) (columns),
     //      RHomo = heatFluxHomo^-1 tempGradHomo
-    const bool primal = (h->scheme == 1);
+    const bool primal = (h->rv[r].scheme == 1);
     Mat rows_g(C * C), cols_g(C * C), rows_q(C * C), cols_q(C * C);
     for (int w = 0; w < C; ++w)
         for (int t = 0; t < C; ++t) {
@@ -1210,10 +1334,10 @@ int m3d_homogenize(m3d_solver* h, double tol_field, double tol_eq, int criterion
     if (Seff) std::memcpy(Seff, Sm.data(), C * C * sizeof(double));
     if (ep_means) std::memcpy(ep_means, strain_store.data(), C * C * sizeof(double));
     if (sig_means) std::memcpy(sig_means, stress_store.data(), C * C * sizeof(double));
-    h->st.solve_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
-    h->st.status = status;
-    return status;
+    return M3D_OK;
 }
+
+extern "C" {
 
 int m3d_get_field(m3d_solver* h, int which, int b, double* out) {
     if (!h || !out) return fail(M3D_ERR_ARG, "NULL argument");
@@ -1222,7 +1346,7 @@ int m3d_get_field(m3d_solver* h, int which, int b, double* out) {
     if (h->kind == M3D_KIND_MECH && h->behav != M3D_BEHAV_ELASTIC) return h->in.get_field(h, which, b, out);
     if (which != M3D_FIELD_STRAIN && which != M3D_FIELD_STRESS)
         return fail(M3D_ERR_ARG, "field not available for this behaviour");
-    const bool state = (which == M3D_FIELD_STRAIN) == (h->scheme == 1);
+    const bool state = (which == M3D_FIELD_STRAIN) == (h->rv[h->rve_of(b)].scheme == 1);
     const double* M = state ? nullptr : h->d_mats + h->off_O;
     if (h->C == 6)
         return h->prec == M3D_PREC_FP32 ? export_field<float, 6>(h, h->d_x, M, b, out) : export_field<double, 6>(h, h->d_x, M, b, out);

@@ -152,6 +152,7 @@ int m3d_solver::run_inelastic(double tol_field, double tol_eq, int nInc, int cri
         for (int i = 0; i < 6; ++i) en += ((i >= 3) ? 2.0 : 1.0) * dE[b * 6 + i] * dE[b * 6 + i];
         c.enorm = en > 0 ? std::sqrt(en) : 1.0;
         c.den = den_ref;
+        set_green(c, 0);
         const double* X = &X0[b * 6];
         double y[6];
         for (int i = 0; i < 6; ++i) {

@@ -1,0 +1,145 @@
+"""Many RVEs in one batch (m3d_create_multi): every RVE's result equals the
+same RVE solved on its own handle, bitwise, and one RVE of the batch is
+checked against the CPU oracle.
+
+Each entry of a batch evaluates its own stop rule and its own deterministic
+fixed-order reductions, and each RVE's tables and Green-operator constants
+are its own, so sharing a launch with other RVEs must not change a single bit.
+"""
+import numpy as np
+import pytest
+
+import mat3d_b200 as m3d
+from oracle import mat3d_oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def sphere_rve(shape, r, center=None):
+    Nx, Ny, Nz = shape
+    X, Y, Z = np.meshgrid(np.arange(Nx), np.arange(Ny), np.arange(Nz), indexing="ij")
+    c = center or (Nx / 2, Ny / 2, Nz / 2)
+    rve = np.ones(shape, np.int32)
+    rve[(X - c[0]) ** 2 + (Y - c[1]) ** 2 + (Z - c[2]) ** 2 <= r * r] = 0
+    return rve.ravel()
+
+
+def mech_mat(contrast, stiff_matrix=False):
+    inc = [contrast * 3e9, 0.2, 1e30, 0, 1, 0, 1e30]
+    mtx = [3e9, 0.35, 1e30, 0, 1, 0, 1e30]
+    return np.array([mtx, inc] if stiff_matrix else [inc, mtx])
+
+
+# three RVEs that differ in microstructure, contrast and scheme (the third has
+# a dominant stiff phase, so the automatic choice is the stress-based scheme)
+MECH_CASES = [
+    (dict(r=3.0), mech_mat(20.0), m3d.SCHEME_AUTO),
+    (dict(r=4.5, center=(5, 9, 7)), mech_mat(3.0), m3d.SCHEME_AUTO),
+    (dict(r=5.0), mech_mat(50.0, stiff_matrix=True), m3d.SCHEME_AUTO),
+]
+
+
+@pytest.mark.parametrize("prec,tol", [("fp64", 1e-10), ("fp32_refine", 1e-9), ("fp32", 1e-5)])
+def test_multi_elastic_homogenize_equals_single(prec, tol):
+    shape = (16, 16, 16)
+    R = len(MECH_CASES)
+    mb = m3d.Solver(m3d.KIND_MECH, *shape, 0, prec, nrve=R, nload=6)
+    rves = [sphere_rve(shape, **geo) for geo, _, _ in MECH_CASES]
+    for r, (_, mat, sch) in enumerate(MECH_CASES):
+        mb.set_material_mech(mat, rves[r], sch, rve=r)
+    Cm, Sm, epm, sgm, _ = mb.homogenize(tol, 0, m3d.CRIT_RESIDUAL)
+    assert Cm.shape == (R, 6, 6)
+    schemes = []
+    for r, (_, mat, sch) in enumerate(MECH_CASES):
+        s1 = m3d.Solver(m3d.KIND_MECH, *shape, 0, prec, 6)
+        s1.set_material_mech(mat, rves[r], sch)
+        schemes.append(s1.stats()["scheme"])
+        C1, S1, ep1, sg1, _ = s1.homogenize(tol, 0, m3d.CRIT_RESIDUAL)
+        assert np.array_equal(Cm[r], C1), (r, np.abs(Cm[r] - C1).max())
+        assert np.array_equal(Sm[r], S1)
+        assert np.array_equal(epm[r], ep1) and np.array_equal(sgm[r], sg1)
+        s1.close()
+    assert 1 in schemes and 2 in schemes  # both schemes share the batch
+    mb.close()
+
+
+def test_multi_elastic_vs_oracle():
+    shape = (12, 12, 12)
+    geo, mat, _ = MECH_CASES[2]
+    rves = [sphere_rve(shape, 2.5), sphere_rve(shape, 3.5)]
+    mats = [mech_mat(10.0), mat]
+    mb = m3d.Solver(m3d.KIND_MECH, *shape, 0, "fp64", nrve=2, nload=6)
+    for r in range(2):
+        mb.set_material_mech(mats[r], rves[r], rve=r)
+    Cm, Sm, *_ = mb.homogenize(1e-10, 1e-10, m3d.CRIT_REFERENCE)
+    for r in range(2):
+        o = O.MechOracle(*shape, "e")
+        o.material(mats[r], rves[r])
+        CH, SH = o.homogenization(1e-10, 1e-10)
+        assert np.abs(Cm[r] - CH).max() / np.abs(CH).max() < 1e-9
+        assert np.abs(Sm[r] - SH).max() / np.abs(SH).max() < 1e-9
+    mb.close()
+
+
+@pytest.mark.parametrize("prec,tol", [("fp64", 1e-10), ("fp32_refine", 1e-9)])
+def test_multi_thermal_homogenize_equals_single(prec, tol):
+    shape = (16, 16, 16)
+    cases = [(1.0, 100.0, sphere_rve(shape, 4.0)),   # gradient-based
+             (100.0, 1.0, sphere_rve(shape, 3.0)),   # flux-based
+             (1.0, 5.0, sphere_rve(shape, 5.5, (4, 4, 4)))]
+    mb = m3d.Solver(m3d.KIND_THERMAL, *shape, 0, prec, nrve=len(cases), nload=3)
+    for r, (km, ki, rve) in enumerate(cases):
+        mb.set_material_thermal(km, ki, rve, rve=r)
+    Km, Rm, *_ = mb.homogenize(tol, 0, m3d.CRIT_RESIDUAL)
+    schemes = []
+    for r, (km, ki, rve) in enumerate(cases):
+        s1 = m3d.Solver(m3d.KIND_THERMAL, *shape, 0, prec, 3)
+        s1.set_material_thermal(km, ki, rve)
+        schemes.append(s1.stats()["scheme"])
+        K1, R1, *_ = s1.homogenize(tol, 0, m3d.CRIT_RESIDUAL)
+        assert np.array_equal(Km[r], K1), (r, np.abs(Km[r] - K1).max())
+        assert np.array_equal(Rm[r], R1)
+        s1.close()
+    assert 1 in schemes and 2 in schemes
+    mb.close()
+
+
+def test_multi_run_fields_and_loads():
+    """nload = 2 with per-entry loads through m3d_run: fields of every entry
+    equal the single-RVE solves."""
+    shape = (16, 16, 16)
+    R, L = 3, 2
+    mb = m3d.Solver(m3d.KIND_MECH, *shape, 0, "fp64", nrve=R, nload=L)
+    rves = [sphere_rve(shape, 3.0 + r) for r in range(R)]
+    mats = [mech_mat(5.0 + 20 * r) for r in range(R)]
+    loads = [np.array([1e-3, 0, 0, 0, 0, 0.0]), np.array([0, 0, 0, 2e-4, 0, 3e-4])]
+    for r in range(R):
+        mb.set_material_mech(mats[r], rves[r], rve=r)
+        for l in range(L):
+            mb.set_load(loads[l], None, b=r * L + l)
+    mb.run(1e-9, 0, 1, m3d.CRIT_RESIDUAL)
+    for r in range(R):
+        s1 = m3d.Solver(m3d.KIND_MECH, *shape, 0, "fp64", L)
+        s1.set_material_mech(mats[r], rves[r])
+        for l in range(L):
+            s1.set_load(loads[l], None, b=l)
+        s1.run(1e-9, 0, 1, m3d.CRIT_RESIDUAL)
+        for l in range(L):
+            for which in (m3d.FIELD_STRAIN, m3d.FIELD_STRESS):
+                assert np.array_equal(mb.field(which, r * L + l), s1.field(which, l)), (r, l, which)
+            em, sm = mb.means(r * L + l)
+            e1, s1m = s1.means(l)
+            assert np.array_equal(em, e1) and np.array_equal(sm, s1m)
+        s1.close()
+    mb.close()
+
+
+def test_multi_rejects_unset_rve_and_bad_index():
+    shape = (8, 8, 8)
+    mb = m3d.Solver(m3d.KIND_MECH, *shape, 0, "fp64", nrve=2, nload=6)
+    mb.set_material_mech(mech_mat(10.0), sphere_rve(shape, 2.0), rve=0)
+    with pytest.raises(m3d.M3DError):
+        mb.homogenize(1e-8)  # RVE 1 has no material yet
+    with pytest.raises(m3d.M3DError):
+        mb.set_material_mech(mech_mat(10.0), sphere_rve(shape, 2.0), rve=2)
+    mb.close()
