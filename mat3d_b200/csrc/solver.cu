@@ -295,6 +295,30 @@ struct m3d_solver {
     int run_linear(double tol_field, double tol_eq, int criterion, int max_iter);
     template <int CC>
     int run_refine(double tol_field, int max_iter);
+    // Graph-captured solves: the whole iteration runs as one CUDA graph launch,
+    // its loops as conditional while nodes that a one-block kernel re-arms
+    // after each sweep (no host round trip until the batch is done).
+    bool use_graph = true;
+    struct GraphSlot {
+        cudaGraphExec_t exec = nullptr;
+        long long key = -1;
+    };
+    GraphSlot gslot[3];  // 0: linear residual rule, 1: linear reference rule, 2: refinement
+    int* d_trips = nullptr;  // [0] loop trips this run, [1] outer trips total, [2] inner trips this round, [3] inner total
+    void drop_graphs() {
+        for (GraphSlot& s : gslot) {
+            if (s.exec) cudaGraphExecDestroy(s.exec);
+            s.exec = nullptr;
+            s.key = -1;
+        }
+    }
+    long long graph_key(int type) const {
+        return ((((long long)type * 8192 + B) * 32 + nph_max()) * 2 + (use_fast ? 1 : 0)) * 4 + prec;
+    }
+    template <typename T, int CC>
+    int run_linear_graph(double tol_field, double tol_eq, int criterion, int max_iter);
+    template <int CC>
+    int run_refine_graph(double tol_field, int max_iter);
     template <typename T, int CC>
     int launch_em(Ctl* ctl, T* x, const float* r, typename Cx<T>::t* sp, int zero_k0, int policy, const Ctl* outer);
     int init_ctl(Ctl* dctl, double tol_field, double tol_eq, int max_iter, bool inner);
@@ -308,6 +332,8 @@ struct m3d_solver {
 m3d_solver::~m3d_solver() { free_all(); }
 
 void m3d_solver::free_all() {
+    drop_graphs();
+    cudaFree(d_trips); d_trips = nullptr;
     cudaFree(d_phase); d_phase = nullptr;
     cudaFree(d_x); d_x = nullptr;
     cudaFree(d_delta); d_delta = nullptr;
@@ -331,6 +357,8 @@ int m3d_solver::alloc(int batch) {
     // batch independent and allocated once.
     const long long V = g.V;
     const size_t specN = (size_t)batch * C * g.NL * g.Hzp;
+    drop_graphs();  // captured launches hold the old buffers
+    if (!d_trips) M3D_CUDA(cudaMalloc(&d_trips, 8 * sizeof(int)));
     cudaFree(d_x); cudaFree(d_delta); cudaFree(d_r32); cudaFree(d_spec); cudaFree(d_part);
     cudaFree(d_ctl); cudaFree(d_ctl_in);
     if (h_ctl) cudaFreeHost(h_ctl);
@@ -762,6 +790,221 @@ int m3d_solver::run_refine(double tol_field, int max_iter) {
     return status;
 }
 
+// ---- graph-captured solves -------------------------------------------------------
+// Loop control of a captured while node: continue while any entry of the batch
+// is not done.  Every entry stops by its own rule or at its iteration cap; the
+// trip count is a second cap on the loop itself.
+__global__ void k_loop_cond(cudaGraphConditionalHandle h, const Ctl* __restrict__ ctl, int B, int* trips, int slot) {
+    int any = 0;
+    for (int b = threadIdx.x; b < B; b += blockDim.x) any |= (ctl[b].done == 0);
+    any = __syncthreads_or(any);
+    if (threadIdx.x == 0) {
+        const int t = ++trips[slot];
+        ++trips[slot + 1];
+        cudaGraphSetConditional(h, (any && t <= ctl[0].max_iter + 2) ? 1u : 0u);
+    }
+}
+
+// Between the FP64 defect sweep and the FP32 correction solve of the
+// refinement: count the inner sweeps of the previous round (aux[1]), give
+// every entry a fresh inner control block (the entries already converged stay
+// done) and arm both loops.
+__global__ void k_refine_mid(cudaGraphConditionalHandle h_outer, cudaGraphConditionalHandle h_inner, Ctl* ctl,
+                             Ctl* ctl_in, int B, double inner_tol, int* trips) {
+    int any = 0;
+    for (int b = threadIdx.x; b < B; b += blockDim.x) {
+        Ctl& o = ctl[b];
+        o.aux[1] += (double)ctl_in[b].iters;
+        Ctl c;
+        memset(&c, 0, sizeof(c));
+        c.gkind = o.gkind; c.gnyq = o.gnyq; c.gxw = o.gxw; c.gp1 = o.gp1; c.gp2 = o.gp2;
+        c.done = o.done;
+        c.max_iter = o.max_iter;
+        c.inner_tol = inner_tol;
+        ctl_in[b] = c;
+        any |= (o.done == 0);
+    }
+    any = __syncthreads_or(any);
+    if (threadIdx.x == 0) {
+        const int t = ++trips[0];
+        ++trips[1];
+        trips[2] = 0;
+        const unsigned go = (any && t <= ctl[0].max_iter + 2) ? 1u : 0u;
+        cudaGraphSetConditional(h_outer, go);
+        cudaGraphSetConditional(h_inner, go);
+    }
+}
+
+// A while node appended to `graph` after `deps`; returns its body graph.
+static cudaError_t add_while(cudaGraph_t graph, const cudaGraphNode_t* deps, size_t ndeps,
+                             cudaGraphConditionalHandle h, cudaGraphNode_t* node, cudaGraph_t* body) {
+    cudaGraphNodeParams p = {cudaGraphNodeTypeConditional};  // the remaining members are zero
+    p.conditional.handle = h;
+    p.conditional.type = cudaGraphCondTypeWhile;
+    p.conditional.size = 1;
+    cudaError_t e = cudaGraphAddNode(node, graph, deps, ndeps, &p);
+    if (e == cudaSuccess) *body = p.conditional.phGraph_out[0];
+    return e;
+}
+
+#define M3D_CAP(call)                                                         \
+    do {                                                                      \
+        cudaError_t e_ = (call);                                              \
+        if (e_ != cudaSuccess) {                                              \
+            cudaGraph_t junk_ = nullptr;                                      \
+            cudaStreamEndCapture(stream, &junk_);                             \
+            if (junk_) cudaGraphDestroy(junk_);                               \
+            cudaGraphDestroy(top);                                            \
+            (void)cudaGetLastError();                                         \
+            return fail(M3D_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e_)); \
+        }                                                                     \
+    } while (0)
+
+template <typename T, int CC>
+int m3d_solver::run_linear_graph(double tol_field, double tol_eq, int criterion, int max_iter) {
+    typedef typename Cx<T>::t C2;
+    int rc = init_ctl(d_ctl, tol_field, tol_eq, max_iter, false);
+    if (rc) return rc;
+    T* x = (T*)d_x;
+    C2* sp = (C2*)d_spec;
+    k_fill_load<T><<<dim3(256, B * CC), 256, 0, stream>>>(x, d_ctl, CC, g.V);
+    M3D_CUDA(cudaMemsetAsync(d_trips, 0, 8 * sizeof(int), stream));
+    const bool resid = (criterion == M3D_CRIT_RESIDUAL);
+    GraphSlot& gs = gslot[resid ? 0 : 1];
+    const long long key = graph_key(resid ? 0 : 1);
+    if (gs.key != key) {
+        drop_graphs();
+        cudaGraph_t top = nullptr;
+        M3D_CUDA(cudaGraphCreate(&top, 0));
+        cudaGraphConditionalHandle h;
+        cudaGraphNode_t node;
+        cudaGraph_t body = nullptr;
+        M3D_CAP(cudaGraphConditionalHandleCreate(&h, top, 1, cudaGraphCondAssignDefault));
+        M3D_CAP(add_while(top, nullptr, 0, h, &node, &body));
+        const long long kl = st.kernel_launches;  // captured launches are counted per executed trip below
+        M3D_CAP(cudaStreamBeginCaptureToGraph(stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+        if (resid) {
+            rc = launch_em<T, CC>(d_ctl, x, nullptr, sp, 0, POL_RESIDUAL, nullptr);
+        } else {
+            rc = launch_em<T, CC>(d_ctl, x, nullptr, sp, 0, POL_REF_SWEEP, nullptr);
+            if (!rc) rc = launch_check<T, CC>(d_ctl, x, sp);
+        }
+        if (rc) M3D_CAP(cudaErrorUnknown);
+        k_loop_cond<<<1, 256, 0, stream>>>(h, d_ctl, B, d_trips, 0);
+        M3D_CAP(cudaGetLastError());
+        cudaGraph_t got = nullptr;
+        M3D_CAP(cudaStreamEndCapture(stream, &got));
+        st.kernel_launches = kl;
+        cudaError_t e = cudaGraphInstantiate(&gs.exec, top, 0);
+        cudaGraphDestroy(top);
+        if (e != cudaSuccess) { gs.exec = nullptr; return fail(M3D_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e)); }
+        gs.key = key;
+    }
+    M3D_CUDA(cudaGraphLaunch(gs.exec, stream));
+    rc = sync_ctl(d_ctl);
+    if (rc) return rc;
+    int trips[8];
+    M3D_CUDA(cudaMemcpy(trips, d_trips, sizeof(trips), cudaMemcpyDeviceToHost));
+    st.kernel_launches += 1 + (long long)trips[0] * (resid ? 6 : 10);
+    long long sw = 0;
+    int status = M3D_OK;
+    for (int b = 0; b < B; ++b) {
+        sw += h_ctl[b].iters;
+        if (h_ctl[b].status == 1 && status == M3D_OK) status = M3D_NOT_CONVERGED;
+        if (h_ctl[b].status == 2) status = M3D_ERR_NAN;
+    }
+    st.sweeps = sw;
+    if (sizeof(T) == 8) { st.sweeps_fp64 = sw; st.sweeps_fp32 = 0; } else { st.sweeps_fp32 = sw; st.sweeps_fp64 = 0; }
+    st.iters = h_ctl[0].iters;
+    st.residual = h_ctl[0].residual;
+    st.eqvar = h_ctl[0].eqvar;
+    st.diff_sum = h_ctl[0].diff_sum;
+    st.diff_eq = h_ctl[0].diff_eq;
+    return status;
+}
+
+template <int CC>
+int m3d_solver::run_refine_graph(double tol_field, int max_iter) {
+    int rc = init_ctl(d_ctl, tol_field, 0, max_iter, false);
+    if (rc) return rc;
+    double* x = (double*)d_x;
+    double2* sp64 = (double2*)d_spec;
+    float2* sp32 = (float2*)d_spec;
+    const size_t dbytes = (size_t)B * CC * g.V * sizeof(float);
+    k_fill_load<double><<<dim3(256, B * CC), 256, 0, stream>>>(x, d_ctl, CC, g.V);
+    M3D_CUDA(cudaMemsetAsync(d_delta, 0, dbytes, stream));
+    M3D_CUDA(cudaMemsetAsync(d_ctl_in, 0, (size_t)B * sizeof(Ctl), stream));
+    M3D_CUDA(cudaMemsetAsync(d_trips, 0, 8 * sizeof(int), stream));
+    GraphSlot& gs = gslot[2];
+    const long long key = graph_key(2);
+    if (gs.key != key) {
+        drop_graphs();
+        cudaGraph_t top = nullptr;
+        M3D_CUDA(cudaGraphCreate(&top, 0));
+        cudaGraphConditionalHandle h_out, h_in;
+        cudaGraphNode_t n_out, n_in;
+        cudaGraph_t b_out = nullptr, b_in = nullptr;
+        M3D_CAP(cudaGraphConditionalHandleCreate(&h_out, top, 1, cudaGraphCondAssignDefault));
+        M3D_CAP(add_while(top, nullptr, 0, h_out, &n_out, &b_out));
+        M3D_CAP(cudaGraphConditionalHandleCreate(&h_in, b_out, 0, 0));
+        const long long kl = st.kernel_launches;  // captured launches are counted per executed trip below
+        // outer body: FP64 defect sweep (folds in the previous correction),
+        // loop control, cleared correction, then the inner while node
+        M3D_CAP(cudaStreamBeginCaptureToGraph(stream, b_out, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+        ProRefine64<CC> pro = tab(ProRefine64<CC>{d_phase, x, d_delta, g.V, dm(off_P), nph_max(), nullptr});
+        EpiDefect<CC> epi = tab(EpiDefect<CC>{d_phase, x, d_r32, g.V, dm(off_Os), nph_max(), nullptr});
+        rc = launch_sweep<double, CC>(pro, green<double, CC>(0), epi, d_ctl, sp64, POL_REFINE_OUTER, nullptr);
+        if (rc) M3D_CAP(cudaErrorUnknown);
+        k_refine_mid<<<1, 256, 0, stream>>>(h_out, h_in, d_ctl, d_ctl_in, B, 2e-4, d_trips);
+        M3D_CAP(cudaGetLastError());
+        M3D_CAP(cudaMemsetAsync(d_delta, 0, dbytes, stream));
+        {
+            cudaStreamCaptureStatus cs;
+            cudaGraph_t capg = nullptr;
+            const cudaGraphNode_t* deps = nullptr;
+            size_t nd = 0;
+            M3D_CAP(cudaStreamGetCaptureInfo(stream, &cs, nullptr, &capg, &deps, &nd));
+            M3D_CAP(add_while(capg, deps, nd, h_in, &n_in, &b_in));
+            M3D_CAP(cudaStreamUpdateCaptureDependencies(stream, &n_in, 1, cudaStreamSetCaptureDependencies));
+        }
+        cudaGraph_t got = nullptr;
+        M3D_CAP(cudaStreamEndCapture(stream, &got));
+        // inner body: FP32 correction sweep + loop control
+        M3D_CAP(cudaStreamBeginCaptureToGraph(stream, b_in, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+        rc = launch_em<float, CC>(d_ctl_in, d_delta, d_r32, sp32, 1, POL_REFINE_INNER, d_ctl);
+        if (rc) M3D_CAP(cudaErrorUnknown);
+        k_loop_cond<<<1, 256, 0, stream>>>(h_in, d_ctl_in, B, d_trips, 2);
+        M3D_CAP(cudaGetLastError());
+        M3D_CAP(cudaStreamEndCapture(stream, &got));
+        st.kernel_launches = kl;
+        cudaError_t e = cudaGraphInstantiate(&gs.exec, top, 0);
+        cudaGraphDestroy(top);
+        if (e != cudaSuccess) { gs.exec = nullptr; return fail(M3D_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e)); }
+        gs.key = key;
+    }
+    M3D_CUDA(cudaGraphLaunch(gs.exec, stream));
+    rc = sync_ctl(d_ctl);
+    if (rc) return rc;
+    int trips[8];
+    M3D_CUDA(cudaMemcpy(trips, d_trips, sizeof(trips), cudaMemcpyDeviceToHost));
+    st.kernel_launches += 1 + (long long)trips[1] * 6 + (long long)trips[3] * 6;
+    long long n64 = 0, n32 = 0;
+    int status = M3D_OK;
+    for (int b = 0; b < B; ++b) {
+        n64 += h_ctl[b].iters;
+        n32 += (long long)h_ctl[b].aux[1];
+        if (h_ctl[b].status == 1 && status == M3D_OK) status = M3D_NOT_CONVERGED;
+        if (h_ctl[b].status == 2) status = M3D_ERR_NAN;
+    }
+    st.sweeps = n64 + n32;
+    st.sweeps_fp64 = n64;
+    st.sweeps_fp32 = n32;
+    st.iters = h_ctl[0].iters;
+    st.residual = h_ctl[0].residual;
+    return status;
+}
+#undef M3D_CAP
+
 int m3d_solver::dispatch_run(double tol_field, double tol_eq, int nInc, int criterion, int max_iter) {
     if (max_iter <= 0) max_iter = (kind == M3D_KIND_MECH) ? 2000 : 500;
     if (kind == M3D_KIND_MECH && behav != M3D_BEHAV_ELASTIC) {
@@ -770,10 +1013,19 @@ int m3d_solver::dispatch_run(double tol_field, double tol_eq, int nInc, int crit
         if (prec == M3D_PREC_FP64) return run_inelastic<double, 6>(tol_field, tol_eq, nInc, criterion, max_iter);
         return run_inelastic<float, 6>(tol_field, tol_eq, nInc, criterion, max_iter);
     }
+    const bool graph = use_graph && !prof;  // per-sweep event timing needs the host-driven loop
     if (prec == M3D_PREC_FP32_REFINE) {
         if (criterion != M3D_CRIT_RESIDUAL)
             return fail(M3D_ERR_UNSUPPORTED, "FP32 refinement stops on the residual criterion only");
+        if (graph) return C == 6 ? run_refine_graph<6>(tol_field, max_iter) : run_refine_graph<3>(tol_field, max_iter);
         return C == 6 ? run_refine<6>(tol_field, max_iter) : run_refine<3>(tol_field, max_iter);
+    }
+    if (graph) {
+        if (prec == M3D_PREC_FP64)
+            return C == 6 ? run_linear_graph<double, 6>(tol_field, tol_eq, criterion, max_iter)
+                          : run_linear_graph<double, 3>(tol_field, tol_eq, criterion, max_iter);
+        return C == 6 ? run_linear_graph<float, 6>(tol_field, tol_eq, criterion, max_iter)
+                      : run_linear_graph<float, 3>(tol_field, tol_eq, criterion, max_iter);
     }
     if (prec == M3D_PREC_FP64)
         return C == 6 ? run_linear<double, 6>(tol_field, tol_eq, criterion, max_iter)
@@ -907,6 +1159,8 @@ static int create_impl(int kind, int Nx, int Ny, int Nz, int behav, int precisio
     {
         const char* e2 = std::getenv("M3D_GENERIC_FFT");
         h->use_fast = !(e2 && e2[0] == '1');
+        const char* e3 = std::getenv("M3D_NO_GRAPH");
+        h->use_graph = !(e3 && e3[0] == '1');
     }
     int rc = h->alloc(batch);
     if (rc) { cudaStreamDestroy(h->stream); delete h; return rc; }
