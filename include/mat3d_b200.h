@@ -109,6 +109,10 @@ int m3d_create(int kind, int Nx, int Ny, int Nz, int behav, int precision, int b
    RVEs (6 or 3 load cases each) and writes nrve consecutive tensors. */
 int m3d_create_multi(int kind, int Nx, int Ny, int Nz, int precision, int nrve, int nload, m3d_solver** out);
 int m3d_destroy(m3d_solver* h);
+/* Device bytes a solver of this shape holds (nrve RVEs, batch entries in all;
+   m3d_create: nrve = 1), without the lazily allocated field-export buffer.
+   -1 for invalid arguments.  Used for admission by HBM footprint. */
+long long m3d_footprint_bytes(int kind, int Nx, int Ny, int Nz, int behav, int precision, int nrve, int batch);
 
 /* Phase properties, rows [E, nu, sigma_y, H, n, P, Y0] (row-major nph x 7), and
    the phase id of every voxel (0 <= id < nph, at most 16 phases). */
@@ -177,6 +181,36 @@ int m3d_get_profile(const m3d_solver* h, m3d_profile* out);
 int m3d_thermal_solve_noalloc(int Nx, int Ny, int Nz, double km, double ki, const uint8_t* d_phase,
                               const double* E, double tol, int max_iter, double* d_grad, int* iters_out,
                               double* residual_out, void* stream);
+
+/* ---- batched homogenization of many RVEs (no counterpart in the reference,
+   which homogenizes one RVE per object, src/3d/FFT_analysis3D.cpp:856-903) --
+   RVEs of any grid sizes are added, then m3d_batch_homogenize gives each its
+   effective tensor, as m3d_homogenize would for it alone (residual stop rule).
+   RVEs of one grid size run together as one multi-RVE solve (all their load
+   cases in one graph launch), split only where the device-memory budget
+   requires. */
+typedef struct m3d_batch m3d_batch;
+typedef struct {
+    long long sweeps, sweeps_fp64, sweeps_fp32;  /* summed over all entries (RVE x load case) */
+    long long voxel_iters;   /* sum over entries of voxels x sweeps */
+    double device_ms;        /* device time of the solves (events around each launch's homogenize) */
+    double wall_ms;          /* wall time of m3d_batch_homogenize, host staging included */
+    int rves;                /* RVEs homogenized */
+    int groups;              /* distinct grid sizes */
+    int launches;            /* multi-RVE solves (groups x memory chunks) */
+    long long kernel_launches;
+} m3d_batch_stats;
+/* mem_budget_bytes <= 0: 85% of the free device memory at creation. */
+int m3d_batch_create(int kind, int precision, double mem_budget_bytes, m3d_batch** out);
+int m3d_batch_add_mech(m3d_batch* b, int Nx, int Ny, int Nz, const double* mat, int nph, const int32_t* phase,
+                       int scheme, int* index);
+int m3d_batch_add_thermal(m3d_batch* b, int Nx, int Ny, int Nz, double km, double ki, const int32_t* phase,
+                          int scheme, int* index);
+/* Ceff, Seff: one C x C block per added RVE, in the order of addition. */
+int m3d_batch_homogenize(m3d_batch* b, double tol_field, int max_iter, double* Ceff, double* Seff);
+int m3d_batch_get_stats(const m3d_batch* b, m3d_batch_stats* out);
+int m3d_batch_clear(m3d_batch* b);
+int m3d_batch_destroy(m3d_batch* b);
 
 /* The CUDA stream (cudaStream_t) all work of the handle is ordered on.
    m3d_set_stream replaces it with a caller-owned stream (NULL: the handle's own). */

@@ -61,6 +61,13 @@ class Stats(ctypes.Structure):
         return d
 
 
+class BatchStats(ctypes.Structure):
+    _fields_ = [("sweeps", ctypes.c_longlong), ("sweeps_fp64", ctypes.c_longlong),
+                ("sweeps_fp32", ctypes.c_longlong), ("voxel_iters", ctypes.c_longlong),
+                ("device_ms", ctypes.c_double), ("wall_ms", ctypes.c_double), ("rves", ctypes.c_int),
+                ("groups", ctypes.c_int), ("launches", ctypes.c_int), ("kernel_launches", ctypes.c_longlong)]
+
+
 class Profile(ctypes.Structure):
     _fields_ = [("ms_fp64", ctypes.c_double), ("n_fp64", ctypes.c_longlong),
                 ("ms_fp32", ctypes.c_double), ("n_fp32", ctypes.c_longlong)]
@@ -74,7 +81,9 @@ EXPORTS = [
     "m3d_homogenize", "m3d_get_field", "m3d_get_means", "m3d_get_stats", "m3d_get_increments",
     "m3d_status_string", "m3d_last_error", "m3d_abi_version", "m3d_get_stream", "m3d_set_stream",
     "m3d_set_profiling", "m3d_get_profile", "m3d_thermal_solve_noalloc",
-    "m3d_create_multi", "m3d_set_material_mech_rve", "m3d_set_material_thermal_rve",
+    "m3d_create_multi", "m3d_set_material_mech_rve", "m3d_set_material_thermal_rve", "m3d_footprint_bytes",
+    "m3d_batch_create", "m3d_batch_add_mech", "m3d_batch_add_thermal", "m3d_batch_homogenize",
+    "m3d_batch_get_stats", "m3d_batch_clear", "m3d_batch_destroy",
 ]
 
 
@@ -104,7 +113,7 @@ def load_library(path: str | None = None):
     L.m3d_last_error.restype = ctypes.c_char_p
     L.m3d_abi_version.restype = i
     for name in EXPORTS:
-        if name not in ("m3d_status_string", "m3d_last_error", "m3d_get_stream"):
+        if name not in ("m3d_status_string", "m3d_last_error", "m3d_get_stream", "m3d_footprint_bytes"):
             getattr(L, name).restype = ctypes.c_int
     L.m3d_get_stream.restype = vp
     L.m3d_get_stream.argtypes = [vp]
@@ -114,6 +123,15 @@ def load_library(path: str | None = None):
     L.m3d_create_multi.argtypes = [i, i, i, i, i, i, i, ctypes.POINTER(vp)]
     L.m3d_set_material_mech_rve.argtypes = [vp, i, vp, i, vp, i]
     L.m3d_set_material_thermal_rve.argtypes = [vp, i, d, d, vp, i]
+    L.m3d_footprint_bytes.argtypes = [i, i, i, i, i, i, i, i]
+    L.m3d_footprint_bytes.restype = ctypes.c_longlong
+    L.m3d_batch_create.argtypes = [i, i, d, ctypes.POINTER(vp)]
+    L.m3d_batch_add_mech.argtypes = [vp, i, i, i, vp, i, vp, i, ctypes.POINTER(ctypes.c_int)]
+    L.m3d_batch_add_thermal.argtypes = [vp, i, i, i, d, d, vp, i, ctypes.POINTER(ctypes.c_int)]
+    L.m3d_batch_homogenize.argtypes = [vp, d, i, vp, vp]
+    L.m3d_batch_get_stats.argtypes = [vp, ctypes.POINTER(BatchStats)]
+    L.m3d_batch_clear.argtypes = [vp]
+    L.m3d_batch_destroy.argtypes = [vp]
     L.m3d_set_profiling.argtypes = [vp, i]
     L.m3d_get_profile.argtypes = [vp, ctypes.POINTER(Profile)]
     if path is None:
@@ -227,6 +245,71 @@ class Solver:
         out = np.zeros((max(n, 1), 9))
         rows = self.L.m3d_get_increments(self.h, _ptr(out), n)
         return out[:rows]
+
+
+def footprint_bytes(kind, shape, behav=ELASTIC, precision=FP64, nrve=1, batch=1):
+    """Device bytes a solver of this shape holds (admission by HBM footprint)."""
+    L = load_library()
+    return int(L.m3d_footprint_bytes(kind, *shape, behav, _PRECISIONS[precision], nrve, batch))
+
+
+class Batch:
+    """Many RVEs of mixed grid sizes homogenized together (m3d_batch_*)."""
+
+    def __init__(self, kind, precision=FP32_REFINE, mem_budget_bytes=0.0):
+        self.L = load_library()
+        self.kind = kind
+        self.C = 6 if kind == KIND_MECH else 3
+        self.n = 0
+        h = ctypes.c_void_p()
+        _check(self.L, self.L.m3d_batch_create(kind, _PRECISIONS[precision], float(mem_budget_bytes),
+                                               ctypes.byref(h)), "batch_create")
+        self.h = h
+
+    def add_mech(self, shape, mat, phase, scheme=SCHEME_AUTO):
+        mat = np.ascontiguousarray(mat, np.float64)
+        ph = np.ascontiguousarray(np.asarray(phase).ravel(), np.int32)
+        idx = ctypes.c_int()
+        _check(self.L, self.L.m3d_batch_add_mech(self.h, *shape, _ptr(mat), mat.shape[0], _ptr(ph), scheme,
+                                                 ctypes.byref(idx)), "batch_add")
+        self.n += 1
+        return idx.value
+
+    def add_thermal(self, shape, km, ki, phase, scheme=SCHEME_AUTO):
+        ph = np.ascontiguousarray(np.asarray(phase).ravel(), np.int32)
+        idx = ctypes.c_int()
+        _check(self.L, self.L.m3d_batch_add_thermal(self.h, *shape, float(km), float(ki), _ptr(ph), scheme,
+                                                    ctypes.byref(idx)), "batch_add")
+        self.n += 1
+        return idx.value
+
+    def homogenize(self, tol_field, max_iter=0):
+        C = self.C
+        Ce = np.zeros((self.n, C, C))
+        Se = np.zeros((self.n, C, C))
+        rc = _check(self.L, self.L.m3d_batch_homogenize(self.h, tol_field, max_iter, _ptr(Ce), _ptr(Se)),
+                    "batch_homogenize")
+        return Ce, Se, rc
+
+    def stats(self):
+        st = BatchStats()
+        _check(self.L, self.L.m3d_batch_get_stats(self.h, ctypes.byref(st)), "batch_stats")
+        return {k: getattr(st, k) for k, _ in st._fields_}
+
+    def clear(self):
+        _check(self.L, self.L.m3d_batch_clear(self.h), "batch_clear")
+        self.n = 0
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.m3d_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def _iso_C(la, mu):

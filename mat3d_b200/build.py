@@ -22,7 +22,8 @@ NVCC_FLAGS = [
     "-Xcompiler", "-fPIC", "-shared",
 ]
 
-SOURCES = [os.path.join(CSRC, "solver.cu"), os.path.join(CSRC, "noalloc.cu"), os.path.join(CSRC, "compat.cpp")]
+SOURCES = [os.path.join(CSRC, "solver.cu"), os.path.join(CSRC, "noalloc.cu"), os.path.join(CSRC, "compat.cpp"),
+           os.path.join(CSRC, "batch.cpp")]
 DEPS = SOURCES + [os.path.join(CSRC, f) for f in os.listdir(CSRC)] + [
     os.path.join(ROOT, "include", f) for f in os.listdir(os.path.join(ROOT, "include"))]
 

@@ -1199,6 +1199,24 @@ int m3d_create(int kind, int Nx, int Ny, int Nz, int behav, int precision, int b
     return create_impl(kind, Nx, Ny, Nz, behav, precision, 1, batch, out);
 }
 
+long long m3d_footprint_bytes(int kind, int Nx, int Ny, int Nz, int behav, int precision, int nrve, int batch) {
+    if (Nx < 2 || Ny < 2 || Nz < 2 || nrve < 1 || batch < nrve || precision < 0 || precision > 2) return -1;
+    const long long C = (kind == M3D_KIND_MECH) ? 6 : 3;
+    const long long V = (long long)Nx * Ny * Nz, NL = (long long)Nx * Ny, Hzp = even_up(Nz / 2 + 1);
+    const long long B = batch;
+    const long long xw = (precision == M3D_PREC_FP32) ? 4 : 8, sw = (precision == M3D_PREC_FP32) ? 8 : 16;
+    long long b = nrve * V                                          // phase maps
+                  + nrve * (4 * kMaxPhases * C * C + kMaxPhases * C) * 8  // table blocks
+                  + (long long)(Nx + Ny + Nz) * 24                 // twiddles
+                  + B * C * V * xw + B * C * NL * Hzp * sw          // state, half spectrum
+                  + std::max(std::max(NL / 2 + 1, (long long)Ny * Hzp), 1024LL) * B * 16 * 8  // partials
+                  + B * (2 * (long long)sizeof(Ctl) + 4) + 64;
+    if (precision == M3D_PREC_FP32_REFINE) b += 2 * B * C * V * 4;  // correction + defect
+    if (kind == M3D_KIND_MECH && behav != M3D_BEHAV_ELASTIC)
+        b += B * V * xw * (18 + (behav == M3D_BEHAV_J2 ? 7 : 1));   // eps, sig, eps_old (+ sig_old, ep | d)
+    return b;
+}
+
 int m3d_create_multi(int kind, int Nx, int Ny, int Nz, int precision, int nrve, int nload, m3d_solver** out) {
     if (nrve < 1 || nrve > 4096) return fail(M3D_ERR_ARG, "nrve must be in [1, 4096]");
     if (nload < 1 || nload > 6) return fail(M3D_ERR_ARG, "nload must be in [1, 6]");

@@ -36,7 +36,10 @@ def _paint_ellipsoid(grid, center, axes_mat, semi, phase=0):
     loc = d @ np.asarray(axes_mat, np.float64).T
     q = (loc[..., 0] / semi[0]) ** 2 + (loc[..., 1] / semi[1]) ** 2 + (loc[..., 2] / semi[2]) ** 2
     m = q <= 1.0
-    grid[X[m] % N[0], Y[m] % N[1], Z[m] % N[2]] = phase
+    flat = np.unique(np.ravel_multi_index((X[m] % N[0], Y[m] % N[1], Z[m] % N[2]), N))
+    changed = int(np.count_nonzero(grid.ravel()[flat] != phase))
+    grid.ravel()[flat] = phase
+    return changed
 
 
 def spheres_rsa(N, radius=6.0, vf=0.20, seed=0, gap=1.0, max_tries=200000, radii_fn=None):
@@ -46,25 +49,40 @@ def spheres_rsa(N, radius=6.0, vf=0.20, seed=0, gap=1.0, max_tries=200000, radii
     Nx, Ny, Nz = (N, N, N) if np.isscalar(N) else tuple(N)
     rng = np.random.default_rng(seed)
     grid = np.ones((Nx, Ny, Nz), np.int32)
-    centers, radii = [], []
+    box = np.array([Nx, Ny, Nz], np.float64)
+    cs = np.zeros((0, 3))
+    rs = np.zeros(0)
+    n_inc = 0  # inclusion voxels, kept up to date as spheres are painted
     tries = 0
-    while np.count_nonzero(grid == 0) / grid.size < vf and tries < max_tries:
+    while n_inc / grid.size < vf and tries < max_tries:
         tries += 1
         r = float(radii_fn(rng)) if radii_fn else float(radius)
-        c = rng.uniform(0, 1, 3) * np.array([Nx, Ny, Nz])
-        ok = True
-        for c2, r2 in zip(centers, radii):
-            d = _periodic_delta(c, c2, np.array([Nx, Ny, Nz]))
-            if np.dot(d, d) < (r + r2 + gap) ** 2:
-                ok = False
-                break
-        if not ok:
-            continue
-        centers.append(c)
-        radii.append(r)
-        _paint_ellipsoid(grid, c, np.eye(3), (r, r, r))
-    meta = dict(n_inclusions=len(centers), vf=float(np.count_nonzero(grid == 0) / grid.size), seed=seed)
+        c = rng.uniform(0, 1, 3) * box
+        if len(rs):
+            d = _periodic_delta(c[None, :], cs, box)
+            if np.any(np.einsum("ij,ij->i", d, d) < (r + rs + gap) ** 2):
+                continue
+        cs = np.vstack([cs, c])
+        rs = np.append(rs, r)
+        n_inc += _paint_ellipsoid(grid, c, np.eye(3), (r, r, r))
+    meta = dict(n_inclusions=len(rs), vf=float(np.count_nonzero(grid == 0) / grid.size), seed=seed)
     return grid, meta
+
+
+def penetrable_spheres(N, radius, vf, seed=0, max_spheres=100000):
+    """Overlapping (penetrable) spheres of one radius at uniform random
+    periodic centres, added until the inclusion fraction reaches ``vf``; any
+    fraction is reachable (non-overlapping placement jams near 38%)."""
+    Nx, Ny, Nz = (N, N, N) if np.isscalar(N) else tuple(N)
+    rng = np.random.default_rng(seed)
+    grid = np.ones((Nx, Ny, Nz), np.int32)
+    box = np.array([Nx, Ny, Nz], np.float64)
+    n_inc, n = 0, 0
+    while n_inc / grid.size < vf and n < max_spheres:
+        c = rng.uniform(0, 1, 3) * box
+        n_inc += _paint_ellipsoid(grid, c, np.eye(3), (radius, radius, radius))
+        n += 1
+    return grid, dict(n_inclusions=n, vf=float(n_inc / grid.size), seed=seed, radius=radius)
 
 
 def _random_rotation(rng):
@@ -124,8 +142,10 @@ def batch_rves(count=512, sizes=(32, 48, 64, 96), seed0=0, vf_range=(0.05, 0.40)
 
 
 def batch_member(seed, N, vf, contrast):
+    """RVE ``seed`` of the batched workload: penetrable spheres of radius N/10
+    to inclusion fraction ``vf``; inclusion E = contrast * 3 GPa, nu 0.2."""
     r = max(2.0, N / 10.0)
-    g, meta = spheres_rsa(N, radius=r, vf=vf, seed=seed, gap=1.0)
+    g, meta = penetrable_spheres(N, radius=r, vf=vf, seed=seed)
     mat = np.array([[contrast * 3e9, 0.2, 1e30, 0, 1, 0, 1e30], [3e9, 0.35, 1e30, 0, 1, 0, 1e30]])
     return g, mat, meta
 

@@ -143,3 +143,60 @@ def test_multi_rejects_unset_rve_and_bad_index():
     with pytest.raises(m3d.M3DError):
         mb.set_material_mech(mech_mat(10.0), sphere_rve(shape, 2.0), rve=2)
     mb.close()
+
+
+# ---- m3d_batch_*: mixed grid sizes, memory-budget chunking ------------------
+def _batch_members(kind, n=7):
+    out = []
+    for i in range(n):
+        N = (12, 16, 20)[i % 3]
+        shape = (N, N, N)
+        rve = sphere_rve(shape, 0.22 * N + 0.3 * (i % 2), (N / 2 + i % 3, N / 2, N / 2 - i % 2))
+        if kind == m3d.KIND_MECH:
+            out.append((shape, mech_mat(2.0 + 15 * i, stiff_matrix=(i % 4 == 3)), rve))
+        else:
+            out.append((shape, (1.0, 2.0 + 20 * i) if i % 2 else (30.0 + i, 1.0), rve))
+    return out
+
+
+@pytest.mark.parametrize("kind,prec", [(m3d.KIND_MECH, "fp32_refine"), (m3d.KIND_MECH, "fp64"),
+                                       (m3d.KIND_THERMAL, "fp32_refine")])
+@pytest.mark.parametrize("budget_rves", [0, 1])
+def test_batch_api_equals_single(kind, prec, budget_rves):
+    """Every tensor of a mixed-size batch equals m3d_homogenize on its RVE alone;
+    a budget of one RVE of the largest grid forces several launches per size."""
+    members = _batch_members(kind)
+    C = 6 if kind == m3d.KIND_MECH else 3
+    budget = 0.0
+    if budget_rves:
+        budget = float(m3d.footprint_bytes(kind, (20, 20, 20), 0, prec, budget_rves, budget_rves * C))
+    bt = m3d.Batch(kind, prec, budget)
+    for shape, mat, rve in members:
+        if kind == m3d.KIND_MECH:
+            bt.add_mech(shape, mat, rve)
+        else:
+            bt.add_thermal(shape, mat[0], mat[1], rve)
+    Ce, Se, _ = bt.homogenize(1e-9)
+    st = bt.stats()
+    assert st["rves"] == len(members) and st["groups"] == 3
+    assert (st["launches"] >= 5) if budget_rves else (st["launches"] == 3)
+    assert st["voxel_iters"] > 0 and st["device_ms"] > 0
+    for i, (shape, mat, rve) in enumerate(members):
+        s1 = m3d.Solver(kind, *shape, 0, prec, C)
+        if kind == m3d.KIND_MECH:
+            s1.set_material_mech(mat, rve)
+        else:
+            s1.set_material_thermal(mat[0], mat[1], rve)
+        C1, S1, *_ = s1.homogenize(1e-9, 0, m3d.CRIT_RESIDUAL)
+        assert np.array_equal(Ce[i], C1), (i, np.abs(Ce[i] - C1).max())
+        assert np.array_equal(Se[i], S1)
+        s1.close()
+    bt.close()
+
+
+def test_batch_budget_too_small():
+    bt = m3d.Batch(m3d.KIND_MECH, "fp64", 1e6)
+    bt.add_mech((16, 16, 16), mech_mat(10.0), sphere_rve((16, 16, 16), 3.0))
+    with pytest.raises(m3d.M3DError):
+        bt.homogenize(1e-8)
+    bt.close()
