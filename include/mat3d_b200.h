@@ -62,7 +62,8 @@ typedef enum {
     M3D_ERR_NAN = 5,           /* non-finite residual */
     M3D_ERR_STATE = 6,         /* call order violated (e.g. run before material) */
     M3D_ERR_UNSUPPORTED = 7,   /* valid request this build does not provide */
-    M3D_ERR_TIMEOUT = 8        /* a bounded device wait expired */
+    M3D_ERR_TIMEOUT = 8,       /* a bounded device wait expired */
+    M3D_PENDING = 9            /* serving: the request has not finished yet */
 } m3d_status;
 
 enum { M3D_KIND_MECH = 1, M3D_KIND_THERMAL = 2 };
@@ -211,6 +212,65 @@ int m3d_batch_homogenize(m3d_batch* b, double tol_field, int max_iter, double* C
 int m3d_batch_get_stats(const m3d_batch* b, m3d_batch_stats* out);
 int m3d_batch_clear(m3d_batch* b);
 int m3d_batch_destroy(m3d_batch* b);
+
+/* ---- serving (no counterpart in the reference) ------------------------------
+   A device-resident request loop: requests of any kind, behaviour, grid and
+   precision are submitted from any host thread; worker threads admit them
+   as soon as a worker is free and their device footprint fits the memory
+   budget (idle solvers of other shapes are released to make room), each on
+   its own CUDA stream so the solves of different requests overlap on the
+   device.  Finished solvers stay resident (buffers, twiddles, captured
+   graphs) and are reused by the next request of the same shape.  A request
+   gives the result it would give alone: each runs on its own solver. */
+typedef struct m3d_server m3d_server;
+typedef struct {
+    int kind;             /* M3D_KIND_MECH / M3D_KIND_THERMAL */
+    int behav;            /* M3D_BEHAV_* (mech) */
+    int Nx, Ny, Nz;
+    int precision;        /* M3D_PREC_*; J2/damage: FP64 or FP32 */
+    const double* mat;    /* mech: nph x 7 rows as m3d_set_material_mech */
+    int nph;
+    double km, ki;        /* thermal conductivities */
+    const int32_t* phase; /* Nx*Ny*Nz phase ids */
+    int scheme;           /* M3D_SCHEME_* */
+    const double* E;      /* load: 6 (mech) or 3 (thermal) values */
+    const double* X0;     /* J2/damage stress direction (6), else NULL */
+    int nInc;             /* J2/damage increments (>= 1) */
+    double tol;           /* residual tolerance (M3D_CRIT_RESIDUAL) */
+    int max_iter;         /* <= 0: the reference's caps */
+    int keep_field;       /* 1: keep the strain field for m3d_serve_get_field */
+} m3d_request;
+typedef struct {
+    int status;                  /* m3d_status of the solve */
+    int iters;                   /* sweeps of the (last) solve */
+    long long sweeps;            /* all sweeps (FP32 + FP64) */
+    double residual;
+    double strain_mean[6], stress_mean[6];
+    double queue_ms;             /* submit -> admitted */
+    double solve_ms;             /* admitted -> finished */
+    double latency_ms;           /* submit -> finished */
+} m3d_result;
+typedef struct {
+    long long submitted, completed, failed;
+    int queued, running, peak_running;
+    int resident_solvers;        /* solvers held (running + idle) */
+    double resident_bytes, budget_bytes;
+} m3d_serve_stats;
+/* mem_budget_bytes <= 0: 85% of the free device memory; workers: concurrent solves. */
+int m3d_serve_create(double mem_budget_bytes, int workers, m3d_server** out);
+/* Copies the request's arrays; thread safe.  ticket > 0 identifies it. */
+int m3d_serve_submit(m3d_server* s, const m3d_request* req, long long* ticket);
+/* M3D_OK and *out filled once finished (the result is then released unless
+   keep_field asked for the field), M3D_PENDING before, M3D_ERR_ARG for an
+   unknown ticket. */
+int m3d_serve_poll(m3d_server* s, long long ticket, m3d_result* out);
+/* Blocks up to timeout_ms (< 0: no limit); M3D_PENDING on timeout. */
+int m3d_serve_wait(m3d_server* s, long long ticket, double timeout_ms, m3d_result* out);
+/* AoS strain field (c values per voxel) of a finished keep_field request; releases it. */
+int m3d_serve_get_field(m3d_server* s, long long ticket, double* out);
+int m3d_serve_get_stats(m3d_server* s, m3d_serve_stats* out);
+/* Finishes the queued and running requests, then frees every solver. */
+int m3d_serve_destroy(m3d_server* s);
 
 /* The CUDA stream (cudaStream_t) all work of the handle is ordered on.
    m3d_set_stream replaces it with a caller-owned stream (NULL: the handle's own). */

@@ -33,7 +33,7 @@ FP64, FP32, FP32_REFINE = 0, 1, 2
 CRIT_REFERENCE, CRIT_RESIDUAL = 0, 1
 SCHEME_AUTO, SCHEME_PRIMAL, SCHEME_DUAL = 0, 1, 2
 FIELD_STRAIN, FIELD_STRESS, FIELD_EPS_P, FIELD_DAMAGE = 0, 1, 2, 3
-OK, NOT_CONVERGED = 0, 4
+OK, NOT_CONVERGED, PENDING = 0, 4, 9
 
 _PRECISIONS = {"fp64": FP64, "fp32": FP32, "fp32_refine": FP32_REFINE, FP64: FP64, FP32: FP32, FP32_REFINE: FP32_REFINE}
 _BEHAV = {"e": ELASTIC, "ep": J2, "ed": DAMAGE}
@@ -68,6 +68,34 @@ class BatchStats(ctypes.Structure):
                 ("groups", ctypes.c_int), ("launches", ctypes.c_int), ("kernel_launches", ctypes.c_longlong)]
 
 
+class Request(ctypes.Structure):
+    _fields_ = [("kind", ctypes.c_int), ("behav", ctypes.c_int), ("Nx", ctypes.c_int), ("Ny", ctypes.c_int),
+                ("Nz", ctypes.c_int), ("precision", ctypes.c_int), ("mat", ctypes.c_void_p), ("nph", ctypes.c_int),
+                ("km", ctypes.c_double), ("ki", ctypes.c_double), ("phase", ctypes.c_void_p),
+                ("scheme", ctypes.c_int), ("E", ctypes.c_void_p), ("X0", ctypes.c_void_p), ("nInc", ctypes.c_int),
+                ("tol", ctypes.c_double), ("max_iter", ctypes.c_int), ("keep_field", ctypes.c_int)]
+
+
+class Result(ctypes.Structure):
+    _fields_ = [("status", ctypes.c_int), ("iters", ctypes.c_int), ("sweeps", ctypes.c_longlong),
+                ("residual", ctypes.c_double), ("strain_mean", ctypes.c_double * 6),
+                ("stress_mean", ctypes.c_double * 6), ("queue_ms", ctypes.c_double),
+                ("solve_ms", ctypes.c_double), ("latency_ms", ctypes.c_double)]
+
+    def as_dict(self):
+        d = {k: getattr(self, k) for k, _ in self._fields_}
+        d["strain_mean"] = np.array(self.strain_mean[:])
+        d["stress_mean"] = np.array(self.stress_mean[:])
+        return d
+
+
+class ServeStats(ctypes.Structure):
+    _fields_ = [("submitted", ctypes.c_longlong), ("completed", ctypes.c_longlong), ("failed", ctypes.c_longlong),
+                ("queued", ctypes.c_int), ("running", ctypes.c_int), ("peak_running", ctypes.c_int),
+                ("resident_solvers", ctypes.c_int), ("resident_bytes", ctypes.c_double),
+                ("budget_bytes", ctypes.c_double)]
+
+
 class Profile(ctypes.Structure):
     _fields_ = [("ms_fp64", ctypes.c_double), ("n_fp64", ctypes.c_longlong),
                 ("ms_fp32", ctypes.c_double), ("n_fp32", ctypes.c_longlong)]
@@ -84,6 +112,8 @@ EXPORTS = [
     "m3d_create_multi", "m3d_set_material_mech_rve", "m3d_set_material_thermal_rve", "m3d_footprint_bytes",
     "m3d_batch_create", "m3d_batch_add_mech", "m3d_batch_add_thermal", "m3d_batch_homogenize",
     "m3d_batch_get_stats", "m3d_batch_clear", "m3d_batch_destroy",
+    "m3d_serve_create", "m3d_serve_submit", "m3d_serve_poll", "m3d_serve_wait", "m3d_serve_get_field",
+    "m3d_serve_get_stats", "m3d_serve_destroy",
 ]
 
 
@@ -132,6 +162,13 @@ def load_library(path: str | None = None):
     L.m3d_batch_get_stats.argtypes = [vp, ctypes.POINTER(BatchStats)]
     L.m3d_batch_clear.argtypes = [vp]
     L.m3d_batch_destroy.argtypes = [vp]
+    L.m3d_serve_create.argtypes = [d, i, ctypes.POINTER(vp)]
+    L.m3d_serve_submit.argtypes = [vp, ctypes.POINTER(Request), ctypes.POINTER(ctypes.c_longlong)]
+    L.m3d_serve_poll.argtypes = [vp, ctypes.c_longlong, ctypes.POINTER(Result)]
+    L.m3d_serve_wait.argtypes = [vp, ctypes.c_longlong, d, ctypes.POINTER(Result)]
+    L.m3d_serve_get_field.argtypes = [vp, ctypes.c_longlong, vp]
+    L.m3d_serve_get_stats.argtypes = [vp, ctypes.POINTER(ServeStats)]
+    L.m3d_serve_destroy.argtypes = [vp]
     L.m3d_set_profiling.argtypes = [vp, i]
     L.m3d_get_profile.argtypes = [vp, ctypes.POINTER(Profile)]
     if path is None:
@@ -303,6 +340,72 @@ class Batch:
     def close(self):
         if getattr(self, "h", None):
             self.L.m3d_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Server:
+    """Device-resident serving loop (m3d_serve_*): submit RVE solves from any
+    thread, poll or wait for their results."""
+
+    def __init__(self, mem_budget_bytes=0.0, workers=8):
+        self.L = load_library()
+        h = ctypes.c_void_p()
+        _check(self.L, self.L.m3d_serve_create(float(mem_budget_bytes), workers, ctypes.byref(h)), "serve_create")
+        self.h = h
+        self.fields = {}
+
+    def submit(self, kind, shape, phase, E, *, mat=None, km=0.0, ki=0.0, behav=ELASTIC, precision=FP32_REFINE,
+               scheme=SCHEME_AUTO, X0=None, nInc=1, tol=1e-6, max_iter=0, keep_field=False):
+        ph = np.ascontiguousarray(np.asarray(phase).ravel(), np.int32)
+        Ea = np.ascontiguousarray(E, np.float64)
+        ma = None if mat is None else np.ascontiguousarray(mat, np.float64)
+        Xa = None if X0 is None else np.ascontiguousarray(X0, np.float64)
+        r = Request(kind, behav, *shape, _PRECISIONS[precision], _ptr(ma), 0 if ma is None else ma.shape[0],
+                    float(km), float(ki), _ptr(ph), scheme, _ptr(Ea), _ptr(Xa), nInc, float(tol), max_iter,
+                    1 if keep_field else 0)
+        t = ctypes.c_longlong()
+        _check(self.L, self.L.m3d_serve_submit(self.h, ctypes.byref(r), ctypes.byref(t)), "serve_submit")
+        if keep_field:
+            self.fields[t.value] = (6 if kind == KIND_MECH else 3, int(np.prod(shape)))
+        return t.value
+
+    def poll(self, ticket):
+        r = Result()
+        rc = self.L.m3d_serve_poll(self.h, ticket, ctypes.byref(r))
+        if rc == PENDING:
+            return None
+        _check(self.L, rc, "serve_poll")
+        return r.as_dict()
+
+    def wait(self, ticket, timeout_ms=-1.0):
+        r = Result()
+        rc = self.L.m3d_serve_wait(self.h, ticket, float(timeout_ms), ctypes.byref(r))
+        if rc == PENDING:
+            return None
+        _check(self.L, rc, "serve_wait")
+        return r.as_dict()
+
+    def field(self, ticket):
+        """(c, V) strain field of a finished keep_field request (released after the call)."""
+        c, V = self.fields.pop(ticket)
+        out = np.zeros(c * V)
+        _check(self.L, self.L.m3d_serve_get_field(self.h, ticket, _ptr(out)), "serve_get_field")
+        return out.reshape(V, c).T
+
+    def stats(self):
+        st = ServeStats()
+        _check(self.L, self.L.m3d_serve_get_stats(self.h, ctypes.byref(st)), "serve_stats")
+        return {k: getattr(st, k) for k, _ in st._fields_}
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.m3d_serve_destroy(self.h)
             self.h = None
 
     def __del__(self):

@@ -15,6 +15,7 @@
 #include <cstring>
 #include <cstdlib>
 #include <mutex>
+#include <set>
 #include <string>
 #include <vector>
 
@@ -134,8 +135,17 @@ std::vector<typename Cx<T>::t> twiddles(int n) {
 
 // Let a kernel use all dynamic shared memory left next to its static arrays
 // (227 KB per block on sm_100 in total).
+// Done once per kernel and device; safe to call from several host threads.
+std::mutex g_attr_mu;
+std::set<std::pair<int, const void*>> g_attr_done;
 template <class K>
 void allow_smem(K kernel) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    {
+        std::lock_guard<std::mutex> lk(g_attr_mu);
+        if (!g_attr_done.insert(std::make_pair(dev, (const void*)kernel)).second) return;
+    }
     cudaFuncAttributes a;
     if (cudaFuncGetAttributes(&a, kernel) == cudaSuccess) {
         const int maxdyn = 227 * 1024 - (int)a.sharedSizeBytes;
@@ -520,8 +530,7 @@ void m3d_solver::pass_zfwd(Pro pro, Ctl* ctl, typename Cx<T>::t* sp) {
     const bool done = use_fast && with_fast_n(Nz, [&](auto nc) {
         constexpr int NN = decltype(nc)::value;
         typedef ZTile<T, NN, CC> Z;
-        static bool init = false;
-        if (!init) { allow_smem(k_zfwd_fast<T, NN, CC, Pro>); init = true; }
+        allow_smem(k_zfwd_fast<T, NN, CC, Pro>);
         const int blk = (int)((g.NL + Z::G - 1) / Z::G);
         k_zfwd_fast<T, NN, CC, Pro><<<dim3(blk, B), kFastThreads, z_fast_smem<T, NN, CC>(extra), stream>>>(
             g, tw<T>(2), sp, pro, ctl);
@@ -530,8 +539,7 @@ void m3d_solver::pass_zfwd(Pro pro, Ctl* ctl, typename Cx<T>::t* sp) {
         const int Gl = G<T>();
         const int zblk = (int)((g.NL + Gl - 1) / Gl);
         const size_t zsmem = (size_t)Nz * sizeof(C2) + 2 * (size_t)(Gl / 2) * CC * Nz * sizeof(C2) + 16 + 32 * 32 * 8 + extra;
-        static bool init = false;
-        if (!init) { allow_smem(k_zfwd<T, CC, Pro>); init = true; }
+        allow_smem(k_zfwd<T, CC, Pro>);
         k_zfwd<T, CC, Pro><<<dim3(zblk, B), 256, zsmem, stream>>>(g, pz, tw<T>(2), sp, pro, ctl, Gl, d_part);
     }
     st.kernel_launches += 1;
@@ -546,12 +554,8 @@ void m3d_solver::pass_y(int sign, int CC, Ctl* ctl, typename Cx<T>::t* sp) {
         const int ntz = (g.Hzp + 4 * CPW - 1) / (4 * CPW);
         const dim3 grid(Nx * ntz, CC * B);
         const size_t sm = ypass_fast_smem<T, NN>();
-        static bool init = false;
-        if (!init) {
-            allow_smem(k_ypass_fast<T, NN, -1>);
-            allow_smem(k_ypass_fast<T, NN, +1>);
-            init = true;
-        }
+        allow_smem(k_ypass_fast<T, NN, -1>);
+        allow_smem(k_ypass_fast<T, NN, +1>);
         if (sign < 0) k_ypass_fast<T, NN, -1><<<grid, kFastThreads, sm, stream>>>(g, tw<T>(1), sp, CC, ctl);
         else k_ypass_fast<T, NN, +1><<<grid, kFastThreads, sm, stream>>>(g, tw<T>(1), sp, CC, ctl);
     });
@@ -559,8 +563,7 @@ void m3d_solver::pass_y(int sign, int CC, Ctl* ctl, typename Cx<T>::t* sp) {
         const int tzy = TZy<T>();
         const size_t ysmem = (size_t)Ny * sizeof(C2) + 2 * (size_t)Ny * tzy * sizeof(C2);
         const int ntzy = (g.Hzp + tzy - 1) / tzy;
-        static bool init = false;
-        if (!init) { allow_smem(k_ypass<T>); init = true; }
+        allow_smem(k_ypass<T>);
         k_ypass<T><<<dim3(Nx * ntzy, CC * B), 256, ysmem, stream>>>(g, py, tw<T>(1), sp, tzy, CC, sign, ctl);
     }
     st.kernel_launches += 1;
@@ -576,8 +579,7 @@ int m3d_solver::pass_x(Spec op, Ctl* ctl, typename Cx<T>::t* sp) {
         constexpr int CPW = 32 / LineSplit<T, NN>::Tl;
         const int ntz = (g.Hzp + WPC * CPW - 1) / (WPC * CPW);
         nblk = Ny * ntz;
-        static bool init = false;
-        if (!init) { allow_smem(k_xturn_fast<T, NN, CC, Spec>); init = true; }
+        allow_smem(k_xturn_fast<T, NN, CC, Spec>);
         k_xturn_fast<T, NN, CC, Spec><<<dim3(nblk, B), WPC * 32, xturn_fast_smem<T, NN, CC, Spec::NSUM>(), stream>>>(
             g, tw<T>(0), sp, op, ctl, d_part);
     });
@@ -586,8 +588,7 @@ int m3d_solver::pass_x(Spec op, Ctl* ctl, typename Cx<T>::t* sp) {
         const size_t xsmem = (size_t)Nx * sizeof(C2) + 2 * (size_t)CC * Nx * tzx * sizeof(C2) + 16 + 32 * 32 * 8;
         const int ntzx = (g.Hzp + tzx - 1) / tzx;
         nblk = Ny * ntzx;
-        static bool init = false;
-        if (!init) { allow_smem(k_xturn<T, CC, Spec>); init = true; }
+        allow_smem(k_xturn<T, CC, Spec>);
         k_xturn<T, CC, Spec><<<dim3(nblk, B), 256, xsmem, stream>>>(g, px, tw<T>(0), sp, tzx, op, ctl, d_part);
     }
     st.kernel_launches += 1;
@@ -603,8 +604,7 @@ int m3d_solver::pass_zinv(Epi epi, Ctl* ctl, typename Cx<T>::t* sp, Fin fin) {
         constexpr int NN = decltype(nc)::value;
         typedef ZTile<T, NN, CC> Z;
         nblk = (int)((g.NL + Z::G - 1) / Z::G);
-        static bool init = false;
-        if (!init) { allow_smem(k_zinv_fast<T, NN, CC, Epi, Fin>); init = true; }
+        allow_smem(k_zinv_fast<T, NN, CC, Epi, Fin>);
         k_zinv_fast<T, NN, CC, Epi, Fin><<<dim3(nblk, B), kFastThreads, zinv_fast_smem<T, NN, CC>(extra), stream>>>(
             g, tw<T>(2), sp, epi, ctl, d_part, fin);
     });
@@ -612,8 +612,7 @@ int m3d_solver::pass_zinv(Epi epi, Ctl* ctl, typename Cx<T>::t* sp, Fin fin) {
         const int Gl = G<T>();
         nblk = (int)((g.NL + Gl - 1) / Gl);
         const size_t zsmem = (size_t)Nz * sizeof(C2) + 2 * (size_t)(Gl / 2) * CC * Nz * sizeof(C2) + 16 + 32 * 32 * 8 + extra;
-        static bool init = false;
-        if (!init) { allow_smem(k_zinv<T, CC, Epi, Fin>); init = true; }
+        allow_smem(k_zinv<T, CC, Epi, Fin>);
         k_zinv<T, CC, Epi, Fin><<<dim3(nblk, B), 256, zsmem, stream>>>(g, pz, tw<T>(2), sp, epi, ctl, Gl, d_part, fin);
     }
     st.kernel_launches += 1;
@@ -1101,6 +1100,7 @@ const char* m3d_status_string(int s) {
         case M3D_ERR_STATE: return "call order violated";
         case M3D_ERR_UNSUPPORTED: return "unsupported";
         case M3D_ERR_TIMEOUT: return "device wait timed out";
+        case M3D_PENDING: return "pending";
         default: return "unknown status";
     }
 }

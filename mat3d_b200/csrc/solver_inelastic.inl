@@ -179,12 +179,8 @@ int m3d_solver::run_inelastic(double tol_field, double tol_eq, int nInc, int cri
     const size_t phb = (size_t)nph * sizeof(PhaseMech) + 64;
     const int cblk = 592;
     const size_t csmem = 32 * 32 * 8 + phb;
-    static bool init = false;
-    if (!init) {
-        allow_smem(k_constitutive<T>);
-        allow_smem(k_commit<T>);
-        init = true;
-    }
+    allow_smem(k_constitutive<T>);
+    allow_smem(k_commit<T>);
     prop.assign((size_t)nInc * 9, 0.0);
     long long total = 0;
     int nx = 0, done_inc = nInc, status = M3D_OK;
