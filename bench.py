@@ -22,6 +22,13 @@ Workloads (synthetic, seeded; the reference project has no dataset):
               nu .2; matrix 3 GPa, .35); 6 unit load cases each -> full C_eff;
               FP32 sweeps + FP64 refinement to residual 1e-6; one graph launch
               per grid size (a step is the whole batch)
+  serve       Poisson arrivals of elastic, thermal and J2 solves (1/3 each), N
+              log-uniform on [32, 256] rounded to the nearest of {32, 48, 64, 96,
+              128, 256} in log scale; elastic as elastic64 (FP32+refine), thermal
+              as thermal128 (FP32+refine), J2 as the 256^3 J2 workload with 5
+              increments to 0.5% (FP32); residual 1e-6.  Capacity is measured
+              with a closed burst first, then offered loads of 0.25x..1.5x that
+              capacity are replayed; p50/p99 latency and throughput per load
 Multi-GPU: replicas only (one independent solve, or batch, per rank), weak scaling.
 """
 from __future__ import annotations
@@ -55,8 +62,14 @@ WORKLOADS = {
                        tol=1e-8, desc="128^3 thermal, 30% ellipsoids (3a,a,a) random orientation, k 100:1, grad z"),
     "elastic64": dict(kind="mech", N=64, E=[1e-3, 0, 0, 0, 0, 0], precision="fp64", tol=1e-6,
                       desc="64^3 elastic, spheres r=6 at 20%, E 70/3 GPa, eps_xx=1e-3"),
+    "j2_256": dict(kind="mech", behav="ep", N=256, E=[1e-3, 0, 0, 0, 0, 0], X0=[1, 0, 0, 0, 0, 0], nInc=20,
+                   precision="fp32", tol=1e-6,
+                   desc="256^3 J2 (E 70 GPa, nu .33, sy 100 MPa, H 1 GPa) with 15% elastic particles (400 GPa, .2), "
+                        "log-normal radii 3-10, 20 increments to 2% uniaxial"),
     "batch512": dict(kind="batch", count=512, precision="fp32_refine", tol=1e-6,
                      desc="512 RVEs N in {32,48,64,96}, vf 5-40%, contrast 2-100, 6 load cases each, full C_eff"),
+    "serve": dict(kind="serve", per_level=24, levels=(0.25, 0.5, 1.0, 1.5), tol=1e-6, workers=8,
+                  desc="Poisson mix of elastic/thermal/J2 solves, N log-uniform 32..256 (rounded), residual 1e-6"),
 }
 
 
@@ -64,6 +77,8 @@ def make_rve(w, seed=0):
     from mat3d_b200 import rve
     if w["kind"] == "thermal":
         g, meta = rve.ellipsoids(w["N"], vf=0.30, aspect=3.0, n_target=100, seed=seed)
+    elif w.get("behav") == "ep":
+        g, meta = rve.lognormal_spheres(w["N"], vf=0.15, median=5.0, sigma=0.4, rmin=3.0, rmax=10.0, seed=seed)
     else:
         g, meta = rve.spheres_rsa(w["N"], radius=6.0, vf=0.20, seed=seed)
     return g.ravel().astype(np.int32), meta
@@ -141,16 +156,19 @@ def cpu_reference(w, steps, warmup, threads):
         t0 = time.perf_counter()
         if w["kind"] == "thermal":
             r = ref.therm_run((N, N, N), w["km"], w["ki"], rve, np.array(w["E"]), 1e30, 1e30)
+        elif w.get("behav") == "ep":
+            r = ref.mech_run((N, N, N), "ep", MAT_J2, rve, np.array(w["E"], float), np.array(w["X0"], float),
+                             1e30, 1e30, 1, 0)
         else:
-            mat = np.array([[70e9, 0.2, 1e30, 0, 1, 0, 1e30], [3e9, 0.35, 1e30, 0, 1, 0, 1e30]])
-            r = ref.mech_run((N, N, N), "e", mat, rve, np.array(w["E"], float), np.zeros(6), 1e30, 1e30, 1, 0)
+            r = ref.mech_run((N, N, N), "e", MAT_ELASTIC, rve, np.array(w["E"], float), np.zeros(6), 1e30, 1e30, 1, 0)
         dt = time.perf_counter() - t0
         if i >= warmup:
             sweeps_all += r["sweeps"]
             secs += dt
             vals.append(V * r["sweeps"] / dt)
+    what = "first increment of the " if w.get("behav") == "ep" else ""
     return dict(value=V * sweeps_all / secs, sweeps=sweeps_all, seconds=secs,
-                sample=f"{steps} x reference solve of the full {N}^3 workload stopped after "
+                sample=f"{steps} x reference solve of the {what}full {N}^3 workload stopped after "
                        f"{sweeps_all // max(steps, 1)} sweeps (set-up included), FP64")
 
 
@@ -338,6 +356,124 @@ def run_batch(args, w, rank, world, local):
         print(json.dumps(line))
 
 
+SERVE_SIZES = (32, 48, 64, 96, 128, 256)
+MAT_ELASTIC = np.array([[70e9, 0.2, 1e30, 0, 1, 0, 1e30], [3e9, 0.35, 1e30, 0, 1, 0, 1e30]])
+MAT_J2 = np.array([[400e9, 0.2, 1e30, 0, 1, 0, 1e30], [70e9, 0.33, 100e6, 1e9, 1, 0, 1e30]])
+
+
+def serve_requests(n, seed):
+    """n request descriptors (kind, N) of the serving mix, seeded."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(n):
+        kind = ("elastic", "thermal", "j2")[rng.integers(3)]
+        x = np.exp(rng.uniform(np.log(32), np.log(256)))
+        N = min(SERVE_SIZES, key=lambda s: abs(np.log(s) - np.log(x)))
+        out.append((kind, N))
+    return out
+
+
+def run_serve(args, w, rank, world, local):
+    """Serving: a step is one offered-load level of the sweep."""
+    import torch
+
+    import mat3d_b200 as m3d
+    from mat3d_b200 import rve as R
+
+    cache = {}
+
+    def template(kind, N):
+        if (kind, N) not in cache:
+            if kind == "thermal":
+                g, _ = R.ellipsoids(N, vf=0.30, aspect=3.0, n_target=100, seed=N)
+            elif kind == "elastic":
+                g, _ = R.spheres_rsa(N, radius=6.0, vf=0.20, seed=N)
+            else:
+                g, _ = R.lognormal_spheres(N, vf=0.15, median=5.0, sigma=0.4, rmin=3.0, rmax=10.0, seed=N)
+            cache[(kind, N)] = g.ravel().astype(np.int32)
+        return cache[(kind, N)]
+
+    def submit(srv, kind, N):
+        ph = template(kind, N)
+        if kind == "thermal":
+            return srv.submit(m3d.KIND_THERMAL, (N,) * 3, ph, [0, 0, 1.0], km=1.0, ki=100.0,
+                              precision="fp32_refine", tol=w["tol"])
+        if kind == "elastic":
+            return srv.submit(m3d.KIND_MECH, (N,) * 3, ph, [1e-3, 0, 0, 0, 0, 0], mat=MAT_ELASTIC,
+                              precision="fp32_refine", tol=w["tol"])
+        return srv.submit(m3d.KIND_MECH, (N,) * 3, ph, [0.005 / 5, 0, 0, 0, 0, 0], mat=MAT_J2, behav=m3d.J2,
+                          X0=[1, 0, 0, 0, 0, 0], nInc=5, precision="fp32", tol=w["tol"])
+
+    t0 = time.perf_counter()
+    for kind in ("elastic", "thermal", "j2"):
+        for N in SERVE_SIZES:
+            template(kind, N)
+    gen_s = time.perf_counter() - t0
+    srv = m3d.Server(workers=w["workers"])
+    # warm-up: every (kind, N) once, so solvers and graphs exist (resident)
+    warm = [submit(srv, k, N) for k in ("elastic", "thermal", "j2") for N in SERVE_SIZES][: max(args.warmup, 1) * 18]
+    for t in warm:
+        srv.wait(t)
+    vox = lambda N: N ** 3
+
+    def replay(descs, rate):
+        """Submit descs with exponential inter-arrival times (rate req/s; inf: all at once)."""
+        rng = np.random.default_rng(len(descs) + int(rate if np.isfinite(rate) else 0))
+        torch.cuda.synchronize()
+        start = time.perf_counter()
+        tickets, t_next = [], start
+        for kind, N in descs:
+            if np.isfinite(rate):
+                t_next += rng.exponential(1.0 / rate)
+                dt = t_next - time.perf_counter()
+                if dt > 0:
+                    time.sleep(dt)
+            tickets.append(submit(srv, kind, N))
+        res = [srv.wait(t) for t in tickets]
+        span = time.perf_counter() - start
+        lat = np.array([r["latency_ms"] for r in res])
+        vi = sum(vox(N) * r["sweeps"] for (k, N), r in zip(descs, res))
+        bad = sum(1 for r in res if r["status"] not in (m3d.OK, m3d.NOT_CONVERGED))
+        return dict(span_s=span, p50_ms=float(np.percentile(lat, 50)), p99_ms=float(np.percentile(lat, 99)),
+                    mean_ms=float(lat.mean()), req_per_s=len(descs) / span, voxel_iters_per_s=vi / span,
+                    failed=bad, n=len(descs))
+
+    descs = serve_requests(w["per_level"], seed=1000 + rank)
+    clk = ClockSampler(local)
+    clk.start()
+    burst = replay(descs, float("inf"))
+    cap = burst["req_per_s"]
+    levels = []
+    for f in w["levels"][: max(args.steps, 1)]:
+        d = serve_requests(w["per_level"], seed=2000 + int(100 * f) + rank)
+        r = replay(d, f * cap)
+        r.update(offered_x_capacity=f, offered_req_per_s=f * cap)
+        levels.append(r)
+    clocks = clk.stop()
+    st = srv.stats()
+    srv.close()
+    if rank == 0:
+        top = levels[-1] if levels else burst
+        line = {
+            "metric": "serving p50/p99 latency at residual 1e-6 (and voxel-iters/s)", "value": top["p99_ms"],
+            "unit": "ms (p99 latency)", "n_gpus": world, "steps": len(levels), "warmup": len(warm),
+            "ms_per_step": 1000 * top["span_s"], "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32+f64", "data": "synthetic",
+            "config": {"workload": args.workload, "desc": w["desc"], "requests_per_level": w["per_level"],
+                       "sizes": list(SERVE_SIZES), "rounding": "N log-uniform on [32,256], nearest size in log scale",
+                       "j2": "5 increments to 0.5% strain, FP32 sweeps", "workers": w["workers"],
+                       "template_generation_s": gen_s, "parallelism": f"replicas x{world}"},
+            "serving": {"capacity_burst": burst, "levels": levels, "peak_running": st["peak_running"],
+                        "resident_solvers": st["resident_solvers"]},
+            "e2e": {"value": top["voxel_iters_per_s"], "unit": UNIT,
+                    "h2d_bytes_per_step": sum(4 * N ** 3 for _, N in descs),
+                    "d2h_bytes_per_step": len(descs) * 12 * 8},
+            "gpu_launches": None,
+            "clocks": clocks,
+        }
+        print(json.dumps(line))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -366,8 +502,8 @@ def main():
     if world > 1:
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=120))
-    if w["kind"] == "batch":
-        run_batch(args, w, rank, world, local)
+    if w["kind"] in ("batch", "serve"):
+        (run_batch if w["kind"] == "batch" else run_serve)(args, w, rank, world, local)
         if world > 1:
             dist.destroy_process_group()
         return
@@ -376,17 +512,20 @@ def main():
     V = N ** 3
     c = 3 if w["kind"] == "thermal" else 6
     rve, meta = make_rve(w, seed=rank)
-    mat = np.array([[70e9, 0.2, 1e30, 0, 1, 0, 1e30], [3e9, 0.35, 1e30, 0, 1, 0, 1e30]])
+    j2 = w.get("behav") == "ep"
+    mat = MAT_J2 if j2 else MAT_ELASTIC
     E = np.array(w["E"], float)
+    X0 = np.array(w["X0"], float) if "X0" in w else None
+    nInc = w.get("nInc", 1)
 
     def make_solver(prec):
         if w["kind"] == "thermal":
             s = m3d.Solver(m3d.KIND_THERMAL, N, N, N, m3d.ELASTIC, prec, 1)
             s.set_material_thermal(w["km"], w["ki"], rve)
         else:
-            s = m3d.Solver(m3d.KIND_MECH, N, N, N, m3d.ELASTIC, prec, 1)
+            s = m3d.Solver(m3d.KIND_MECH, N, N, N, m3d.J2 if j2 else m3d.ELASTIC, prec, 1)
             s.set_material_mech(mat, rve)
-        s.set_load(E)
+        s.set_load(E, X0)
         return s
 
     def barrier():
@@ -415,8 +554,8 @@ def main():
         for _ in range(warmup):
             if e2e:
                 s.set_material_thermal(w["km"], w["ki"], rve) if w["kind"] == "thermal" else s.set_material_mech(mat, rve)
-            s.set_load(E)
-            s.run(w["tol"], 0.0, 1, m3d.CRIT_RESIDUAL)
+            s.set_load(E, X0)
+            s.run(w["tol"], w["tol"], nInc, m3d.CRIT_RESIDUAL)
             if e2e:
                 host_out[:] = s.field(m3d.FIELD_STRAIN)
         if profile:
@@ -432,8 +571,8 @@ def main():
                     s.set_material_thermal(w["km"], w["ki"], rve)
                 else:
                     s.set_material_mech(mat, rve)
-            s.set_load(E)
-            s.run(w["tol"], 0.0, 1, m3d.CRIT_RESIDUAL)
+            s.set_load(E, X0)
+            s.run(w["tol"], w["tol"], nInc, m3d.CRIT_RESIDUAL)
             if e2e:
                 host_out[:] = s.field(m3d.FIELD_STRAIN)
             st = s.stats()
@@ -481,7 +620,8 @@ def main():
     else:
         peak, peak_src = 6650.0, "fallback"
     pr = pres["prof"]
-    b32, b64 = bytes_per_vi(c, 4), bytes_per_vi(c, 8)
+    # J2 adds the previous strain and stress and the plastic strain: 8cw + w + 1
+    b32, b64 = (8 * c * 4 + 4 + 1, 8 * c * 8 + 8 + 1) if j2 else (bytes_per_vi(c, 4), bytes_per_vi(c, 8))
     # whole timed region: algorithmic bytes of all its sweeps / its device time
     alg_bytes = V * (res["n32"] * b32 + res["n64"] * b64)
     achieved = alg_bytes / (res["ms"] / 1000.0) / 1e9 if res["ms"] > 0 else None
