@@ -120,6 +120,18 @@ struct EpiConstitutive {
     static constexpr int NSUM = 13;
     InelasticPtrs<T> p;
     PhaseMech* sm;
+    // entry-bound base pointers (bind)
+    T *eb = nullptr, *sb = nullptr, *db = nullptr;
+    const T *eob = nullptr, *sob = nullptr, *epb = nullptr;
+    __device__ __forceinline__ void bind(int b) {
+        const long long o6 = (long long)b * 6 * p.V, o1 = (long long)b * p.V;
+        eb = p.eps + o6;
+        sb = p.sig + o6;
+        eob = p.eps_old ? p.eps_old + o6 : nullptr;
+        sob = p.sig_old ? p.sig_old + o6 : nullptr;
+        epb = p.ep ? p.ep + o1 : nullptr;
+        db = p.dmg ? p.dmg + o1 : nullptr;
+    }
     __device__ __forceinline__ void load_smem(char* s, int = 0) {
         sm = (PhaseMech*)s;
         const double* src = (const double*)p.ph;
@@ -128,38 +140,36 @@ struct EpiConstitutive {
         for (int i = threadIdx.x; i < n; i += blockDim.x) dst[i] = src[i];
     }
     // xc: increment from the inverse transform (zero for the standalone update)
-    __device__ __forceinline__ void apply(int b, long long v, const T (&xc)[6], double* acc) const {
+    __device__ __forceinline__ void apply(int, long long v, const T (&xc)[6], double* acc) const {
         const int k = p.phase[v];
         const PhaseMech& P = sm[k];
+        const long long V = p.V;
         double e[6], sg[6];
         double dd = 0;
 #pragma unroll
         for (int c = 0; c < 6; ++c) {
-            const long long idx = ((long long)b * 6 + c) * p.V + v;
             const double inc = (double)xc[c];
-            e[c] = (double)p.eps[idx] + inc;
+            e[c] = (double)eb[c * V + v] + inc;
             dd += ((c >= 3) ? 2.0 : 1.0) * inc * inc;
         }
         if (p.behav == BEHAV_J2) {
             double eo[6], so[6];
 #pragma unroll
             for (int c = 0; c < 6; ++c) {
-                const long long idx = ((long long)b * 6 + c) * p.V + v;
-                eo[c] = (double)p.eps_old[idx];
-                so[c] = (double)p.sig_old[idx];
+                eo[c] = (double)eob[c * V + v];
+                so[c] = (double)sob[c * V + v];
             }
             double phi;
-            j2_update(P, e, eo, so, (double)p.ep[(long long)b * p.V + v], sg, phi, p.nr_fail);
+            j2_update(P, e, eo, so, (double)epb[v], sg, phi, p.nr_fail);
         } else {
-            double d = (double)p.dmg[(long long)b * p.V + v];
+            double d = (double)db[v];
             damage_update(P, e, d, sg);
-            p.dmg[(long long)b * p.V + v] = (T)d;
+            db[v] = (T)d;
         }
 #pragma unroll
         for (int c = 0; c < 6; ++c) {
-            const long long idx = ((long long)b * 6 + c) * p.V + v;
-            p.eps[idx] = (T)e[c];
-            p.sig[idx] = (T)sg[c];
+            eb[c * V + v] = (T)e[c];
+            sb[c * V + v] = (T)sg[c];
             acc[c] += sg[c];
             acc[6 + c] += e[c];
         }
@@ -173,14 +183,16 @@ struct ProStress {
     static constexpr int NSUM = 0;
     const T* sig;
     long long V;
+    const T* sb = nullptr;
     struct Pre {
         T s[6];
     };
+    __device__ __forceinline__ void bind(int b) { sb = sig + (long long)b * 6 * V; }
     __device__ __forceinline__ void load_smem(char*, int = 0) {}
-    __device__ __forceinline__ Pre load(int b, long long v) const {
+    __device__ __forceinline__ Pre load(int, long long v) const {
         Pre q;
 #pragma unroll
-        for (int c = 0; c < 6; ++c) q.s[c] = sig[((long long)b * 6 + c) * V + v];
+        for (int c = 0; c < 6; ++c) q.s[c] = sb[c * V + v];
         return q;
     }
     __device__ __forceinline__ void eval_pre(const Pre& q, int, long long, T (&out)[6]) const {
@@ -213,6 +225,7 @@ struct EpiBasic {
     static constexpr bool kPrefetch = false;  // 19 values per voxel: loaded at use
     EpiConstitutive<T> c;
     struct Pre {};
+    __device__ __forceinline__ void bind(int b) { c.bind(b); }
     __device__ __forceinline__ Pre load(int, long long) const { return Pre{}; }
     __device__ __forceinline__ void apply_pre(const Pre&, int b, long long v, T (&xc)[6], double* acc) const {
         c.apply(b, v, xc, acc);
@@ -228,6 +241,7 @@ __global__ void k_constitutive(EpiConstitutive<T> epi, const Ctl* ctl, double* p
     if (ctl[b].done) return;
     extern __shared__ __align__(16) char smem_raw[];
     double* red = (double*)smem_raw;
+    epi.bind(b);
     epi.load_smem(smem_raw + 32 * 32 * sizeof(double));
     __syncthreads();
     double acc[13] = {};

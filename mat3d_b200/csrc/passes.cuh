@@ -127,6 +127,7 @@ __global__ void __launch_bounds__(256) k_zfwd(GridDims g, LinePlan pz, const typ
     double* red = (double*)extra;
     extra += 32 * 32 * sizeof(double);
     for (int i = threadIdx.x; i < Nz; i += blockDim.x) tw[i] = twz[i];
+    pro.bind(b);
     pro.load_smem(extra, b);
     __syncthreads();
 
@@ -292,6 +293,7 @@ __global__ void __launch_bounds__(256) k_zinv(GridDims g, LinePlan pz, const typ
     double* red = (double*)extra;
     extra += 32 * 32 * sizeof(double);
     for (int i = threadIdx.x; i < Nz; i += blockDim.x) tw[i] = twz[i];
+    epi.bind(b);
     epi.load_smem(extra, b);
     const long long l0 = (long long)blockIdx.x * G;
     for (int i = threadIdx.x; i < nl * Hz; i += blockDim.x) {

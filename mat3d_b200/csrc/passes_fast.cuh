@@ -259,9 +259,32 @@ constexpr size_t z_fast_smem(size_t extra) {
     return (size_t)N * sizeof(C2) + (size_t)Z::SLOTS * Z::ROW * sizeof(C2) + 16 + 32 * 16 * sizeof(double) + extra;
 }
 
+// half-spectrum row length as stored: N/2 + 1 modes rounded up to even (the
+// grid's Hzp for Nz = N), so pairs of modes are 16-byte (FP32) aligned
+template <int N> struct HzOf {
+    static constexpr int Hz = N / 2 + 1, Hzp = (Hz + 1) & ~1, P2 = Hzp / 2;
+};
+
 template <typename T, int N, int C>
 constexpr size_t zinv_fast_smem(size_t extra) {
-    return z_fast_smem<T, N, C>(extra) + (size_t)ZTile<T, N, C>::G * C * (N / 2 + 1) * sizeof(typename Cx<T>::t);
+    return z_fast_smem<T, N, C>(extra) + 16 + (size_t)ZTile<T, N, C>::G * C * HzOf<N>::Hzp * sizeof(typename Cx<T>::t);
+}
+
+// two consecutive modes to global memory (one 16-byte store for FP32)
+__device__ __forceinline__ void store_pair(float2* p, float2 a, float2 b) {
+    *reinterpret_cast<float4*>(p) = make_float4(a.x, a.y, b.x, b.y);
+}
+__device__ __forceinline__ void store_pair(double2* p, double2 a, double2 b) {
+    p[0] = a;
+    p[1] = b;
+}
+// asynchronous copy of two consecutive modes (zero-filled when !ok)
+__device__ __forceinline__ void cp_async_pair(float2* dst, const float2* src, bool ok) {
+    cp_async(dst, src, 16, ok ? 16 : 0);
+}
+__device__ __forceinline__ void cp_async_pair(double2* dst, const double2* src, bool ok) {
+    cp_async(dst, src, 16, ok ? 16 : 0);
+    cp_async(dst + 1, src + 1, 16, ok ? 16 : 0);
 }
 
 // transform the tile's complex lines in place (FWD: natural order in,
@@ -304,6 +327,7 @@ __global__ void __launch_bounds__(kFastThreads) k_zfwd_fast(GridDims g, const ty
     typedef ZTile<T, N, C> Z;
     const int b = blockIdx.y;
     if (ctl[b].done) return;
+    pro.bind(b);
     extern __shared__ __align__(16) char smem_raw[];
     C2* tw = (C2*)smem_raw;
     C2* tile = tw + N;
@@ -342,22 +366,29 @@ __global__ void __launch_bounds__(kFastThreads) k_zfwd_fast(GridDims g, const ty
     __syncthreads();
     z_tile_fft<C2, N, Z::E, Z::TL, Z::SLOTS, Z::ROW, Z::SW, true>(tile, tw);
     __syncthreads();
-    const int Hz = g.Hz, Hzp = g.Hzp;
-    for (int i = threadIdx.x; i < Z::G * C * Hzp; i += blockDim.x) {
-        const int k = i % Hzp, gc = i / Hzp;
+    // split into the C half spectra, two modes per thread and store
+    constexpr int Hz = HzOf<N>::Hz, Hzp = HzOf<N>::Hzp, P2 = HzOf<N>::P2;
+    C2* ob = spec + ((long long)b * C * g.NL + l0) * Hzp;
+    const long long cst = g.NL * (long long)Hzp;
+    for (int i = threadIdx.x; i < Z::G * C * P2; i += kFastThreads) {
+        const int k2 = i % P2, gc = i / P2;
         const int gi = gc / C, c = gc - gi * C;
-        const long long l = l0 + gi;
-        if (l >= g.NL) continue;
-        C2 out = mk<C2>(0, 0);
-        if (k < Hz) {
-            const int rw = gi * Z::NCL + c / 2, sw = (rw & 1) * Z::SW;
-            const C2* row = tile + rw * Z::ROW;
-            const C2 Zk = row[k ^ sw];
-            const C2 Zm = row[(k == 0 ? 0 : N - k) ^ sw];
-            out = (c & 1) ? mk<C2>((T)0.5 * (Zk.y + Zm.y), (T)-0.5 * (Zk.x - Zm.x))
-                          : mk<C2>((T)0.5 * (Zk.x + Zm.x), (T)0.5 * (Zk.y - Zm.y));
+        if (l0 + gi >= g.NL) continue;
+        const int rw = gi * Z::NCL + c / 2, sw = (rw & 1) * Z::SW;
+        const C2* row = tile + rw * Z::ROW;
+        C2 o[2];
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int k = 2 * k2 + h;
+            o[h] = mk<C2>(0, 0);
+            if (k < Hz) {
+                const C2 Zk = row[k ^ sw];
+                const C2 Zm = row[(k == 0 ? 0 : N - k) ^ sw];
+                o[h] = (c & 1) ? mk<C2>((T)0.5 * (Zk.y + Zm.y), (T)-0.5 * (Zk.x - Zm.x))
+                               : mk<C2>((T)0.5 * (Zk.x + Zm.x), (T)0.5 * (Zk.y - Zm.y));
+            }
         }
-        spec[(((long long)b * C + c) * g.NL + l) * Hzp + k] = out;
+        store_pair(ob + c * cst + gi * Hzp + 2 * k2, o[0], o[1]);
     }
 }
 
@@ -369,23 +400,25 @@ __global__ void __launch_bounds__(kFastThreads) k_zinv_fast(GridDims g, const ty
     typedef ZTile<T, N, C> Z;
     const int b = blockIdx.y;
     if (ctl[b].done) return;
+    epi.bind(b);
     extern __shared__ __align__(16) char smem_raw[];
     C2* tw = (C2*)smem_raw;
     C2* tile = tw + N;
-    C2* raw = tile + Z::SLOTS * Z::ROW;  // [gi][c][k] half spectra as stored
-    double* red = (double*)align_up((char*)(raw + Z::G * C * (N / 2 + 1)), 16);
+    constexpr int Hz = HzOf<N>::Hz, Hzp = HzOf<N>::Hzp, P2 = HzOf<N>::P2;
+    C2* raw = (C2*)align_up((char*)(tile + Z::SLOTS * Z::ROW), 16);  // [gi][c][Hzp] half spectra as stored
+    double* red = (double*)align_up((char*)(raw + Z::G * C * Hzp), 16);
     char* extra = (char*)red + 32 * 16 * sizeof(double);
     const long long l0 = (long long)blockIdx.x * Z::G;
-    constexpr int Hz = N / 2 + 1;
-    const int Hzp = g.Hzp;
-    // asynchronous copies of the G x C half-spectrum rows (coalesced along kz)
-    for (int i = threadIdx.x; i < Z::G * C * Hz; i += kFastThreads) {
-        const int k = i % Hz, gc = i / Hz;
-        const int gi = gc / C, c = gc - gi * C;
-        const long long l = l0 + gi;
-        const bool okl = l < g.NL;
-        cp_async(raw + i, spec + (((long long)b * C + c) * g.NL + (okl ? l : 0)) * Hzp + k, (int)sizeof(C2),
-                 okl ? (int)sizeof(C2) : 0);
+    // asynchronous copies of the G x C half-spectrum rows, two modes per copy
+    {
+        const C2* ib = spec + ((long long)b * C * g.NL + l0) * Hzp;
+        const long long cst = g.NL * (long long)Hzp;
+        for (int i = threadIdx.x; i < Z::G * C * P2; i += kFastThreads) {
+            const int k2 = i % P2, gc = i / P2;
+            const int gi = gc / C, c = gc - gi * C;
+            const bool okl = l0 + gi < g.NL;
+            cp_async_pair(raw + gc * Hzp + 2 * k2, okl ? ib + c * cst + gi * Hzp + 2 * k2 : ib, okl);
+        }
     }
     // epilogue loads do not depend on the transform: issue them meanwhile
     typename Epi::Pre pre[Epi::kPrefetch ? Z::PER : 1];
@@ -404,8 +437,8 @@ __global__ void __launch_bounds__(kFastThreads) k_zinv_fast(GridDims g, const ty
     for (int i = threadIdx.x; i < Z::G * Z::NCL * Hz; i += kFastThreads) {
         const int k = i % Hz, gl = i / Hz;
         const int gi = gl / Z::NCL, cl = gl - gi * Z::NCL;
-        const C2 a = raw[(gi * C + 2 * cl) * Hz + k];
-        const C2 bb = (2 * cl + 1 < C) ? raw[(gi * C + 2 * cl + 1) * Hz + k] : mk<C2>(0, 0);
+        const C2 a = raw[(gi * C + 2 * cl) * Hzp + k];
+        const C2 bb = (2 * cl + 1 < C) ? raw[(gi * C + 2 * cl + 1) * Hzp + k] : mk<C2>(0, 0);
         C2* row = tile + gl * Z::ROW;
         const int sw = (gl & 1) * Z::SW;
         if (k == 0 || 2 * k == N) {

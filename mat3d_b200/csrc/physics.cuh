@@ -191,20 +191,28 @@ struct ProMat {
     T* sm;
     int lc = 0;             // batch entries per RVE (0: one RVE shared by all entries)
     long long mstride = 0;  // stride of an RVE's table block in `mats`
+    const uint8_t* phb = nullptr;  // phase map and state of the bound entry (bind)
+    const TX* xb = nullptr;
     struct Pre {
         int p;
         T xv[C];
     };
+    // per-block: address the entry's RVE and state once, so per-voxel loads
+    // are plain offsets
+    __device__ __forceinline__ void bind(int b) {
+        phb = phase + (lc ? (long long)(b / lc) * V : 0);
+        xb = x + (long long)b * C * V;
+    }
     __device__ __forceinline__ void load_smem(char* s, int b) {
         sm = (T*)s;
         const double* m = mats + (lc ? (long long)(b / lc) * mstride : 0);
         for (int i = threadIdx.x; i < nph * C * C; i += blockDim.x) sm[i] = (T)m[i];
     }
-    __device__ __forceinline__ Pre load(int b, long long v) const {
+    __device__ __forceinline__ Pre load(int, long long v) const {
         Pre q;
-        q.p = phase[(lc ? (long long)(b / lc) * V : 0) + v];
+        q.p = phb[v];
 #pragma unroll
-        for (int c = 0; c < C; ++c) q.xv[c] = (T)x[((long long)b * C + c) * V + v];
+        for (int c = 0; c < C; ++c) q.xv[c] = (T)xb[c * V + v];
         return q;
     }
     __device__ __forceinline__ void eval_pre(const Pre& q, int, long long, T (&out)[C]) const {
@@ -234,31 +242,38 @@ struct ProRefine64 {
     double* sm;
     int lc = 0;
     long long mstride = 0;
+    const uint8_t* phb = nullptr;
+    double* xb = nullptr;
+    const float* db = nullptr;
     struct Pre {
         int p;
         double xv[C];
     };
+    __device__ __forceinline__ void bind(int b) {
+        phb = phase + (lc ? (long long)(b / lc) * V : 0);
+        xb = x + (long long)b * C * V;
+        db = delta ? delta + (long long)b * C * V : nullptr;
+    }
     __device__ __forceinline__ void load_smem(char* s, int b) {
         sm = (double*)s;
         const double* m = mats + (lc ? (long long)(b / lc) * mstride : 0);
         for (int i = threadIdx.x; i < nph * C * C; i += blockDim.x) sm[i] = m[i];
     }
-    __device__ __forceinline__ Pre load(int b, long long v) const {
+    __device__ __forceinline__ Pre load(int, long long v) const {
         Pre q;
-        q.p = phase[(lc ? (long long)(b / lc) * V : 0) + v];
+        q.p = phb[v];
 #pragma unroll
         for (int c = 0; c < C; ++c) {
-            const long long idx = ((long long)b * C + c) * V + v;
-            q.xv[c] = x[idx];
-            if (delta) q.xv[c] += (double)delta[idx];
+            q.xv[c] = xb[c * V + v];
+            if (db) q.xv[c] += (double)db[c * V + v];
         }
         return q;
     }
-    __device__ __forceinline__ void eval_pre(const Pre& q, int b, long long v, double (&out)[C]) const {
+    __device__ __forceinline__ void eval_pre(const Pre& q, int, long long v, double (&out)[C]) const {
         const double* M = sm + q.p * C * C;
-        if (delta) {
+        if (db) {
 #pragma unroll
-            for (int c = 0; c < C; ++c) x[((long long)b * C + c) * V + v] = q.xv[c];
+            for (int c = 0; c < C; ++c) xb[c * V + v] = q.xv[c];
         }
 #pragma unroll
         for (int i = 0; i < C; ++i) {
@@ -291,29 +306,36 @@ struct EpiEM {
     T* sm;
     int lc = 0;
     long long mstride = 0;
+    const uint8_t* phb = nullptr;
+    T* xb = nullptr;
+    const float* rb = nullptr;
     struct Pre {
         int p;
         T xv[C];
         T rv[C];
     };
+    __device__ __forceinline__ void bind(int b) {
+        phb = phase + (lc ? (long long)(b / lc) * V : 0);
+        xb = x + (long long)b * C * V;
+        rb = r ? r + (long long)b * C * V : nullptr;
+    }
     __device__ __forceinline__ void load_smem(char* s, int b) {
         sm = (T*)s;
         const long long o = lc ? (long long)(b / lc) * mstride : 0;
         for (int i = threadIdx.x; i < nph * C * C; i += blockDim.x) sm[i] = (T)amats[o + i];
         for (int i = threadIdx.x; i < nph * C; i += blockDim.x) sm[nph * C * C + i] = (T)osum[o + i];
     }
-    __device__ __forceinline__ Pre load(int b, long long v) const {
+    __device__ __forceinline__ Pre load(int, long long v) const {
         Pre q;
-        q.p = phase[(lc ? (long long)(b / lc) * V : 0) + v];
+        q.p = phb[v];
 #pragma unroll
         for (int c = 0; c < C; ++c) {
-            const long long idx = ((long long)b * C + c) * V + v;
-            q.xv[c] = x[idx];
-            q.rv[c] = r ? (T)r[idx] : (T)0;
+            q.xv[c] = xb[c * V + v];
+            q.rv[c] = rb ? (T)rb[c * V + v] : (T)0;
         }
         return q;
     }
-    __device__ __forceinline__ void apply_pre(const Pre& q, int b, long long v, T (&xc)[C], double* acc) const {
+    __device__ __forceinline__ void apply_pre(const Pre& q, int, long long v, T (&xc)[C], double* acc) const {
         const T* Am = sm + q.p * C * C;
         const T* os = sm + nph * C * C + q.p * C;
         T d[C], xn[C];
@@ -328,7 +350,7 @@ struct EpiEM {
 #pragma unroll
             for (int j = 0; j < C; ++j) s += Am[i * C + j] * d[j];
             xn[i] = q.xv[i] + s;
-            x[((long long)b * C + i) * V + v] = xn[i];
+            xb[i * V + v] = xn[i];
         }
 #pragma unroll
         for (int c = 0; c < C; ++c) ot += (double)os[c] * (double)xn[c];
@@ -355,28 +377,36 @@ struct EpiDefect {
     double* sm;
     int lc = 0;
     long long mstride = 0;
+    const uint8_t* phb = nullptr;
+    const double* xb = nullptr;
+    float* rb = nullptr;
     struct Pre {
         int p;
         double xv[C];
     };
+    __device__ __forceinline__ void bind(int b) {
+        phb = phase + (lc ? (long long)(b / lc) * V : 0);
+        xb = x + (long long)b * C * V;
+        rb = r + (long long)b * C * V;
+    }
     __device__ __forceinline__ void load_smem(char* s, int b) {
         sm = (double*)s;
         const double* m = osum + (lc ? (long long)(b / lc) * mstride : 0);
         for (int i = threadIdx.x; i < nph * C; i += blockDim.x) sm[i] = m[i];
     }
-    __device__ __forceinline__ Pre load(int b, long long v) const {
+    __device__ __forceinline__ Pre load(int, long long v) const {
         Pre q;
-        q.p = phase[(lc ? (long long)(b / lc) * V : 0) + v];
+        q.p = phb[v];
 #pragma unroll
-        for (int c = 0; c < C; ++c) q.xv[c] = x[((long long)b * C + c) * V + v];
+        for (int c = 0; c < C; ++c) q.xv[c] = xb[c * V + v];
         return q;
     }
-    __device__ __forceinline__ void apply_pre(const Pre& q, int b, long long v, double (&xc)[C], double* acc) const {
+    __device__ __forceinline__ void apply_pre(const Pre& q, int, long long v, double (&xc)[C], double* acc) const {
         double rs = 0, ot = 0;
 #pragma unroll
         for (int c = 0; c < C; ++c) {
             const double d = xc[c] - q.xv[c];
-            r[((long long)b * C + c) * V + v] = (float)d;
+            rb[c * V + v] = (float)d;
             const double w = (C == 6 && c >= 3) ? 2.0 : 1.0;
             rs += w * d * d;
             ot += sm[q.p * C + c] * q.xv[c];
