@@ -181,6 +181,7 @@ struct EpiConstitutive {
 template <typename T>
 struct ProStress {
     static constexpr int NSUM = 0;
+    static constexpr int kW = 1;  // scalar loads only
     const T* sig;
     long long V;
     const T* sb = nullptr;
@@ -223,6 +224,7 @@ template <typename T>
 struct EpiBasic {
     static constexpr int NSUM = 13;
     static constexpr bool kPrefetch = false;  // 19 values per voxel: loaded at use
+    static constexpr int kW = 1;
     EpiConstitutive<T> c;
     struct Pre {};
     __device__ __forceinline__ void bind(int b) { c.bind(b); }

@@ -239,6 +239,10 @@ __global__ void __launch_bounds__(kFastThreads) k_xturn_fast(GridDims g, const t
 // ---------------------------------------------------------------------------
 template <int C> struct NclOf { static constexpr int value = (C + 1) / 2; };
 
+// per-thread prefetch record of an operator: four voxels (kW = 4) or one
+template <class Op, bool V = (Op::kW > 1)> struct PreOf { typedef typename Op::Pre type; };
+template <class Op> struct PreOf<Op, true> { typedef typename Op::PreW type; };
+
 template <typename T, int N, int C>
 struct ZTile {
     static constexpr int E = LineSplit<T, N>::E, TL = LineSplit<T, N>::Tl, LPW = 32 / TL;
@@ -333,34 +337,45 @@ __global__ void __launch_bounds__(kFastThreads) k_zfwd_fast(GridDims g, const ty
     C2* tile = tw + N;
     char* extra = align_up((char*)(tile + Z::SLOTS * Z::ROW), 16) + 32 * 16 * sizeof(double);
     const long long l0 = (long long)blockIdx.x * Z::G;
-    // all prologue loads first
-    typename Pro::Pre pre[Z::PER];
+    // all prologue loads first: W consecutive voxels per load (kW of the operator)
+    constexpr int W = Pro::kW;
+    constexpr int NV = Z::TOT / W, PERW = (NV + kFastThreads - 1) / kFastThreads;
+    typename PreOf<Pro>::type pre[PERW];
 #pragma unroll
-    for (int k = 0; k < Z::PER; ++k) {
-        const int i = threadIdx.x + k * kFastThreads;
+    for (int k = 0; k < PERW; ++k) {
+        const int i = (threadIdx.x + k * kFastThreads) * W;
         const int gi = i / N, z = i - gi * N;
-        if (i < Z::TOT && l0 + gi < g.NL) pre[k] = pro.load(b, (l0 + gi) * N + z);
+        if (i < Z::TOT && l0 + gi < g.NL) {
+            if constexpr (W > 1) pre[k] = pro.loadw((l0 + gi) * N + z);
+            else pre[k] = pro.load(b, (l0 + gi) * N + z);
+        }
     }
     for (int i = threadIdx.x; i < N; i += blockDim.x) tw[i] = twz[i];
     pro.load_smem(extra, b);
     __syncthreads();
 #pragma unroll
-    for (int k = 0; k < Z::PER; ++k) {
-        const int i = threadIdx.x + k * kFastThreads;
+    for (int k = 0; k < PERW; ++k) {
+        const int i = (threadIdx.x + k * kFastThreads) * W;
         if (i >= Z::TOT) break;
-        const int gi = i / N, z = i - gi * N;
+        const int gi = i / N, z0 = i - gi * N;
         const long long l = l0 + gi;
-        T val[C];
-        if (l < g.NL) {
-            pro.eval_pre(pre[k], b, l * N + z, val);
-        } else {
 #pragma unroll
-            for (int c = 0; c < C; ++c) val[c] = (T)0;
-        }
+        for (int w = 0; w < W; ++w) {
+            const int z = z0 + w;
+            T val[C];
+            if (l < g.NL) {
+                if constexpr (W > 1) pro.eval_prew(pre[k], w, val);
+                else pro.eval_pre(pre[k], b, l * N + z, val);
+            } else {
 #pragma unroll
-        for (int cl = 0; cl < Z::NCL; ++cl) {
-            const int rw = gi * Z::NCL + cl;
-            tile[rw * Z::ROW + (z ^ ((rw & 1) * Z::SW))] = mk<C2>(val[2 * cl], (2 * cl + 1 < C) ? val[2 * cl + 1] : (T)0);
+                for (int c = 0; c < C; ++c) val[c] = (T)0;
+            }
+#pragma unroll
+            for (int cl = 0; cl < Z::NCL; ++cl) {
+                const int rw = gi * Z::NCL + cl;
+                tile[rw * Z::ROW + (z ^ ((rw & 1) * Z::SW))] =
+                    mk<C2>(val[2 * cl], (2 * cl + 1 < C) ? val[2 * cl + 1] : (T)0);
+            }
         }
     }
     __syncthreads();
@@ -421,13 +436,18 @@ __global__ void __launch_bounds__(kFastThreads) k_zinv_fast(GridDims g, const ty
         }
     }
     // epilogue loads do not depend on the transform: issue them meanwhile
-    typename Epi::Pre pre[Epi::kPrefetch ? Z::PER : 1];
+    constexpr int W = Epi::kW;
+    constexpr int NV = Z::TOT / W, PERW = (NV + kFastThreads - 1) / kFastThreads;
+    typename PreOf<Epi>::type pre[Epi::kPrefetch ? PERW : 1];
     if constexpr (Epi::kPrefetch) {
 #pragma unroll
-        for (int k = 0; k < Z::PER; ++k) {
-            const int i = threadIdx.x + k * kFastThreads;
+        for (int k = 0; k < PERW; ++k) {
+            const int i = (threadIdx.x + k * kFastThreads) * W;
             const int gi = i / N, z = i - gi * N;
-            if (i < Z::TOT && l0 + gi < g.NL) pre[k] = epi.load(b, (l0 + gi) * N + z);
+            if (i < Z::TOT && l0 + gi < g.NL) {
+                if constexpr (W > 1) pre[k] = epi.loadw((l0 + gi) * N + z);
+                else pre[k] = epi.load(b, (l0 + gi) * N + z);
+            }
         }
     }
     for (int i = threadIdx.x; i < N; i += blockDim.x) tw[i] = twz[i];
@@ -454,22 +474,30 @@ __global__ void __launch_bounds__(kFastThreads) k_zinv_fast(GridDims g, const ty
     const T invV = (T)(1.0 / (double)g.V);
     double acc[Epi::NSUM > 0 ? Epi::NSUM : 1] = {};
 #pragma unroll
-    for (int k = 0; k < Z::PER; ++k) {
-        const int i = threadIdx.x + k * kFastThreads;
+    for (int k = 0; k < PERW; ++k) {
+        const int i = (threadIdx.x + k * kFastThreads) * W;
         if (i >= Z::TOT) break;
-        const int gi = i / N, z = i - gi * N;
+        const int gi = i / N, z0 = i - gi * N;
         const long long l = l0 + gi;
         if (l >= g.NL) continue;
-        T xc[C];
+        T xc[W][C];
 #pragma unroll
-        for (int cl = 0; cl < Z::NCL; ++cl) {
-            const int rw = gi * Z::NCL + cl;
-            const C2 w = tile[rw * Z::ROW + (z ^ ((rw & 1) * Z::SW))];
-            xc[2 * cl] = w.x * invV;
-            if (2 * cl + 1 < C) xc[2 * cl + 1] = w.y * invV;
+        for (int w = 0; w < W; ++w) {
+#pragma unroll
+            for (int cl = 0; cl < Z::NCL; ++cl) {
+                const int rw = gi * Z::NCL + cl;
+                const C2 u = tile[rw * Z::ROW + ((z0 + w) ^ ((rw & 1) * Z::SW))];
+                xc[w][2 * cl] = u.x * invV;
+                if (2 * cl + 1 < C) xc[w][2 * cl + 1] = u.y * invV;
+            }
         }
-        if constexpr (Epi::kPrefetch) epi.apply_pre(pre[k], b, l * N + z, xc, acc);
-        else epi.apply(b, l * N + z, xc, acc);
+        if constexpr (W > 1) {
+            epi.apply_prew(pre[k], l * N + z0, xc, acc);
+        } else if constexpr (Epi::kPrefetch) {
+            epi.apply_pre(pre[k], b, l * N + z0, xc[0], acc);
+        } else {
+            epi.apply(b, l * N + z0, xc[0], acc);
+        }
     }
     if constexpr (Epi::NSUM > 0) {
         block_reduce_store<Epi::NSUM>(acc, red, partials, b, gridDim.x, blockIdx.x);

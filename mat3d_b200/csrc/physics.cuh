@@ -177,8 +177,30 @@ struct SpecEqVar {
 // ----------------------------------------------------------------------------
 // Every prologue/epilogue splits into load() -- the global reads of one voxel
 // -- and a compute step, so a pass can issue the loads of all its voxels
-// before the first compute and keep them in flight together.
+// before the first compute and keep them in flight together.  Operators with
+// kW = 4 also offer loadw()/..._prew(): four consecutive voxels per call with
+// 16-byte loads and stores of each component (the fast z passes use them;
+// voxel offsets are multiples of 4 there).
 // ----------------------------------------------------------------------------
+__device__ __forceinline__ void ld4(const float* p, float (&o)[4]) {
+    const float4 v = *reinterpret_cast<const float4*>(p);
+    o[0] = v.x; o[1] = v.y; o[2] = v.z; o[3] = v.w;
+}
+__device__ __forceinline__ void ld4(const double* p, double (&o)[4]) {
+    const double2 a = reinterpret_cast<const double2*>(p)[0], b = reinterpret_cast<const double2*>(p)[1];
+    o[0] = a.x; o[1] = a.y; o[2] = b.x; o[3] = b.y;
+}
+__device__ __forceinline__ void ld4(const uint8_t* p, int (&o)[4]) {
+    const uchar4 v = *reinterpret_cast<const uchar4*>(p);
+    o[0] = v.x; o[1] = v.y; o[2] = v.z; o[3] = v.w;
+}
+__device__ __forceinline__ void st4(float* p, const float (&o)[4]) {
+    *reinterpret_cast<float4*>(p) = make_float4(o[0], o[1], o[2], o[3]);
+}
+__device__ __forceinline__ void st4(double* p, const double (&o)[4]) {
+    reinterpret_cast<double2*>(p)[0] = make_double2(o[0], o[1]);
+    reinterpret_cast<double2*>(p)[1] = make_double2(o[2], o[3]);
+}
 // out = M[ph] x  (M: per phase CxC, row-major, double in global -> T in smem)
 template <typename T, int C, typename TX = T>
 struct ProMat {
@@ -226,6 +248,33 @@ struct ProMat {
         }
     }
     __device__ __forceinline__ void eval(int b, long long v, T (&out)[C], double*) const { eval_pre(load(b, v), b, v, out); }
+    static constexpr int kW = 4;
+    struct PreW {
+        int p[4];
+        T xv[4][C];
+    };
+    __device__ __forceinline__ PreW loadw(long long v) const {
+        PreW q;
+        ld4(phb + v, q.p);
+#pragma unroll
+        for (int c = 0; c < C; ++c) {
+            TX t[4];
+            ld4(xb + c * V + v, t);
+#pragma unroll
+            for (int w = 0; w < 4; ++w) q.xv[w][c] = (T)t[w];
+        }
+        return q;
+    }
+    __device__ __forceinline__ void eval_prew(const PreW& q, int w, T (&out)[C]) const {
+        const T* M = sm + q.p[w] * C * C;
+#pragma unroll
+        for (int i = 0; i < C; ++i) {
+            T s = 0;
+#pragma unroll
+            for (int j = 0; j < C; ++j) s += M[i * C + j] * q.xv[w][j];
+            out[i] = s;
+        }
+    }
 };
 
 // FP64 defect pass of the refinement: x += delta (FP32 correction of the
@@ -285,6 +334,42 @@ struct ProRefine64 {
     }
     __device__ __forceinline__ void eval(int b, long long v, double (&out)[C], double*) const {
         eval_pre(load(b, v), b, v, out);
+    }
+    static constexpr int kW = 4;
+    struct PreW {
+        int p[4];
+        double xv[4][C];
+    };
+    // the folded state x + delta is written back at load time (each voxel
+    // belongs to one thread and nothing else in the pass reads x)
+    __device__ __forceinline__ PreW loadw(long long v) const {
+        PreW q;
+        ld4(phb + v, q.p);
+#pragma unroll
+        for (int c = 0; c < C; ++c) {
+            double t[4];
+            ld4(xb + c * V + v, t);
+            if (db) {
+                float d[4];
+                ld4(db + c * V + v, d);
+#pragma unroll
+                for (int w = 0; w < 4; ++w) t[w] += (double)d[w];
+                st4(xb + c * V + v, t);
+            }
+#pragma unroll
+            for (int w = 0; w < 4; ++w) q.xv[w][c] = t[w];
+        }
+        return q;
+    }
+    __device__ __forceinline__ void eval_prew(const PreW& q, int w, double (&out)[C]) const {
+        const double* M = sm + q.p[w] * C * C;
+#pragma unroll
+        for (int i = 0; i < C; ++i) {
+            double s = 0;
+#pragma unroll
+            for (int j = 0; j < C; ++j) s += M[i * C + j] * q.xv[w][j];
+            out[i] = s;
+        }
     }
 };
 
@@ -360,6 +445,56 @@ struct EpiEM {
     __device__ __forceinline__ void apply(int b, long long v, T (&xc)[C], double* acc) const {
         apply_pre(load(b, v), b, v, xc, acc);
     }
+    static constexpr int kW = 4;
+    struct PreW {
+        int p[4];
+        T xv[4][C];
+        T rv[4][C];
+    };
+    __device__ __forceinline__ PreW loadw(long long v) const {
+        PreW q;
+        ld4(phb + v, q.p);
+#pragma unroll
+        for (int c = 0; c < C; ++c) {
+            T t[4];
+            ld4(xb + c * V + v, t);
+            float u[4] = {0.f, 0.f, 0.f, 0.f};
+            if (rb) ld4(rb + c * V + v, u);
+#pragma unroll
+            for (int w = 0; w < 4; ++w) {
+                q.xv[w][c] = t[w];
+                q.rv[w][c] = (T)u[w];
+            }
+        }
+        return q;
+    }
+    __device__ __forceinline__ void apply_prew(const PreW& q, long long v, T (&xc)[4][C], double* acc) const {
+        T xn[C][4];
+#pragma unroll
+        for (int w = 0; w < 4; ++w) {
+            const T* Am = sm + q.p[w] * C * C;
+            const T* os = sm + nph * C * C + q.p[w] * C;
+            T d[C];
+#pragma unroll
+            for (int c = 0; c < C; ++c) d[c] = (xc[w][c] + q.rv[w][c]) - q.xv[w][c];
+            double rs = 0, ot = 0;
+#pragma unroll
+            for (int i = 0; i < C; ++i) {
+                const double wt = (C == 6 && i >= 3) ? 2.0 : 1.0;
+                rs += wt * (double)d[i] * (double)d[i];
+                T s = 0;
+#pragma unroll
+                for (int j = 0; j < C; ++j) s += Am[i * C + j] * d[j];
+                xn[i][w] = q.xv[w][i] + s;
+            }
+#pragma unroll
+            for (int c = 0; c < C; ++c) ot += (double)os[c] * (double)xn[c][w];
+            acc[0] += rs;
+            acc[1] += ot;
+        }
+#pragma unroll
+        for (int c = 0; c < C; ++c) st4(xb + c * V + v, xn[c]);
+    }
 };
 
 // FP64 defect of the refinement: r = x_c - x (stored FP32), x unchanged.
@@ -416,6 +551,42 @@ struct EpiDefect {
     }
     __device__ __forceinline__ void apply(int b, long long v, double (&xc)[C], double* acc) const {
         apply_pre(load(b, v), b, v, xc, acc);
+    }
+    static constexpr int kW = 4;
+    struct PreW {
+        int p[4];
+        double xv[4][C];
+    };
+    __device__ __forceinline__ PreW loadw(long long v) const {
+        PreW q;
+        ld4(phb + v, q.p);
+#pragma unroll
+        for (int c = 0; c < C; ++c) {
+            double t[4];
+            ld4(xb + c * V + v, t);
+#pragma unroll
+            for (int w = 0; w < 4; ++w) q.xv[w][c] = t[w];
+        }
+        return q;
+    }
+    __device__ __forceinline__ void apply_prew(const PreW& q, long long v, double (&xc)[4][C], double* acc) const {
+        float rr[C][4];
+#pragma unroll
+        for (int w = 0; w < 4; ++w) {
+            double rs = 0, ot = 0;
+#pragma unroll
+            for (int c = 0; c < C; ++c) {
+                const double d = xc[w][c] - q.xv[w][c];
+                rr[c][w] = (float)d;
+                const double wt = (C == 6 && c >= 3) ? 2.0 : 1.0;
+                rs += wt * d * d;
+                ot += sm[q.p[w] * C + c] * q.xv[w][c];
+            }
+            acc[0] += rs;
+            acc[1] += ot;
+        }
+#pragma unroll
+        for (int c = 0; c < C; ++c) st4(rb + c * V + v, rr[c]);
     }
 };
 
