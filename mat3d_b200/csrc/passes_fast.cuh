@@ -20,6 +20,7 @@
 #pragma once
 #include "fft_reg.cuh"
 #include "passes.cuh"
+#include "tma.cuh"
 
 namespace m3d {
 
@@ -503,6 +504,132 @@ __global__ void __launch_bounds__(kFastThreads) k_zinv_fast(GridDims g, const ty
         block_reduce_store<Epi::NSUM>(acc, red, partials, b, gridDim.x, blockIdx.x);
         fused_finalize(fin, ctl, partials, Epi::NSUM, b);
     }
+}
+
+
+// ---------------------------------------------------------------------------
+// TMA-staged y pass.  A tile is KC = 4*CPW consecutive kz columns of all Ny
+// rows of one (batch*comp, x) plane: TMA copies it into shared memory as
+// 128-byte-wide boxes with the 128-byte swizzle (16-byte chunk index XOR
+// row mod 8, which makes the column reads of the line FFT conflict-free),
+// the warps transform the columns in place, and TMA stores the tile back.
+// Persistent CTAs walk the tiles with kYStages tiles in flight, so the copies
+// of the next tiles overlap the transforms of the current one.
+// ---------------------------------------------------------------------------
+constexpr int kYStages = 2;
+
+template <typename T, int N>
+struct YTma {
+    typedef typename Cx<T>::t C2;
+    static constexpr int E = LineSplit<T, N>::E, TL = LineSplit<T, N>::Tl, CPW = 32 / TL, KC = 4 * CPW;
+    static constexpr int CPB = 128 / (int)sizeof(C2);  // columns per 128-byte box row
+    static constexpr int NB = KC / CPB;                // boxes per tile
+    static constexpr int BOXE = 128 / (int)sizeof(T);  // box width in scalars
+    static constexpr int STAGE = NB * N * 128;         // bytes per tile
+    static constexpr int XS = RowLen<T, N, false>::value, SWX = RowLen<T, N, false>::sw;
+    static_assert(KC % CPB == 0, "a tile is a whole number of boxes");
+    static constexpr size_t smem() {
+        return 1024 + (size_t)kYStages * STAGE + (size_t)N * sizeof(C2) + (size_t)KC * XS * sizeof(C2) + 8 +
+               kYStages * sizeof(uint64_t);
+    }
+    // byte offset of (column, row) in a tile
+    static __device__ __forceinline__ int off(int col, int y) {
+        const int box = col / CPB, cib = col - box * CPB;
+        if constexpr (sizeof(C2) == 8)
+            return box * N * 128 + y * 128 + ((((cib >> 1) ^ (y & 7)) << 4) | ((cib & 1) << 3));
+        else
+            return box * N * 128 + y * 128 + ((cib ^ (y & 7)) << 4);
+    }
+};
+
+template <typename T, int N, int SIGN>
+__global__ void __launch_bounds__(kFastThreads) k_ypass_tma(const __grid_constant__ CUtensorMap map, GridDims g,
+                                                           const typename Cx<T>::t* __restrict__ twy, int C, int ntiles,
+                                                           const Ctl* __restrict__ ctl, int* err) {
+    typedef typename Cx<T>::t C2;
+    typedef YTma<T, N> Y;
+    constexpr int E = Y::E, TL = Y::TL, CPW = Y::CPW, S = kYStages;
+    extern __shared__ __align__(16) char smem_raw[];
+    char* stage = align_up(smem_raw, 1024);
+    C2* tw = (C2*)(stage + S * Y::STAGE);
+    C2* xch = tw + N;
+    uint64_t* full = (uint64_t*)align_up((char*)(xch + Y::KC * Y::XS), 8);
+    const int ntz = (g.Hzp + Y::KC - 1) / Y::KC;
+    const int per_cb = g.Nx * ntz;
+    for (int i = threadIdx.x; i < N; i += blockDim.x) tw[i] = twy[i];
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < S; ++s) mbar_init(&full[s], 1);
+        mbar_fence_init();
+    }
+    __syncthreads();
+    // the tiles of this CTA whose entry is still iterating, in order
+    auto next = [&](int id) {
+        for (; id < ntiles; id += gridDim.x)
+            if (!ctl[(id / per_cb) / C].done) return id;
+        return -1;
+    };
+    auto coords = [&](int id, int& c0, int& r0) {
+        const int cb = id / per_cb, rem = id - cb * per_cb;
+        const int x = rem / ntz, kzt = rem - x * ntz;
+        r0 = (cb * g.Nx + x) * N;
+        c0 = 2 * kzt * Y::KC;
+    };
+    auto issue = [&](int id, int s) {
+        int c0, r0;
+        coords(id, c0, r0);
+        mbar_expect_tx(&full[s], Y::STAGE);
+#pragma unroll
+        for (int nb = 0; nb < Y::NB; ++nb) tma_load_2d(stage + s * Y::STAGE + nb * N * 128, &map, c0 + nb * Y::BOXE, r0, &full[s]);
+    };
+    int pid = -1;
+    if (threadIdx.x == 0) {
+        pid = next(blockIdx.x);
+        for (int s = 0; s < S && pid >= 0; ++s) {
+            issue(pid, s);
+            pid = next(pid + gridDim.x);
+        }
+    }
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int t = lane % TL, col = warp * CPW + lane / TL;
+    C2* xl = xch + col * Y::XS;
+    const int sw = (col & 1) * Y::SWX;
+    int it = 0;
+    for (int id = next(blockIdx.x); id >= 0; id = next(id + gridDim.x), ++it) {
+        const int s = it % S;
+        const bool ok = mbar_wait(&full[s], (uint32_t)((it / S) & 1), err);
+        if (__syncthreads_or(!ok)) break;
+        char* tile = stage + s * Y::STAGE;
+        C2 v[E];
+        if constexpr (SIGN < 0) {
+#pragma unroll
+            for (int j = 0; j < E; ++j) v[j] = *(const C2*)(tile + Y::off(col, t + TL * j));
+            line_fwd<C2, E, TL>(v, t, xl, tw, sw);
+#pragma unroll
+            for (int r = 0; r < E; ++r) *(C2*)(tile + Y::off(col, spec_mode<E, TL>(t, r))) = v[r];
+        } else {
+#pragma unroll
+            for (int r = 0; r < E; ++r) v[r] = *(const C2*)(tile + Y::off(col, spec_mode<E, TL>(t, r)));
+            line_inv<C2, E, TL>(v, t, xl, tw, sw);
+#pragma unroll
+            for (int j = 0; j < E; ++j) *(C2*)(tile + Y::off(col, t + TL * j)) = v[j];
+        }
+        fence_proxy_async();
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            int c0, r0;
+            coords(id, c0, r0);
+#pragma unroll
+            for (int nb = 0; nb < Y::NB; ++nb) tma_store_2d(&map, c0 + nb * Y::BOXE, r0, tile + nb * N * 128);
+            bulk_commit();
+            bulk_wait_read0();  // the stage may be refilled once the store has read it
+            if (pid >= 0) {
+                issue(pid, s);
+                pid = next(pid + gridDim.x);
+            }
+        }
+    }
+    if (threadIdx.x == 0) bulk_wait0();
+    (void)CPW;
 }
 
 }  // namespace m3d

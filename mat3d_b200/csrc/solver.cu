@@ -24,6 +24,8 @@
 #include "inelastic.cuh"
 #include "passes_fast.cuh"
 
+#include <cudaTypedefs.h>
+
 using namespace m3d;
 
 namespace {
@@ -300,6 +302,14 @@ struct m3d_solver {
     template <typename T, int CC, class Spec> int pass_x(Spec op, Ctl* ctl, typename Cx<T>::t* sp);
     template <typename T, int CC, class Epi, class Fin> int pass_zinv(Epi epi, Ctl* ctl, typename Cx<T>::t* sp, Fin fin);
     int* d_counter = nullptr;  // completion counters of the fused finalize, one per batch entry
+    // TMA-staged y pass: tensor maps of the half spectrum viewed as rows of
+    // 2*Hzp FP32 / FP64 scalars (built for the current buffer and batch)
+    bool use_tma_y = false;
+    CUtensorMap ymap32{}, ymap64{};
+    const void* ymap_base = nullptr;
+    int ymap_B = -1;
+    int* d_err = nullptr;  // device-side error word (bounded waits that expired)
+    bool ensure_ymaps(int CC);
     bool use_fast = true;
     template <typename T, int CC>
     int run_linear(double tol_field, double tol_eq, int criterion, int max_iter);
@@ -334,6 +344,7 @@ struct m3d_solver {
     int init_ctl(Ctl* dctl, double tol_field, double tol_eq, int max_iter, bool inner);
     int sync_ctl(Ctl* dctl);
     int dispatch_run(double tol_field, double tol_eq, int nInc, int criterion, int max_iter);
+    int dispatch_core(double tol_field, double tol_eq, int nInc, int criterion, int max_iter);
     SpecGreen<double, 6> green_params_d6(int zero_k0) const;
     template <typename T, int CC> SpecGreen<T, CC> green(int zero_k0) const;
     template <typename T, int CC> int run_inelastic(double tol_field, double tol_eq, int nInc, int criterion, int max_iter);
@@ -344,6 +355,7 @@ m3d_solver::~m3d_solver() { free_all(); }
 void m3d_solver::free_all() {
     drop_graphs();
     cudaFree(d_trips); d_trips = nullptr;
+    cudaFree(d_err); d_err = nullptr;
     cudaFree(d_phase); d_phase = nullptr;
     cudaFree(d_x); d_x = nullptr;
     cudaFree(d_delta); d_delta = nullptr;
@@ -369,6 +381,11 @@ int m3d_solver::alloc(int batch) {
     const size_t specN = (size_t)batch * C * g.NL * g.Hzp;
     drop_graphs();  // captured launches hold the old buffers
     if (!d_trips) M3D_CUDA(cudaMalloc(&d_trips, 8 * sizeof(int)));
+    if (!d_err) {
+        M3D_CUDA(cudaMalloc(&d_err, sizeof(int)));
+        M3D_CUDA(cudaMemset(d_err, 0, sizeof(int)));
+    }
+    ymap_base = nullptr;  // tensor maps name the old spectrum
     cudaFree(d_x); cudaFree(d_delta); cudaFree(d_r32); cudaFree(d_spec); cudaFree(d_part);
     cudaFree(d_ctl); cudaFree(d_ctl_in);
     if (h_ctl) cudaFreeHost(h_ctl);
@@ -545,6 +562,44 @@ void m3d_solver::pass_zfwd(Pro pro, Ctl* ctl, typename Cx<T>::t* sp) {
     st.kernel_launches += 1;
 }
 
+static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = (PFN_cuTensorMapEncodeTiled_v12000)p;
+        (void)cudaGetLastError();
+    });
+    return fn;
+}
+
+// Tensor maps of the half spectrum for the TMA y pass: 2-D, rows of 2*Hzp
+// scalars (one (batch, comp, x, y) line each), boxes 128 bytes wide and Ny rows
+// high with the 128-byte swizzle.  False if TMA cannot be used for this shape.
+bool m3d_solver::ensure_ymaps(int CC) {
+    if (ymap_base == d_spec && ymap_B == B) return true;
+    auto enc = tensor_map_encoder();
+    const long long R = (long long)B * CC * Nx * Ny;
+    if (!enc || R >= (1LL << 31) || Ny > 256 || !d_err) return false;
+    for (int w = 0; w < 2; ++w) {
+        const int sz = w ? 8 : 4;
+        const cuuint64_t dims[2] = {(cuuint64_t)2 * g.Hzp, (cuuint64_t)R};
+        const cuuint64_t strides[1] = {(cuuint64_t)g.Hzp * 2 * sz};
+        const cuuint32_t box[2] = {(cuuint32_t)(128 / sz), (cuuint32_t)Ny};
+        const cuuint32_t estr[2] = {1, 1};
+        const CUresult r = enc(w ? &ymap64 : &ymap32, w ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2,
+                               d_spec, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                               CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+        if (r != CUDA_SUCCESS) return false;
+    }
+    ymap_base = d_spec;
+    ymap_B = B;
+    return true;
+}
+
 template <typename T>
 void m3d_solver::pass_y(int sign, int CC, Ctl* ctl, typename Cx<T>::t* sp) {
     typedef typename Cx<T>::t C2;
@@ -552,6 +607,20 @@ void m3d_solver::pass_y(int sign, int CC, Ctl* ctl, typename Cx<T>::t* sp) {
         constexpr int NN = decltype(nc)::value;
         constexpr int CPW = 32 / LineSplit<T, NN>::Tl;
         const int ntz = (g.Hzp + 4 * CPW - 1) / (4 * CPW);
+        if (use_tma_y && ensure_ymaps(CC)) {
+            typedef YTma<T, NN> Y;
+            const int ntiles = CC * B * Nx * ntz;
+            auto kern = sign < 0 ? k_ypass_tma<T, NN, -1> : k_ypass_tma<T, NN, +1>;
+            allow_smem(kern);
+            int per_sm = 1, dev = 0, nsm = 148;
+            cudaGetDevice(&dev);
+            cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kFastThreads, Y::smem());
+            const int grid = std::max(1, std::min(ntiles, nsm * std::max(per_sm, 1)));
+            kern<<<grid, kFastThreads, Y::smem(), stream>>>(sizeof(T) == 8 ? ymap64 : ymap32, g, tw<T>(1), CC, ntiles,
+                                                             ctl, d_err);
+            return;
+        }
         const dim3 grid(Nx * ntz, CC * B);
         const size_t sm = ypass_fast_smem<T, NN>();
         allow_smem(k_ypass_fast<T, NN, -1>);
@@ -1005,6 +1074,18 @@ int m3d_solver::run_refine_graph(double tol_field, int max_iter) {
 #undef M3D_CAP
 
 int m3d_solver::dispatch_run(double tol_field, double tol_eq, int nInc, int criterion, int max_iter) {
+    int rc = dispatch_core(tol_field, tol_eq, nInc, criterion, max_iter);
+    if (use_tma_y && d_err) {
+        int e = 0;
+        if (cudaMemcpy(&e, d_err, sizeof(int), cudaMemcpyDeviceToHost) == cudaSuccess && e) {
+            cudaMemset(d_err, 0, sizeof(int));
+            return fail(M3D_ERR_TIMEOUT, "a TMA pipeline wait expired on the device; results are invalid");
+        }
+    }
+    return rc;
+}
+
+int m3d_solver::dispatch_core(double tol_field, double tol_eq, int nInc, int criterion, int max_iter) {
     if (max_iter <= 0) max_iter = (kind == M3D_KIND_MECH) ? 2000 : 500;
     if (kind == M3D_KIND_MECH && behav != M3D_BEHAV_ELASTIC) {
         if (prec == M3D_PREC_FP32_REFINE)
@@ -1161,6 +1242,8 @@ static int create_impl(int kind, int Nx, int Ny, int Nz, int behav, int precisio
         h->use_fast = !(e2 && e2[0] == '1');
         const char* e3 = std::getenv("M3D_NO_GRAPH");
         h->use_graph = !(e3 && e3[0] == '1');
+        const char* e4 = std::getenv("M3D_TMA_Y");
+        h->use_tma_y = (e4 && e4[0] == '1');
     }
     int rc = h->alloc(batch);
     if (rc) { cudaStreamDestroy(h->stream); delete h; return rc; }
