@@ -420,7 +420,7 @@ __global__ void __launch_bounds__(kFastThreads) k_zinv_fast(GridDims g, const ty
     extern __shared__ __align__(16) char smem_raw[];
     C2* tw = (C2*)smem_raw;
     C2* tile = tw + N;
-    constexpr int Hz = HzOf<N>::Hz, Hzp = HzOf<N>::Hzp, P2 = HzOf<N>::P2;
+    constexpr int Hzp = HzOf<N>::Hzp, P2 = HzOf<N>::P2;
     C2* raw = (C2*)align_up((char*)(tile + Z::SLOTS * Z::ROW), 16);  // [gi][c][Hzp] half spectra as stored
     double* red = (double*)align_up((char*)(raw + Z::G * C * Hzp), 16);
     char* extra = (char*)red + 32 * 16 * sizeof(double);
@@ -455,22 +455,42 @@ __global__ void __launch_bounds__(kFastThreads) k_zinv_fast(GridDims g, const ty
     epi.load_smem(extra, b);
     cp_async_wait_all();
     __syncthreads();
-    for (int i = threadIdx.x; i < Z::G * Z::NCL * Hz; i += kFastThreads) {
-        const int k = i % Hz, gl = i / Hz;
-        const int gi = gl / Z::NCL, cl = gl - gi * Z::NCL;
-        const C2 a = raw[(gi * C + 2 * cl) * Hzp + k];
-        const C2 bb = (2 * cl + 1 < C) ? raw[(gi * C + 2 * cl + 1) * Hzp + k] : mk<C2>(0, 0);
-        C2* row = tile + gl * Z::ROW;
-        const int sw = (gl & 1) * Z::SW;
-        if (k == 0 || 2 * k == N) {
-            row[k ^ sw] = mk<C2>(a.x, bb.x);
-        } else {
-            row[k ^ sw] = mk<C2>(a.x - bb.y, a.y + bb.x);
-            row[(N - k) ^ sw] = mk<C2>(a.x + bb.y, bb.x - a.y);
+    // Inverse transform of each complex line (components 2cl + i (2cl+1) of
+    // voxel line gi); its spectrum is assembled from the two stored half
+    // spectra as the lanes load it (Hermitian extension; the imaginary parts of
+    // the k = 0 and k = N/2 modes are dropped, as FFTW's c2r does).  The line's
+    // tile row is the exchange buffer and receives the natural-order result.
+    {
+        constexpr int E = Z::E, TL = Z::TL, LPW = 32 / TL, NW = kFastThreads / 32;
+        const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+        const int t = lane % TL, lw = lane / TL;
+#pragma unroll 1
+        for (int r0 = warp * LPW; r0 < Z::SLOTS; r0 += NW * LPW) {
+            const int gl = r0 + lw;
+            C2* row = tile + gl * Z::ROW;
+            const int sw = (gl & 1) * Z::SW;
+            const bool live = gl < Z::G * Z::NCL;
+            const int gi = gl / Z::NCL, cl = gl - gi * Z::NCL;
+            const bool hasb = live && (2 * cl + 1 < C);
+            const C2* ra = raw + (live ? (gi * C + 2 * cl) * Hzp : 0);
+            const C2* rb = raw + (hasb ? (gi * C + 2 * cl + 1) * Hzp : 0);
+            C2 v[E];
+#pragma unroll
+            for (int r = 0; r < E; ++r) {
+                const int k = spec_mode<E, TL>(t, r);
+                const bool lo = 2 * k <= N;
+                const int kk = lo ? k : N - k;
+                const C2 a = live ? ra[kk] : mk<C2>(0, 0);
+                const C2 q = hasb ? rb[kk] : mk<C2>(0, 0);
+                if (kk == 0 || 2 * kk == N) v[r] = mk<C2>(a.x, q.x);
+                else if (lo) v[r] = mk<C2>(a.x - q.y, a.y + q.x);
+                else v[r] = mk<C2>(a.x + q.y, q.x - a.y);
+            }
+            line_inv<C2, E, TL>(v, t, row, tw, sw);
+#pragma unroll
+            for (int j = 0; j < E; ++j) row[(t + TL * j) ^ sw] = v[j];
         }
     }
-    __syncthreads();
-    z_tile_fft<C2, N, Z::E, Z::TL, Z::SLOTS, Z::ROW, Z::SW, false>(tile, tw);
     __syncthreads();
     const T invV = (T)(1.0 / (double)g.V);
     double acc[Epi::NSUM > 0 ? Epi::NSUM : 1] = {};
