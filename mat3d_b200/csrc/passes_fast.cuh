@@ -380,31 +380,53 @@ __global__ void __launch_bounds__(kFastThreads) k_zfwd_fast(GridDims g, const ty
         }
     }
     __syncthreads();
-    z_tile_fft<C2, N, Z::E, Z::TL, Z::SLOTS, Z::ROW, Z::SW, true>(tile, tw);
-    __syncthreads();
-    // split into the C half spectra, two modes per thread and store
-    constexpr int Hz = HzOf<N>::Hz, Hzp = HzOf<N>::Hzp, P2 = HzOf<N>::P2;
-    C2* ob = spec + ((long long)b * C * g.NL + l0) * Hzp;
-    const long long cst = g.NL * (long long)Hzp;
-    for (int i = threadIdx.x; i < Z::G * C * P2; i += kFastThreads) {
-        const int k2 = i % P2, gc = i / P2;
-        const int gi = gc / C, c = gc - gi * C;
-        if (l0 + gi >= g.NL) continue;
-        const int rw = gi * Z::NCL + c / 2, sw = (rw & 1) * Z::SW;
-        const C2* row = tile + rw * Z::ROW;
-        C2 o[2];
+    // Each warp transforms its tile rows (complex lines c0 + i c1 of voxel line
+    // gi) and, without a block barrier, splits each row into the two
+    // components' half spectra (Z[k] and Z[N-k] are in the same row) and
+    // stores them, two modes per store.
+    {
+        constexpr int E = Z::E, TL = Z::TL, LPW = 32 / TL, NW = kFastThreads / 32;
+        constexpr int Hz = HzOf<N>::Hz, Hzp = HzOf<N>::Hzp, P2 = HzOf<N>::P2;
+        const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+        const int t = lane % TL, lw = lane / TL;
+        C2* ob = spec + ((long long)b * C * g.NL + l0) * Hzp;
+        const long long cst = g.NL * (long long)Hzp;
+#pragma unroll 1
+        for (int r0 = warp * LPW; r0 < Z::SLOTS; r0 += NW * LPW) {
+            const int gl = r0 + lw;
+            C2* row = tile + gl * Z::ROW;
+            const int sw = (gl & 1) * Z::SW;
+            C2 v[E];
 #pragma unroll
-        for (int h = 0; h < 2; ++h) {
-            const int k = 2 * k2 + h;
-            o[h] = mk<C2>(0, 0);
-            if (k < Hz) {
-                const C2 Zk = row[k ^ sw];
-                const C2 Zm = row[(k == 0 ? 0 : N - k) ^ sw];
-                o[h] = (c & 1) ? mk<C2>((T)0.5 * (Zk.y + Zm.y), (T)-0.5 * (Zk.x - Zm.x))
-                               : mk<C2>((T)0.5 * (Zk.x + Zm.x), (T)0.5 * (Zk.y - Zm.y));
+            for (int j = 0; j < E; ++j) v[j] = row[(t + TL * j) ^ sw];
+            __syncwarp();
+            line_fwd<C2, E, TL>(v, t, row, tw, sw);
+#pragma unroll
+            for (int r = 0; r < E; ++r) row[spec_mode<E, TL>(t, r) ^ sw] = v[r];
+            __syncwarp();
+            const int gi = gl / Z::NCL, cl = gl - gi * Z::NCL;
+            if (gl >= Z::G * Z::NCL || l0 + gi >= g.NL) continue;
+            const bool two = 2 * cl + 1 < C;
+            C2* oa = ob + (2 * cl) * cst + gi * Hzp;
+#pragma unroll 1
+            for (int k2 = t; k2 < P2; k2 += TL) {
+                C2 ea[2], eb[2];
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    const int k = 2 * k2 + h;
+                    ea[h] = mk<C2>(0, 0);
+                    eb[h] = mk<C2>(0, 0);
+                    if (k < Hz) {
+                        const C2 Zk = row[k ^ sw];
+                        const C2 Zm = row[(k == 0 ? 0 : N - k) ^ sw];
+                        ea[h] = mk<C2>((T)0.5 * (Zk.x + Zm.x), (T)0.5 * (Zk.y - Zm.y));
+                        eb[h] = mk<C2>((T)0.5 * (Zk.y + Zm.y), (T)-0.5 * (Zk.x - Zm.x));
+                    }
+                }
+                store_pair(oa + 2 * k2, ea[0], ea[1]);
+                if (two) store_pair(oa + cst + 2 * k2, eb[0], eb[1]);
             }
         }
-        store_pair(ob + c * cst + gi * Hzp + 2 * k2, o[0], o[1]);
     }
 }
 
