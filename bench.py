@@ -57,6 +57,34 @@ def bytes_per_vi(c, w):
     return 6 * c * w + 1
 
 
+PASS_NAMES = ("z_forward", "y_forward", "x_turnaround", "y_inverse", "z_inverse")
+PASS_KERNELS = ("k_zfwd_fast (prologue + z R2C)", "k_ypass_fast<-1>", "k_xturn_fast (x FFT, Green, x IFFT)",
+                "k_ypass_fast<+1>", "k_zinv_fast (z C2R + EM update + finalize)")
+
+
+def pass_bytes(c, w, N, forcing):
+    """Algorithmic bytes per launch of each sweep pass on an N^3 grid with c
+    components of w-byte reals: the pass's own inputs and outputs (half
+    spectrum N*N*Hzp complex per component, Hzp = N/2+1 rounded up to even;
+    state c*V reals; 1-byte phase; the FP32 defect read by the refinement's
+    inner sweeps)."""
+    V = N ** 3
+    hzp = ((N // 2 + 1) + 1) & ~1
+    spec = c * N * N * hzp * 2 * w
+    state = c * V * w
+    zfwd = state + V + spec
+    zinv = spec + 2 * state + V + (c * V * 4 if forcing else 0)
+    return (zfwd, 2 * spec, 2 * spec, 2 * spec, zinv)
+
+
+# DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum, warm
+# cache) from the ncu capture summarised in
+# profiles/thermal128_fp32_sweep_kernels.md, keyed (workload, pass, word bytes)
+MEASURED_TRAFFIC = {
+    ("thermal128", "z_inverse", 4): (12.0e6, "profiles/thermal128_fp32_sweep_kernels.md"),
+}
+
+
 WORKLOADS = {
     "thermal128": dict(kind="thermal", N=128, km=1.0, ki=100.0, E=[0.0, 0.0, 1.0], precision="fp32_refine",
                        tol=1e-8, desc="128^3 thermal, 30% ellipsoids (3a,a,a) random orientation, k 100:1, grad z"),
@@ -627,6 +655,27 @@ def main():
     achieved = alg_bytes / (res["ms"] / 1000.0) / 1e9 if res["ms"] > 0 else None
     sweep_fp32_us = 1000 * pr["ms_fp32"] / pr["n_fp32"] if pr["n_fp32"] else None
     sweep_fp64_us = 1000 * pr["ms_fp64"] / pr["n_fp64"] if pr["n_fp64"] else None
+    # dominant kernel: the pass with the largest share of the profiled solve's
+    # device time (events around every pass), its algorithmic bytes per launch
+    # = the pass's own inputs and outputs
+    kern = None
+    if not j2:
+        fp32 = pr["n_fp32"] > 0
+        n = pr["n_fp32"] if fp32 else pr["n_fp64"]
+        pms = pr["pass_ms_fp32"] if fp32 else pr["pass_ms_fp64"]
+        if n and sum(pms) > 0:
+            p = int(np.argmax(pms))
+            wb = 4 if fp32 else 8
+            forcing = w["precision"] == "fp32_refine" and fp32  # inner sweeps read the FP32 defect
+            pb = pass_bytes(c, wb, N, forcing)[p]
+            us = 1000 * pms[p] / n
+            tr = MEASURED_TRAFFIC.get((args.workload, PASS_NAMES[p], wb))
+            kern = {"bound": "hbm", "kernel": PASS_KERNELS[p], "pass": PASS_NAMES[p],
+                    "achieved": pb / (us * 1e-6) / 1e9, "peak": peak, "unit": "GB/s",
+                    "frac": pb / (us * 1e-6) / 1e9 / peak, "traffic": tr[0] if tr else None,
+                    "traffic_source": tr[1] if tr else None, "peak_source": peak_src,
+                    "bytes_per_launch": pb, "launch_us": us, "share_of_sweep": pms[p] / sum(pms),
+                    "pass_us": {PASS_NAMES[q]: 1000 * pms[q] / n for q in range(5)}}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -646,15 +695,20 @@ def main():
                        "fp64_sweeps_per_solve": res["n64"] / args.steps,
                        "fp32_sweeps_per_solve": res["n32"] / args.steps,
                        "residual_reached": st["residual"], "rve": meta,
-                       "l2": "inputs larger than L2: state + defect + correction + spectrum > 126 MB"
-                             if w["kind"] == "thermal" else "64^3 working set is L2-resident by design",
+                       "l2": ("a step is one complete solve; its state (FP64 field, FP32 correction and "
+                              "defect, spectrum: 152 MB) exceeds L2, the FP32 inner sweeps' own working set "
+                              "(78 MB) is reused from L2 by the algorithm")
+                             if w["kind"] == "thermal" else
+                             ("a step is one complete solve; 64^3 working set is L2-resident by design" if N <= 64
+                              else "a step is one complete solve; working set exceeds L2"),
                        "parallelism": f"replicas x{world}"},
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": (achieved / peak) if achieved else None, "traffic": None,
-                         "peak_source": peak_src,
-                         "kernel": "the timed solves (one graph launch each: sweeps of 5 fused FFT passes)",
-                         "bytes_per_voxel_iter": {"fp32": b32, "fp64": b64},
-                         "sweep_us": {"fp32": sweep_fp32_us, "fp64": sweep_fp64_us}},
+            "roofline": kern,
+            "roofline_solve": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                               "frac": (achieved / peak) if achieved else None,
+                               "peak_source": peak_src,
+                               "kernel": "the timed solves (one graph launch each: sweeps of 5 fused FFT passes)",
+                               "bytes_per_voxel_iter": {"fp32": b32, "fp64": b64},
+                               "sweep_us": {"fp32": sweep_fp32_us, "fp64": sweep_fp64_us}},
             "fp64_solver": {"value": val64, "unit": UNIT, "ms_per_solve": ms64 / steps64,
                             "sweeps_per_solve": r64["sweeps"] / steps64,
                             "time_to_solution_ratio": (ms64 / steps64) / (ms_max / args.steps)},
@@ -663,6 +717,8 @@ def main():
             "gpu_launches": res["launches"],
             "clocks": clocks,
         }
+        if line["roofline"] is None:  # J2: the whole-solve model
+            line["roofline"] = dict(line["roofline_solve"], traffic=None)
         if cpu:
             line["cpu_baseline"] = {"value": cpu["value"], "unit": UNIT, "cores": os.cpu_count(),
                                     "kind": "reference", "sample": cpu["sample"]}

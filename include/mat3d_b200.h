@@ -158,6 +158,10 @@ typedef struct {
     long long n_fp64;    /* FP64 sweeps timed */
     double ms_fp32;      /* summed device time of FP32 sweeps */
     long long n_fp32;    /* FP32 sweeps timed */
+    /* the same time split by pass (events around each pass of the linear
+       sweeps): z forward, y forward, x turnaround, y inverse, z inverse */
+    double pass_ms_fp64[5];
+    double pass_ms_fp32[5];
 } m3d_profile;
 int m3d_set_profiling(m3d_solver* h, int enable);  /* enabling also resets the counters */
 int m3d_get_profile(const m3d_solver* h, m3d_profile* out);

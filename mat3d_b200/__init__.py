@@ -98,7 +98,8 @@ class ServeStats(ctypes.Structure):
 
 class Profile(ctypes.Structure):
     _fields_ = [("ms_fp64", ctypes.c_double), ("n_fp64", ctypes.c_longlong),
-                ("ms_fp32", ctypes.c_double), ("n_fp32", ctypes.c_longlong)]
+                ("ms_fp32", ctypes.c_double), ("n_fp32", ctypes.c_longlong),
+                ("pass_ms_fp64", ctypes.c_double * 5), ("pass_ms_fp32", ctypes.c_double * 5)]
 
 
 _lib = None
@@ -270,7 +271,10 @@ class Solver:
     def profile(self):
         p = Profile()
         _check(self.L, self.L.m3d_get_profile(self.h, ctypes.byref(p)), "get_profile")
-        return {k: getattr(p, k) for k, _ in p._fields_}
+        d = {k: getattr(p, k) for k, _ in p._fields_}
+        d["pass_ms_fp64"] = list(p.pass_ms_fp64)
+        d["pass_ms_fp32"] = list(p.pass_ms_fp32)
+        return d
 
     def stream_ptr(self):
         """cudaStream_t of the handle (for timing with events on the launching stream)."""

@@ -259,9 +259,20 @@ struct m3d_solver {
     static constexpr int kChunk = 8;
     bool prof = false;
     cudaEvent_t pev[kChunk + 1] = {};
+    cudaEvent_t ppev[kChunk][6] = {};  // around each of the 5 passes of a sweep (launch_sweep)
+    bool pass_rec[kChunk] = {};
+    int prof_k = 0;
     m3d_profile pr{};
     void prof_mark(int k) {
-        if (prof) cudaEventRecord(pev[k], stream);
+        if (!prof) return;
+        cudaEventRecord(pev[k], stream);
+        prof_k = k;
+        if (k < kChunk) pass_rec[k] = false;
+    }
+    void prof_pass(int p) {
+        if (!prof || prof_k >= kChunk) return;
+        cudaEventRecord(ppev[prof_k][p], stream);
+        if (p == 5) pass_rec[prof_k] = true;
     }
     // add the first `executed` sweep intervals of the last chunk (host has synced)
     void prof_collect(int executed, bool fp64) {
@@ -270,7 +281,14 @@ struct m3d_solver {
             float ms = 0;
             if (cudaEventElapsedTime(&ms, pev[k], pev[k + 1]) != cudaSuccess) continue;
             if (fp64) { pr.ms_fp64 += ms; pr.n_fp64 += 1; } else { pr.ms_fp32 += ms; pr.n_fp32 += 1; }
+            if (!pass_rec[k]) continue;
+            for (int p = 0; p < 5; ++p) {
+                float mp = 0;
+                if (cudaEventElapsedTime(&mp, ppev[k][p], ppev[k][p + 1]) != cudaSuccess) continue;
+                (fp64 ? pr.pass_ms_fp64 : pr.pass_ms_fp32)[p] += mp;
+            }
         }
+        (void)cudaGetLastError();
     }
     int max_iters() const {
         int m = 0;
@@ -693,11 +711,17 @@ int m3d_solver::pass_zinv(Epi epi, Ctl* ctl, typename Cx<T>::t* sp, Fin fin) {
 template <typename T, int CC, class Pro, class Spec, class Epi>
 int m3d_solver::launch_sweep(Pro pro, Spec spec, Epi epi, Ctl* ctl, typename Cx<T>::t* sp, int policy,
                              const Ctl* outer) {
+    prof_pass(0);
     pass_zfwd<T, CC>(pro, ctl, sp);
+    prof_pass(1);
     pass_y<T>(-1, CC, ctl, sp);
+    prof_pass(2);
     pass_x<T, CC>(spec, ctl, sp);
+    prof_pass(3);
     pass_y<T>(+1, CC, ctl, sp);
+    prof_pass(4);
     pass_zinv<T, CC>(epi, ctl, sp, FinLinear{policy, (double)g.V, outer, d_counter});
+    prof_pass(5);
     M3D_CUDA(cudaGetLastError());
     return M3D_OK;
 }
@@ -1312,6 +1336,9 @@ int m3d_destroy(m3d_solver* h) {
     if (h->stream) cudaStreamSynchronize(h->stream);
     for (int k = 0; k <= m3d_solver::kChunk; ++k)
         if (h->pev[k]) cudaEventDestroy(h->pev[k]);
+    for (int k = 0; k < m3d_solver::kChunk; ++k)
+        for (int p = 0; p < 6; ++p)
+            if (h->ppev[k][p]) cudaEventDestroy(h->ppev[k][p]);
     h->free_all();
     if (h->own_stream) cudaStreamDestroy(h->own_stream);
     delete h;
@@ -1710,8 +1737,11 @@ int m3d_get_field(m3d_solver* h, int which, int b, double* out) {
 
 int m3d_set_profiling(m3d_solver* h, int enable) {
     if (!h) return fail(M3D_ERR_ARG, "NULL handle");
-    if (enable && !h->pev[0])
+    if (enable && !h->pev[0]) {
         for (int k = 0; k <= m3d_solver::kChunk; ++k) M3D_CUDA(cudaEventCreate(&h->pev[k]));
+        for (int k = 0; k < m3d_solver::kChunk; ++k)
+            for (int p = 0; p < 6; ++p) M3D_CUDA(cudaEventCreate(&h->ppev[k][p]));
+    }
     h->prof = enable != 0;
     std::memset(&h->pr, 0, sizeof(h->pr));
     return M3D_OK;
