@@ -624,6 +624,16 @@ __device__ __forceinline__ void sum_partials(const double* partials, int NS, int
 __device__ __forceinline__ void policy_linear(Ctl& c, const double* tot, int policy, double V, const Ctl* outer,
                                               int b);
 
+// Stop ratio of the FP32 correction solve of the refinement (its defect norm
+// relative to the FP64 defect it started from): the correction only has to
+// shrink the defect by the factor still missing to reach the tolerance (with
+// a 0.3 margin), but never asks for less than 2e-5, what FP32 sweeps reach
+// reliably, nor more than 0.1.  Same arithmetic on host and device.
+__host__ __device__ inline double refine_inner_tol(double tol, double res) {
+    const double need = res > 0 ? 0.3 * tol / res : 0.1;
+    return fmin(0.1, fmax(2e-5, need));
+}
+
 static __global__ void k_finalize(Ctl* ctl, const double* __restrict__ partials, int NS, int nblk, int policy, double V,
                                   const Ctl* outer) {
     const int b = blockIdx.x;

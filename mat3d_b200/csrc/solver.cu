@@ -845,7 +845,7 @@ int m3d_solver::run_refine(double tol_field, int max_iter) {
             set_green(c, rve_of(b));
             c.done = outer[b].done;
             c.max_iter = max_iter;
-            c.inner_tol = 2e-4;
+            c.inner_tol = refine_inner_tol(outer[b].tol_field, outer[b].residual);
             h_ctl[b] = c;
         }
         M3D_CUDA(cudaMemcpyAsync(d_ctl_in, h_ctl, B * sizeof(Ctl), cudaMemcpyHostToDevice, stream));
@@ -902,7 +902,7 @@ __global__ void k_loop_cond(cudaGraphConditionalHandle h, const Ctl* __restrict_
 // every entry a fresh inner control block (the entries already converged stay
 // done) and arm both loops.
 __global__ void k_refine_mid(cudaGraphConditionalHandle h_outer, cudaGraphConditionalHandle h_inner, Ctl* ctl,
-                             Ctl* ctl_in, int B, double inner_tol, int* trips) {
+                             Ctl* ctl_in, int B, int* trips) {
     int any = 0;
     for (int b = threadIdx.x; b < B; b += blockDim.x) {
         Ctl& o = ctl[b];
@@ -912,7 +912,7 @@ __global__ void k_refine_mid(cudaGraphConditionalHandle h_outer, cudaGraphCondit
         c.gkind = o.gkind; c.gnyq = o.gnyq; c.gxw = o.gxw; c.gp1 = o.gp1; c.gp2 = o.gp2;
         c.done = o.done;
         c.max_iter = o.max_iter;
-        c.inner_tol = inner_tol;
+        c.inner_tol = refine_inner_tol(o.tol_field, o.residual);
         ctl_in[b] = c;
         any |= (o.done == 0);
     }
@@ -1047,7 +1047,7 @@ int m3d_solver::run_refine_graph(double tol_field, int max_iter) {
         EpiDefect<CC> epi = tab(EpiDefect<CC>{d_phase, x, d_r32, g.V, dm(off_Os), nph_max(), nullptr});
         rc = launch_sweep<double, CC>(pro, green<double, CC>(0), epi, d_ctl, sp64, POL_REFINE_OUTER, nullptr);
         if (rc) M3D_CAP(cudaErrorUnknown);
-        k_refine_mid<<<1, 256, 0, stream>>>(h_out, h_in, d_ctl, d_ctl_in, B, 2e-4, d_trips);
+        k_refine_mid<<<1, 256, 0, stream>>>(h_out, h_in, d_ctl, d_ctl_in, B, d_trips);
         M3D_CAP(cudaGetLastError());
         M3D_CAP(cudaMemsetAsync(d_delta, 0, dbytes, stream));
         {
