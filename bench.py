@@ -283,6 +283,7 @@ def run_batch(args, w, rank, world, local):
 
     def make_batch(prec):
         bt = m3d.Batch(m3d.KIND_MECH, prec)
+        bt.set_autotune(True)  # schedule per grid size picked by the autotuner (timed inside each step)
         for (g, mat, _), d in zip(members, desc):
             bt.add_mech((d[1],) * 3, mat, g)
         return bt
@@ -308,7 +309,7 @@ def run_batch(args, w, rank, world, local):
         barrier()
         bt.close()
         return dict(dev_ms=dev_ms, wall_ms=wall_ms, vi=vi, sweeps=sw, n64=n64, n32=n32, launches=launches,
-                    kl=kl, Ce=Ce, groups=st["groups"])
+                    kl=kl, Ce=Ce, groups=st["groups"], autotuned=st["autotuned"])
 
     def e2e_run(prec, steps):
         """Through the public API from host arrays: batch creation, adding every
@@ -362,6 +363,7 @@ def run_batch(args, w, rank, world, local):
                        "sweeps_per_entry": res["sweeps"] / args.steps / (6 * len(desc)),
                        "fp64_sweeps": res["n64"] / args.steps, "fp32_sweeps": res["n32"] / args.steps,
                        "launches_per_step": res["launches"] / args.steps, "groups": res["groups"],
+                       "autotuned_groups": res["autotuned"],
                        "rve_generation_s": gen_s,
                        "l2": "inputs larger than L2 (tens of GB of state per grid-size group)",
                        "parallelism": f"replicas x{world}"},

@@ -204,6 +204,7 @@ typedef struct {
     int groups;              /* distinct grid sizes */
     int launches;            /* multi-RVE solves (groups x memory chunks) */
     long long kernel_launches;
+    int autotuned;           /* groups whose launch schedule the autotuner picked */
 } m3d_batch_stats;
 /* mem_budget_bytes <= 0: 85% of the free device memory at creation. */
 int m3d_batch_create(int kind, int precision, double mem_budget_bytes, m3d_batch** out);
@@ -214,6 +215,9 @@ int m3d_batch_add_thermal(m3d_batch* b, int Nx, int Ny, int Nz, double km, doubl
 /* Ceff, Seff: one C x C block per added RVE, in the order of addition. */
 int m3d_batch_homogenize(m3d_batch* b, double tol_field, int max_iter, double* Ceff, double* Seff);
 int m3d_batch_get_stats(const m3d_batch* b, m3d_batch_stats* out);
+/* on != 0: before the first solve of each grid size, time the launch
+   schedules (m3d_autotune, 3 sweeps each) and use the fastest for that size. */
+int m3d_batch_set_autotune(m3d_batch* b, int on);
 int m3d_batch_clear(m3d_batch* b);
 int m3d_batch_destroy(m3d_batch* b);
 
@@ -275,6 +279,25 @@ int m3d_serve_get_field(m3d_server* s, long long ticket, double* out);
 int m3d_serve_get_stats(m3d_server* s, m3d_serve_stats* out);
 /* Finishes the queued and running requests, then frees every solver. */
 int m3d_serve_destroy(m3d_server* s);
+
+/* ---- autotuner (no counterpart in the reference) ----------------------------
+   Times the launch schedules that compute the same sweep -- the compile-time
+   warp-split FFT kernels or the generic shared-memory ones, the TMA-staged or
+   the register-staged y pass, and the generic kernels' tile sizes -- over
+   `sweeps` full sweeps of the handle's own batch (after its material is set;
+   its field state is overwritten), keeps the fastest on the handle and
+   remembers it for the shape and precision.  sweeps = 0 applies the
+   remembered schedule without timing (M3D_ERR_STATE if there is none).
+   Schedules agree to rounding (the generic and the compile-time FFTs
+   associate differently); the y-pass variants agree bitwise. */
+typedef struct {
+    int fast;         /* 1: compile-time warp-split kernels, 0: generic kernels */
+    int tma_y;        /* 1: TMA-staged y pass (compile-time kernels only) */
+    int G, tzy, tzx;  /* generic kernels: z lines per CTA, y / x tile columns */
+    double sweep_us;  /* measured time of one sweep with this schedule */
+    int candidates;   /* schedules timed */
+} m3d_tune;
+int m3d_autotune(m3d_solver* h, int sweeps, m3d_tune* out);
 
 /* The CUDA stream (cudaStream_t) all work of the handle is ordered on.
    m3d_set_stream replaces it with a caller-owned stream (NULL: the handle's own). */

@@ -65,7 +65,13 @@ class BatchStats(ctypes.Structure):
     _fields_ = [("sweeps", ctypes.c_longlong), ("sweeps_fp64", ctypes.c_longlong),
                 ("sweeps_fp32", ctypes.c_longlong), ("voxel_iters", ctypes.c_longlong),
                 ("device_ms", ctypes.c_double), ("wall_ms", ctypes.c_double), ("rves", ctypes.c_int),
-                ("groups", ctypes.c_int), ("launches", ctypes.c_int), ("kernel_launches", ctypes.c_longlong)]
+                ("groups", ctypes.c_int), ("launches", ctypes.c_int), ("kernel_launches", ctypes.c_longlong),
+                ("autotuned", ctypes.c_int)]
+
+
+class Tune(ctypes.Structure):
+    _fields_ = [("fast", ctypes.c_int), ("tma_y", ctypes.c_int), ("G", ctypes.c_int), ("tzy", ctypes.c_int),
+                ("tzx", ctypes.c_int), ("sweep_us", ctypes.c_double), ("candidates", ctypes.c_int)]
 
 
 class Request(ctypes.Structure):
@@ -113,6 +119,7 @@ EXPORTS = [
     "m3d_create_multi", "m3d_set_material_mech_rve", "m3d_set_material_thermal_rve", "m3d_footprint_bytes",
     "m3d_batch_create", "m3d_batch_add_mech", "m3d_batch_add_thermal", "m3d_batch_homogenize",
     "m3d_batch_get_stats", "m3d_batch_clear", "m3d_batch_destroy",
+    "m3d_autotune", "m3d_batch_set_autotune",
     "m3d_serve_create", "m3d_serve_submit", "m3d_serve_poll", "m3d_serve_wait", "m3d_serve_get_field",
     "m3d_serve_get_stats", "m3d_serve_destroy",
 ]
@@ -163,6 +170,8 @@ def load_library(path: str | None = None):
     L.m3d_batch_get_stats.argtypes = [vp, ctypes.POINTER(BatchStats)]
     L.m3d_batch_clear.argtypes = [vp]
     L.m3d_batch_destroy.argtypes = [vp]
+    L.m3d_autotune.argtypes = [vp, i, ctypes.POINTER(Tune)]
+    L.m3d_batch_set_autotune.argtypes = [vp, i]
     L.m3d_serve_create.argtypes = [d, i, ctypes.POINTER(vp)]
     L.m3d_serve_submit.argtypes = [vp, ctypes.POINTER(Request), ctypes.POINTER(ctypes.c_longlong)]
     L.m3d_serve_poll.argtypes = [vp, ctypes.c_longlong, ctypes.POINTER(Result)]
@@ -265,6 +274,13 @@ class Solver:
         _check(self.L, self.L.m3d_get_stats(self.h, ctypes.byref(st)), "get_stats")
         return st.as_dict()
 
+    def autotune(self, sweeps=3):
+        """Time the launch schedules and keep the fastest (sweeps = 0: apply
+        the schedule remembered for this shape)."""
+        t = Tune()
+        _check(self.L, self.L.m3d_autotune(self.h, sweeps, ctypes.byref(t)), "autotune")
+        return {k: getattr(t, k) for k, _ in t._fields_}
+
     def set_profiling(self, enable=True):
         _check(self.L, self.L.m3d_set_profiling(self.h, 1 if enable else 0), "set_profiling")
 
@@ -323,6 +339,9 @@ class Batch:
                                                     ctypes.byref(idx)), "batch_add")
         self.n += 1
         return idx.value
+
+    def set_autotune(self, on=True):
+        _check(self.L, self.L.m3d_batch_set_autotune(self.h, 1 if on else 0), "batch_set_autotune")
 
     def homogenize(self, tol_field, max_iter=0):
         C = self.C

@@ -46,6 +46,7 @@ struct m3d_batch {
     double budget = 0;  // bytes
     std::vector<BatchRve> rves;
     m3d_batch_stats st{};
+    bool autotune = false;
 };
 
 extern "C" {
@@ -176,6 +177,13 @@ int m3d_batch_homogenize(m3d_batch* b, double tol_field, int max_iter, double* C
                          : m3d_set_material_thermal_rve(h, k, m.km, m.ki, m.phase.data(), m.scheme);
             }
             if (rc) break;
+            if (b->autotune) {
+                // time the schedules on the group's first solver, reuse the choice afterwards
+                m3d_tune t;
+                rc = m3d_autotune(h, c0 == 0 ? 3 : 0, &t);
+                if (rc) break;
+                if (c0 == 0) b->st.autotuned += 1;
+            }
             Ce.assign((size_t)r * C * C, 0.0);
             Se.assign((size_t)r * C * C, 0.0);
             cudaStream_t s = (cudaStream_t)m3d_get_stream(h);
@@ -216,6 +224,12 @@ int m3d_batch_homogenize(m3d_batch* b, double tol_field, int max_iter, double* C
     b->st.rves = (int)b->rves.size();
     if (rc) return rc;
     return status;
+}
+
+int m3d_batch_set_autotune(m3d_batch* b, int on) {
+    if (!b) return bfail(M3D_ERR_ARG, "NULL batch");
+    b->autotune = on != 0;
+    return M3D_OK;
 }
 
 int m3d_batch_get_stats(const m3d_batch* b, m3d_batch_stats* out) {

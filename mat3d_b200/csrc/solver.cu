@@ -14,7 +14,9 @@
 #include <cstdio>
 #include <cstring>
 #include <cstdlib>
+#include <map>
 #include <mutex>
+#include <tuple>
 #include <set>
 #include <string>
 #include <vector>
@@ -329,6 +331,8 @@ struct m3d_solver {
     int* d_err = nullptr;  // device-side error word (bounded waits that expired)
     bool ensure_ymaps(int CC);
     bool use_fast = true;
+    template <typename T, int CC> int tune_time(int sweeps, float* ms);
+    int autotune(int sweeps, m3d_tune* out);
     template <typename T, int CC>
     int run_linear(double tol_field, double tol_eq, int criterion, int max_iter);
     template <int CC>
@@ -1733,6 +1737,145 @@ int m3d_get_field(m3d_solver* h, int which, int b, double* out) {
     if (h->C == 6)
         return h->prec == M3D_PREC_FP32 ? export_field<float, 6>(h, h->d_x, M, b, out) : export_field<double, 6>(h, h->d_x, M, b, out);
     return h->prec == M3D_PREC_FP32 ? export_field<float, 3>(h, h->d_x, M, b, out) : export_field<double, 3>(h, h->d_x, M, b, out);
+}
+
+}  // extern "C"
+
+// ---- autotuner ----------------------------------------------------------------
+// Launch schedules that give identical arithmetic per line but run at
+// different speeds: the compile-time warp-split kernels or the generic
+// shared-memory Stockham kernels, the TMA-staged or the register-staged y pass,
+// and the generic kernels' tile sizes (G z lines per CTA, TZ columns per y / x
+// tile).  Each candidate is timed with CUDA events over a few full sweeps of
+// the handle's own batch (stop rule disabled); the fastest is kept, and
+// remembered per shape and precision for later handles (m3d_autotune with
+// sweeps = 0).
+namespace {
+struct TuneKey {
+    int kind, Nx, Ny, Nz, prec;
+    bool operator<(const TuneKey& o) const {
+        return std::tie(kind, Nx, Ny, Nz, prec) < std::tie(o.kind, o.Nx, o.Ny, o.Nz, o.prec);
+    }
+};
+std::mutex g_tune_mu;
+std::map<TuneKey, m3d_tune> g_tune;
+}  // namespace
+
+template <typename T, int CC>
+int m3d_solver::tune_time(int sweeps, float* ms) {
+    typedef typename Cx<T>::t C2;
+    drop_graphs();
+    int rc = init_ctl(d_ctl, 0.0, 0.0, 1 << 30, false);  // tolerance 0: no entry stops
+    if (rc) return rc;
+    // time a few entries only (the others skip every pass), so tuning a large batch stays cheap
+    for (int b = 6; b < B; ++b) h_ctl[b].done = 1;
+    M3D_CUDA(cudaMemcpyAsync(d_ctl, h_ctl, B * sizeof(Ctl), cudaMemcpyHostToDevice, stream));
+    T* x = (prec == M3D_PREC_FP32_REFINE) ? (T*)(void*)d_delta : (T*)d_x;
+    const float* r = (prec == M3D_PREC_FP32_REFINE) ? d_r32 : nullptr;
+    k_fill_load<T><<<dim3(256, B * CC), 256, 0, stream>>>(x, d_ctl, CC, g.V);
+    C2* sp = (C2*)d_spec;
+    cudaEvent_t e0, e1;
+    M3D_CUDA(cudaEventCreate(&e0));
+    M3D_CUDA(cudaEventCreate(&e1));
+    rc = launch_em<T, CC>(d_ctl, x, r, sp, 0, POL_RESIDUAL, nullptr);  // warm-up (attributes, tensor maps)
+    cudaEventRecord(e0, stream);
+    for (int k = 0; k < sweeps && !rc; ++k) rc = launch_em<T, CC>(d_ctl, x, r, sp, 0, POL_RESIDUAL, nullptr);
+    cudaEventRecord(e1, stream);
+    cudaError_t e = cudaEventSynchronize(e1);
+    if (!rc && e == cudaSuccess) cudaEventElapsedTime(ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (!rc && e != cudaSuccess) return fail(M3D_ERR_CUDA, cudaGetErrorString(e));
+    return rc;
+}
+
+int m3d_solver::autotune(int sweeps, m3d_tune* out) {
+    const bool fp64 = (prec == M3D_PREC_FP64);
+    const size_t csz = fp64 ? 16 : 8;
+    std::vector<m3d_tune> cand;
+    const bool fast_ok = fast_size(Nx) && fast_size(Ny) && fast_size(Nz);
+    const int G0 = fp64 ? G64 : G32, Y0 = fp64 ? TZy64 : TZy32, X0 = fp64 ? TZx64 : TZx32;  // heuristic tiles
+    const size_t lim = 200 * 1024;
+    if (fast_ok) {
+        // compile-time kernels with either y pass, and the generic kernels with their default tiles
+        cand.push_back(m3d_tune{1, 0, G0, Y0, X0, 0, 0});
+        cand.push_back(m3d_tune{1, 1, G0, Y0, X0, 0, 0});
+        cand.push_back(m3d_tune{0, 0, G0, Y0, X0, 0, 0});
+    } else {
+        // generic kernels: every tile size whose shared memory fits comfortably
+        for (int Gv : {2, 4, 8, 16}) {
+            if ((size_t)Nz * csz * (1 + (size_t)Gv * C) + 32 * 32 * 8 + op_smem<double, 6>() > lim) continue;
+            for (int tz : {2, 4, 8, 16}) {
+                if (2 * (size_t)C * Nx * tz * csz + (size_t)Nx * csz > lim || 2 * (size_t)Ny * tz * csz > lim) continue;
+                cand.push_back(m3d_tune{0, 0, Gv, tz, tz, 0, 0});
+            }
+        }
+    }
+    const bool f0 = use_fast, t0 = use_tma_y;
+    const int g32 = G32, g64 = G64, y32 = TZy32, y64 = TZy64, x32 = TZx32, x64 = TZx64;
+    int best = -1;
+    for (size_t i = 0; i < cand.size(); ++i) {
+        m3d_tune& c = cand[i];
+        use_fast = c.fast != 0;
+        use_tma_y = c.tma_y != 0;
+        (fp64 ? G64 : G32) = c.G;
+        (fp64 ? TZy64 : TZy32) = c.tzy;
+        (fp64 ? TZx64 : TZx32) = c.tzx;
+        float ms = 0;
+        int rc = fp64 ? (C == 6 ? tune_time<double, 6>(sweeps, &ms) : tune_time<double, 3>(sweeps, &ms))
+                      : (C == 6 ? tune_time<float, 6>(sweeps, &ms) : tune_time<float, 3>(sweeps, &ms));
+        if (rc) {
+            (void)cudaGetLastError();
+            continue;
+        }
+        c.sweep_us = 1000.0 * ms / sweeps;
+        if (best < 0 || c.sweep_us < cand[best].sweep_us) best = (int)i;
+    }
+    use_fast = f0; use_tma_y = t0;
+    G32 = g32; G64 = g64; TZy32 = y32; TZy64 = y64; TZx32 = x32; TZx64 = x64;
+    drop_graphs();
+    if (best < 0) return fail(M3D_ERR_CUDA, "autotune: no candidate ran");
+    m3d_tune t = cand[best];
+    t.candidates = (int)cand.size();
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        g_tune[TuneKey{kind, Nx, Ny, Nz, prec}] = t;
+    }
+    if (out) *out = t;
+    return M3D_OK;
+}
+
+extern "C" {
+
+int m3d_autotune(m3d_solver* h, int sweeps, m3d_tune* out) {
+    if (!h) return fail(M3D_ERR_ARG, "NULL handle");
+    if (h->kind == M3D_KIND_MECH && h->behav != M3D_BEHAV_ELASTIC)
+        return fail(M3D_ERR_UNSUPPORTED, "the autotuner times the linear sweeps (elastic or thermal solvers)");
+    if (sweeps < 0 || sweeps > 1000) return fail(M3D_ERR_ARG, "sweeps must be in [0, 1000]");
+    m3d_tune t{};
+    if (sweeps > 0) {
+        if (!h->material_set) return fail(M3D_ERR_STATE, "material not set");
+        const int rc = h->autotune(sweeps, &t);
+        if (rc) return rc;
+    } else {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        auto it = g_tune.find(TuneKey{h->kind, h->Nx, h->Ny, h->Nz, h->prec});
+        if (it == g_tune.end()) return fail(M3D_ERR_STATE, "no tuned schedule for this shape yet");
+        t = it->second;
+    }
+    // apply
+    const bool fp64 = (h->prec == M3D_PREC_FP64);
+    h->use_fast = t.fast != 0;
+    h->use_tma_y = t.tma_y != 0;
+    (fp64 ? h->G64 : h->G32) = t.G;
+    (fp64 ? h->TZy64 : h->TZy32) = t.tzy;
+    (fp64 ? h->TZx64 : h->TZx32) = t.tzx;
+    if (h->prec == M3D_PREC_FP32_REFINE) {  // its FP64 defect sweeps keep the fast/TMA choice, generic sizes of FP32
+        h->G64 = std::max(2, t.G / 2) & ~1;
+    }
+    h->drop_graphs();
+    if (out) *out = t;
+    return M3D_OK;
 }
 
 int m3d_set_profiling(m3d_solver* h, int enable) {
