@@ -643,3 +643,92 @@ class ThermOracle:
         up = fi_i * ki + fi_m * km - fi_i * fi_m * (km - ki) ** 2 / (3 * ki - fi_i * (ki - km))
         lo = fi_i * ki + fi_m * km - fi_i * fi_m * (km - ki) ** 2 / (3 * km + fi_m * (ki - km))
         return dict(mori_tanaka=mt, hs_low=lo, hs_up=up)
+
+
+# ============================================================================
+# 2-D elastic solver, src/2d/FFT_analysis2D.cpp (plane, 3 components
+# [11, 22, 12] with tensor shear, complex fields, basic scheme, fixed number
+# of iterations).
+# ============================================================================
+class Mech2DOracle:
+    """Restatement of FFT_Analysis2D.  Fields are (3, Nx*Ny) complex with
+    voxel index y + Ny*x (src/2d/FFT_analysis2D.cpp:11-19 allocates 3 x xy)."""
+
+    # GF component s -> tensor indices (i, j, k, h)  (:64-70)
+    Q = ((0, 0, 0, 0), (0, 0, 1, 1), (0, 0, 0, 1), (1, 1, 1, 1), (1, 1, 0, 1), (0, 1, 0, 1))
+    # row j of the symmetric 3 x 3 operator -> GF component (:107-110)
+    W = ((0, 1, 2), (1, 3, 4), (2, 4, 5))
+
+    def __init__(self, Nx, Ny):
+        self.Nx, self.Ny, self.xy = Nx, Ny, Nx * Ny
+        self.eps = np.zeros((3, self.xy), np.complex128)
+        self.sig = np.zeros((3, self.xy), np.complex128)
+        self.E = np.zeros(3, np.complex128)
+
+    def material(self, props, rve):  # :189-224
+        Em, vm, Ei, vi = [float(p) for p in props[:4]]
+        mum = Em / (1 + vm) / 2
+        lam = vm * Em / (1 + vm) / (1 - 2 * vm)
+        mui = Ei / (1 + vi) / 2
+        lai = vi * Ei / (1 + vi) / (1 - 2 * vi)
+        self.Cm = np.array([[lam + 2 * mum, lam, 0], [lam, lam + 2 * mum, 0], [0, 0, 2 * mum]])
+        self.Ci = np.array([[lai + 2 * mui, lai, 0], [lai, lai + 2 * mui, 0], [0, 0, 2 * mui]])
+        self.C0 = 1.0 * (self.Cm + self.Ci) / 2.0
+        self.la0 = 1.0 * (lai + lam) / 2.0
+        self.mu0 = 1.0 * (mui + mum) / 2.0
+        self.rve = np.asarray(rve).ravel().astype(np.float64)
+
+    def setLoad(self, E):  # :226-233
+        self.E = np.asarray(E, np.complex128).copy()
+        self.eps[:] = self.E[:, None]
+
+    def green(self):  # setGF, :49-103 (x wraps with Ny as in :85-86)
+        Nx, Ny = self.Nx, self.Ny
+        d1 = 1 / (4 * self.mu0)
+        d2 = (self.la0 + self.mu0) / (self.mu0 * (self.la0 + 2 * self.mu0))
+        x = np.arange(Nx)
+        y = np.arange(Ny)
+        x1 = np.where(x <= (Nx - 1) // 2, x, -(Ny - x)).astype(np.float64)
+        y1 = np.where(y <= (Ny - 1) // 2, y, -(Ny - y)).astype(np.float64)
+        X, Y = np.meshgrid(x1, y1, indexing="ij")
+        z = (X.ravel(), Y.ravel())
+        n2 = z[0] * z[0] + z[1] * z[1]
+        dl = lambda a, b: 1.0 if a == b else 0.0
+        GF = np.zeros((6, self.xy))
+        with np.errstate(divide="ignore", invalid="ignore"):
+            for s, (i, j, k, h) in enumerate(self.Q):
+                GF[s] = (d1 / n2) * (dl(k, i) * z[h] * z[j] + dl(h, i) * z[k] * z[j] + dl(k, j) * z[h] * z[i]
+                                     + dl(h, j) * z[k] * z[i]) - (d2 * z[i] * z[j] * z[k] * z[h]) / (n2 * n2)
+        return GF
+
+    def iterate(self, GF):
+        Nx, Ny, xy = self.Nx, self.Ny, self.xy
+        # multipCx (:106-116): sigma = C(x) eps
+        mtx = self.rve == 1
+        self.sig = np.where(mtx[None, :], self.Cm @ self.eps, self.Ci @ self.eps)
+        tau = self.sig - self.C0 @ self.eps  # runAnalysis :240
+        t2 = np.fft.fft2(tau.reshape(3, Nx, Ny), axes=(1, 2)).reshape(3, xy)  # FFT_tau :118-122
+        t1 = np.empty_like(t2)
+        for j in range(3):  # multiplyGF :124-137
+            w = self.W[j]
+            t1[j] = -(GF[w[0]] * t2[0] + GF[w[1]] * t2[1] + GF[w[2]] * t2[2] * 2)
+        t1[:, 0] = self.E * xy
+        t2 = np.fft.ifft2(t1.reshape(3, Nx, Ny), axes=(1, 2)).reshape(3, xy) * xy  # FFTW backward, unnormalised
+        self.eps = t2 / xy  # FFTBCKWRD_epsilon :140-145
+
+    def runAnalysis(self, iterations=25):  # :235-247
+        GF = self.green()
+        for _ in range(iterations):
+            self.iterate(GF)
+
+    def homogenization(self, iterations=25):  # :250-283 (no setLoad between load cases)
+        epH = np.zeros((3, 3))
+        sgH = np.zeros((3, 3))
+        for w in range(3):
+            self.E = np.zeros(3, np.complex128)
+            self.E[w] = 0.005
+            self.runAnalysis(iterations)
+            epH[w, :] = self.eps.real.sum(axis=1) / self.xy
+            sgH[:, w] = self.sig.real.sum(axis=1) / self.xy
+        C = np.linalg.inv(epH) @ sgH
+        return C, epH, sgH

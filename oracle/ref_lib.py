@@ -98,3 +98,29 @@ class RefLib:
         self.L.ref_therm_homog(Nx, Ny, Nz, D(km), D(ki), _p(rve), D(tol_field), D(tol_eq), self.threads, None, _p(K),
                                _p(R), ctypes.byref(sw), ctypes.byref(sch))
         return dict(K=K.reshape(3, 3), R=R.reshape(3, 3), sweeps=sw.value, scheme=sch.value)
+
+    # ---- 2-D solver (src/2d/FFT_analysis2D.cpp) -----------------------------
+    def mech2d_run(self, shape, props, rve, E):
+        """material(props, RVE), setLoad(E), runAnalysis() (25 iterations);
+        epsilon and sigma as (3, Nx*Ny) complex arrays."""
+        Nx, Ny = shape
+        xy = Nx * Ny
+        props = np.ascontiguousarray(props, np.float64)
+        rve = np.ascontiguousarray(np.asarray(rve).ravel(), np.int32)
+        Ec = np.ascontiguousarray(np.asarray(E, np.complex128))
+        eps, sig = np.zeros(3 * xy, np.complex128), np.zeros(3 * xy, np.complex128)
+        self.L.ref_2d_run(Nx, Ny, _p(props), _p(rve), _p(Ec), _p(eps), _p(sig))
+        return dict(eps=eps.reshape(xy, 3).T.copy(), sig=sig.reshape(xy, 3).T.copy())
+
+    def mech2d_homog(self, shape, props, rve, E):
+        """setLoad(E) then homogenization(): CHomo, epHomo, sigHomo (3 x 3)."""
+        Nx, Ny = shape
+        props = np.ascontiguousarray(props, np.float64)
+        rve = np.ascontiguousarray(np.asarray(rve).ravel(), np.int32)
+        Ec = np.ascontiguousarray(np.asarray(E, np.complex128))
+        C, ep, sg = np.zeros(9), np.zeros(9), np.zeros(9)
+        rc = self.L.ref_2d_homog(Nx, Ny, _p(props), _p(rve), _p(Ec), _p(C), _p(ep), _p(sg))
+        if rc:
+            raise RuntimeError(f"ref_2d_homog failed ({rc})")
+        # Eigen storage is column-major
+        return dict(C=C.reshape(3, 3).T, epHomo=ep.reshape(3, 3).T, sigHomo=sg.reshape(3, 3).T)

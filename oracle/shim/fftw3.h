@@ -121,7 +121,8 @@ struct Line1D {
 };
 
 struct Plan {
-    int kind = 0; /* 0 = r2c, 1 = c2r */
+    int kind = 0; /* 0 = r2c, 1 = c2r, 2 = c2c forward, 3 = c2c backward (cin -> cbuf) */
+    fftw_complex* cin = nullptr;
     int rank = 0;
     std::vector<fftw_iodim64> dims;
     std::vector<fftw_iodim64> howmany;
@@ -168,6 +169,43 @@ inline void execute(Plan* p) {
     const int nt = p->nthreads;
 
     for (std::ptrdiff_t h = 0; h < hm_n; ++h) {
+        if (p->kind >= 2) {
+            /* complex to complex: gather the input (input strides), scatter it
+               to the output strides, then in-place 1-D transforms along every
+               dimension of the output */
+            const fftw_complex* in = p->cin + h * hm_is;
+            fftw_complex* out = p->cbuf + h * hm_os;
+            const int sign = (p->kind == 2) ? -1 : +1;
+            std::vector<std::ptrdiff_t> is(r), os(r), ext(r);
+            for (int i = 0; i < r; ++i) { is[i] = p->dims[i].is; os[i] = p->dims[i].os; ext[i] = p->dims[i].n; }
+            {
+                std::ptrdiff_t total = 1;
+                for (int i = 0; i < r; ++i) total *= ext[i];
+                std::vector<cplx> tmp((std::size_t)total);
+                for (std::ptrdiff_t lin = 0; lin < total; ++lin) {
+                    std::ptrdiff_t rem = lin, oi = 0;
+                    for (int i = r - 1; i >= 0; --i) { oi += (rem % ext[i]) * is[i]; rem /= ext[i]; }
+                    tmp[(std::size_t)lin] = cplx(in[oi][0], in[oi][1]);
+                }
+                for (std::ptrdiff_t lin = 0; lin < total; ++lin) {
+                    std::ptrdiff_t rem = lin, oo = 0;
+                    for (int i = r - 1; i >= 0; --i) { oo += (rem % ext[i]) * os[i]; rem /= ext[i]; }
+                    out[oo][0] = tmp[(std::size_t)lin].real();
+                    out[oo][1] = tmp[(std::size_t)lin].imag();
+                }
+            }
+            for (int ax = r - 1; ax >= 0; --ax) {
+                const Line1D& L = p->lines[ax];
+                const std::ptrdiff_t n = p->dims[ax].n, s = p->dims[ax].os;
+                for_each_line(p->dims, os, os, ext, ax, nt, [&](std::ptrdiff_t oi, std::ptrdiff_t) {
+                    std::vector<cplx> a(n), b(n);
+                    for (std::ptrdiff_t j = 0; j < n; ++j) a[j] = cplx(out[oi + j * s][0], out[oi + j * s][1]);
+                    L.exec(a.data(), b.data(), sign);
+                    for (std::ptrdiff_t j = 0; j < n; ++j) { out[oi + j * s][0] = b[j].real(); out[oi + j * s][1] = b[j].imag(); }
+                });
+            }
+            continue;
+        }
         if (p->kind == 0) {
             const double* in = p->rbuf + h * hm_is;
             fftw_complex* out = p->cbuf + h * hm_os;
@@ -273,6 +311,17 @@ inline fftw_plan fftw_plan_guru64_dft_c2r(int rank, const fftw_iodim64* dims, in
                                           const fftw_iodim64* howmany_dims, fftw_complex* in, double* out,
                                           unsigned) {
     return m3d_fftw_make_plan(1, rank, dims, howmany_rank, howmany_dims, out, in);
+}
+
+#define FFTW_FORWARD (-1)
+#define FFTW_BACKWARD (+1)
+
+inline fftw_plan fftw_plan_guru64_dft(int rank, const fftw_iodim64* dims, int howmany_rank,
+                                      const fftw_iodim64* howmany_dims, fftw_complex* in, fftw_complex* out, int sign,
+                                      unsigned) {
+    fftw_plan p = m3d_fftw_make_plan(sign < 0 ? 2 : 3, rank, dims, howmany_rank, howmany_dims, nullptr, out);
+    p->cin = in;
+    return p;
 }
 
 inline void fftw_execute(const fftw_plan p) { m3d_fftw_shim::execute(p); }

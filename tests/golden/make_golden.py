@@ -79,6 +79,20 @@ def main():
         h = ref.therm_homog(shape, km, ki, rve, 1e-10, 1e-10)
         np.savez_compressed(os.path.join(HERE, f"{name}.npz"), shape=shape, rve=rve, km=km, ki=ki, E=E, tol=1e-10,
                             **r, K=h["K"], R=h["R"], homog_sweeps=h["sweeps"])
+    # 2-D solver (src/2d/FFT_analysis2D.cpp): single run (25 iterations) and
+    # homogenization, an even and an odd square grid (non-square grids make
+    # the reference divide by a zero wave vector: x wraps with Ny)
+    props = np.array([68.9e9, 0.35, 400e9, 0.23])
+    for N in (16, 15):
+        X, Y = np.meshgrid(np.arange(N), np.arange(N), indexing="ij")
+        rve = np.ones((N, N), np.int32)
+        rve[(X - N / 2) ** 2 + (Y - N / 2.5) ** 2 <= 16] = 0
+        rve = rve.ravel()
+        E = np.array([0, 0.001j, 0.005], np.complex128)
+        r = ref.mech2d_run((N, N), props, rve, E)
+        h = ref.mech2d_homog((N, N), props, rve, E)
+        np.savez_compressed(os.path.join(HERE, f"mech2d_{N}.npz"), shape=(N, N), rve=rve, props=props, E=E,
+                            eps=r["eps"], sig=r["sig"], C=h["C"], epHomo=h["epHomo"], sigHomo=h["sigHomo"])
     print("fixtures written to", HERE)
 
 

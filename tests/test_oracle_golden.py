@@ -88,3 +88,24 @@ def test_thermal(name):
     o2.material(float(f["km"]), float(f["ki"]), f["rve"])
     K, R = o2.homogenization(float(f["tol"]), float(f["tol"]))
     assert np.abs(K - f["K"]).max() / np.abs(f["K"]).max() < 1e-12
+
+
+@pytest.mark.parametrize("name", ["mech2d_16", "mech2d_15"])
+def test_mech2d(name):
+    """The 2-D solver (src/2d/FFT_analysis2D.cpp): 25 basic-scheme iterations
+    from setLoad(E), complex fields, and homogenization() continuing from that
+    field."""
+    f = load(name)
+    Nx, Ny = (int(v) for v in f["shape"])
+    o = O.Mech2DOracle(Nx, Ny)
+    o.material(f["props"], f["rve"])
+    o.setLoad(f["E"])
+    o.runAnalysis()
+    assert rel(o.eps, f["eps"]) < 1e-12
+    assert rel(o.sig, f["sig"]) < 1e-12
+    C, ep, sg = o.homogenization()
+    # the means agree to rounding; C = epHomo^-1 sigHomo amplifies the rounding
+    # of the near-zero off-diagonal means (sequential vs pairwise sums)
+    assert np.abs(ep - f["epHomo"]).max() < 1e-15
+    assert np.abs(sg - f["sigHomo"]).max() / np.abs(f["sigHomo"]).max() < 1e-12
+    assert np.abs(C - f["C"]).max() / np.abs(f["C"]).max() < 1e-6
