@@ -299,6 +299,31 @@ typedef struct {
 } m3d_tune;
 int m3d_autotune(m3d_solver* h, int sweeps, m3d_tune* out);
 
+/* ---- the 2-D elastic solver -------------------------------------------------
+   Replaces FFT_Analysis2D (include/FFT_analysis2D.hpp:20-100,
+   src/2d/FFT_analysis2D.cpp): plane problem on an Nx x Ny grid, 3 components
+   [11, 22, 12] with tensor shear, complex FP64 fields, the basic scheme for
+   a fixed number of iterations (the reference runs 25, :236).  Fields are
+   exchanged as the reference stores them: 3 complex values (re, im) per
+   voxel, voxel index y + Ny*x.
+     m3d2d_create       FFT_Analysis2D(Nx, Ny)                 src/2d/FFT_analysis2D.cpp:3
+     m3d2d_material     material(properties, RVE)              :189-224 (props = E_m, nu_m, E_i, nu_i;
+                                                                         phase 1 = matrix)
+     m3d2d_set_load     setLoad(E)                             :226-233 (E = 3 complex values)
+     m3d2d_run          runAnalysis()                          :235-247
+     m3d2d_homogenize   homogenization()                       :250-283 (row-major 3 x 3 outputs)
+     m3d2d_get_fields   the public fields epsilon, sigma       include/FFT_analysis2D.hpp:35-36 */
+typedef struct m3d_solver2d m3d_solver2d;
+int m3d2d_create(int Nx, int Ny, m3d_solver2d** out);
+int m3d2d_destroy(m3d_solver2d* h);
+int m3d2d_material(m3d_solver2d* h, const double* props, const int32_t* phase);
+int m3d2d_set_load(m3d_solver2d* h, const double* E);
+int m3d2d_run(m3d_solver2d* h, int iterations);
+int m3d2d_homogenize(m3d_solver2d* h, int iterations, double* CHomo, double* epHomo, double* sigHomo);
+int m3d2d_get_fields(m3d_solver2d* h, double* eps, double* sig);
+long long m3d2d_kernel_launches(const m3d_solver2d* h);
+void* m3d2d_get_stream(const m3d_solver2d* h);
+
 /* The CUDA stream (cudaStream_t) all work of the handle is ordered on.
    m3d_set_stream replaces it with a caller-owned stream (NULL: the handle's own). */
 void* m3d_get_stream(const m3d_solver* h);

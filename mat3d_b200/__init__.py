@@ -120,6 +120,8 @@ EXPORTS = [
     "m3d_batch_create", "m3d_batch_add_mech", "m3d_batch_add_thermal", "m3d_batch_homogenize",
     "m3d_batch_get_stats", "m3d_batch_clear", "m3d_batch_destroy",
     "m3d_autotune", "m3d_batch_set_autotune",
+    "m3d2d_create", "m3d2d_destroy", "m3d2d_material", "m3d2d_set_load", "m3d2d_run", "m3d2d_homogenize",
+    "m3d2d_get_fields", "m3d2d_kernel_launches", "m3d2d_get_stream",
     "m3d_serve_create", "m3d_serve_submit", "m3d_serve_poll", "m3d_serve_wait", "m3d_serve_get_field",
     "m3d_serve_get_stats", "m3d_serve_destroy",
 ]
@@ -151,7 +153,8 @@ def load_library(path: str | None = None):
     L.m3d_last_error.restype = ctypes.c_char_p
     L.m3d_abi_version.restype = i
     for name in EXPORTS:
-        if name not in ("m3d_status_string", "m3d_last_error", "m3d_get_stream", "m3d_footprint_bytes"):
+        if name not in ("m3d_status_string", "m3d_last_error", "m3d_get_stream", "m3d_footprint_bytes",
+                        "m3d2d_kernel_launches", "m3d2d_get_stream"):
             getattr(L, name).restype = ctypes.c_int
     L.m3d_get_stream.restype = vp
     L.m3d_get_stream.argtypes = [vp]
@@ -170,6 +173,17 @@ def load_library(path: str | None = None):
     L.m3d_batch_get_stats.argtypes = [vp, ctypes.POINTER(BatchStats)]
     L.m3d_batch_clear.argtypes = [vp]
     L.m3d_batch_destroy.argtypes = [vp]
+    L.m3d2d_create.argtypes = [i, i, ctypes.POINTER(vp)]
+    L.m3d2d_destroy.argtypes = [vp]
+    L.m3d2d_material.argtypes = [vp, vp, vp]
+    L.m3d2d_set_load.argtypes = [vp, vp]
+    L.m3d2d_run.argtypes = [vp, i]
+    L.m3d2d_homogenize.argtypes = [vp, i, vp, vp, vp]
+    L.m3d2d_get_fields.argtypes = [vp, vp, vp]
+    L.m3d2d_kernel_launches.argtypes = [vp]
+    L.m3d2d_kernel_launches.restype = ctypes.c_longlong
+    L.m3d2d_get_stream.argtypes = [vp]
+    L.m3d2d_get_stream.restype = vp
     L.m3d_autotune.argtypes = [vp, i, ctypes.POINTER(Tune)]
     L.m3d_batch_set_autotune.argtypes = [vp, i]
     L.m3d_serve_create.argtypes = [d, i, ctypes.POINTER(vp)]
@@ -370,6 +384,100 @@ class Batch:
             self.close()
         except Exception:
             pass
+
+
+class Solver2D:
+    """The 2-D elastic solver (m3d2d_*): complex FP64 fields, basic scheme."""
+
+    def __init__(self, Nx, Ny):
+        self.L = load_library()
+        self.Nx, self.Ny, self.xy = Nx, Ny, Nx * Ny
+        h = ctypes.c_void_p()
+        _check(self.L, self.L.m3d2d_create(Nx, Ny, ctypes.byref(h)), "m3d2d_create")
+        self.h = h
+
+    def material(self, props, phase):
+        p = np.ascontiguousarray(props, np.float64)
+        ph = np.ascontiguousarray(np.asarray(phase).ravel(), np.int32)
+        _check(self.L, self.L.m3d2d_material(self.h, _ptr(p), _ptr(ph)), "material")
+
+    def set_load(self, E):
+        e = np.ascontiguousarray(np.asarray(E, np.complex128))
+        _check(self.L, self.L.m3d2d_set_load(self.h, _ptr(e)), "setLoad")
+
+    def run(self, iterations=25):
+        _check(self.L, self.L.m3d2d_run(self.h, iterations), "runAnalysis")
+
+    def homogenize(self, iterations=25):
+        C, ep, sg = np.zeros((3, 3)), np.zeros((3, 3)), np.zeros((3, 3))
+        _check(self.L, self.L.m3d2d_homogenize(self.h, iterations, _ptr(C), _ptr(ep), _ptr(sg)), "homogenization")
+        return C, ep, sg
+
+    def fields(self):
+        """epsilon, sigma as (3, Nx*Ny) complex arrays."""
+        e = np.zeros(3 * self.xy, np.complex128)
+        s = np.zeros(3 * self.xy, np.complex128)
+        _check(self.L, self.L.m3d2d_get_fields(self.h, _ptr(e), _ptr(s)), "get_fields")
+        return e.reshape(self.xy, 3).T.copy(), s.reshape(self.xy, 3).T.copy()
+
+    def kernel_launches(self):
+        return int(self.L.m3d2d_kernel_launches(self.h))
+
+    def stream_ptr(self):
+        return self.L.m3d2d_get_stream(self.h)
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.m3d2d_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class FFT_Analysis2D:
+    """Drop-in mirror of the reference's ``FFT_Analysis2D``
+    (include/FFT_analysis2D.hpp:20-100): material(q, RVE) with
+    q = [E_m, nu_m, E_i, nu_i] and RVE 1 = matrix; setLoad(E) with E = 3
+    complex strains [E11, E22, E12]; runAnalysis() runs 25 iterations;
+    homogenization() fills CHomo, SHomo, epHomo, sigHomo."""
+
+    ITERATIONS = 25
+
+    def __init__(self, Nx, Ny):
+        self.Nx, self.Ny, self.xy = Nx, Ny, Nx * Ny
+        self._s = Solver2D(Nx, Ny)
+
+    def material(self, properties, RVE):
+        q = [float(v) for v in properties[:4]]
+        self.Em, self.vm, self.Ei, self.vi = q
+        self.mum, self.lam = q[0] / (1 + q[1]) / 2, q[1] * q[0] / (1 + q[1]) / (1 - 2 * q[1])
+        self.mui, self.lai = q[2] / (1 + q[3]) / 2, q[3] * q[2] / (1 + q[3]) / (1 - 2 * q[3])
+        self.Cm = np.array([[self.lam + 2 * self.mum, self.lam, 0], [self.lam, self.lam + 2 * self.mum, 0],
+                            [0, 0, 2 * self.mum]])
+        self.Ci = np.array([[self.lai + 2 * self.mui, self.lai, 0], [self.lai, self.lai + 2 * self.mui, 0],
+                            [0, 0, 2 * self.mui]])
+        self.C0 = (self.Cm + self.Ci) / 2.0
+        self.la0, self.mu0 = (self.lai + self.lam) / 2.0, (self.mui + self.mum) / 2.0
+        self.RVE = np.asarray(RVE).ravel()
+        self._s.material(q, (self.RVE == 1).astype(np.int32))
+
+    def setLoad(self, E):
+        self.E = np.asarray(E, np.complex128).ravel()[:3]
+        self._s.set_load(self.E)
+
+    def runAnalysis(self):
+        self._s.run(self.ITERATIONS)
+        self.epsilon, self.sigma = self._s.fields()
+
+    def homogenization(self):
+        self.CHomo, self.epHomo, self.sigHomo = self._s.homogenize(self.ITERATIONS)
+        self.SHomo = np.linalg.inv(self.CHomo)
+        self.epsilon, self.sigma = self._s.fields()
+        return self.CHomo
 
 
 class Server:

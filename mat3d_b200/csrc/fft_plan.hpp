@@ -1,0 +1,43 @@
+// fft_plan.hpp -- host-side set-up of the generic line FFTs: the radix
+// schedule of a length and its twiddle table (shared by the 3-D and 2-D solvers).
+#pragma once
+#include <cmath>
+#include <vector>
+
+#include "fft_smem.cuh"
+
+namespace m3d {
+
+// radix schedule 8, 4, 2, then odd primes up to kMaxGenericRadix; false if a factor is larger
+inline bool make_plan(int n, LinePlan& p) {
+    std::vector<int> f;
+    int m = n;
+    while (m % 8 == 0) { f.push_back(8); m /= 8; }
+    while (m % 4 == 0) { f.push_back(4); m /= 4; }
+    while (m % 2 == 0) { f.push_back(2); m /= 2; }
+    for (int q = 3; q <= m; q += 2)
+        while (m % q == 0) { f.push_back(q); m /= q; }
+    if (f.empty()) f.push_back(1);
+    if ((int)f.size() > kMaxStages) return false;
+    for (int r : f)
+        if (r > kMaxGenericRadix) return false;
+    p.n = n;
+    p.nstages = (n == 1) ? 0 : (int)f.size();
+    for (int i = 0; i < kMaxStages; ++i) p.radix[i] = i < (int)f.size() ? f[i] : 1;
+    return true;
+}
+
+// tw[m] = exp(-2 pi i m / n), evaluated in long double
+template <typename T>
+inline std::vector<typename Cx<T>::t> twiddles(int n) {
+    std::vector<typename Cx<T>::t> t(n);
+    const long double two_pi = 6.283185307179586476925286766559L;
+    for (int m = 0; m < n; ++m) {
+        const long double a = -two_pi * (long double)m / (long double)n;
+        t[m].x = (T)cosl(a);
+        t[m].y = (T)sinl(a);
+    }
+    return t;
+}
+
+}  // namespace m3d

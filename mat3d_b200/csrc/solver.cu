@@ -25,6 +25,7 @@
 #include "physics.cuh"
 #include "inelastic.cuh"
 #include "passes_fast.cuh"
+#include "fft_plan.hpp"
 
 #include <cudaTypedefs.h>
 
@@ -106,36 +107,6 @@ Mat diag(int n, double v) {
     return o;
 }
 
-// ---- FFT plans --------------------------------------------------------------
-bool make_plan(int n, LinePlan& p) {
-    std::vector<int> f;
-    int m = n;
-    while (m % 8 == 0) { f.push_back(8); m /= 8; }
-    while (m % 4 == 0) { f.push_back(4); m /= 4; }
-    while (m % 2 == 0) { f.push_back(2); m /= 2; }
-    for (int q = 3; q <= m; q += 2)
-        while (m % q == 0) { f.push_back(q); m /= q; }
-    if (f.empty()) f.push_back(1);
-    if ((int)f.size() > kMaxStages) return false;
-    for (int r : f)
-        if (r > kMaxGenericRadix) return false;
-    p.n = n;
-    p.nstages = (n == 1) ? 0 : (int)f.size();
-    for (int i = 0; i < kMaxStages; ++i) p.radix[i] = i < (int)f.size() ? f[i] : 1;
-    return true;
-}
-
-template <typename T>
-std::vector<typename Cx<T>::t> twiddles(int n) {
-    std::vector<typename Cx<T>::t> t(n);
-    const long double two_pi = 6.283185307179586476925286766559L;
-    for (int m = 0; m < n; ++m) {
-        const long double a = -two_pi * (long double)m / (long double)n;
-        t[m].x = (T)cosl(a);
-        t[m].y = (T)sinl(a);
-    }
-    return t;
-}
 
 // Let a kernel use all dynamic shared memory left next to its static arrays
 // (227 KB per block on sm_100 in total).
