@@ -96,6 +96,9 @@ WORKLOADS = {
                         "log-normal radii 3-10, 20 increments to 2% uniaxial"),
     "batch512": dict(kind="batch", count=512, precision="fp32_refine", tol=1e-6,
                      desc="512 RVEs N in {32,48,64,96}, vf 5-40%, contrast 2-100, 6 load cases each, full C_eff"),
+    "elastic2d": dict(kind="2d", N=1024, iterations=25, props=(68.9e9, 0.35, 400e9, 0.23),
+                      desc="2-D plane elastic (FFT_Analysis2D), 1024^2, discs at 20%, E 68.9/400 GPa, "
+                           "E12 = 0.005, 25 basic-scheme iterations, complex FP64"),
     "serve": dict(kind="serve", per_level=24, levels=(0.25, 0.5, 1.0, 1.5), tol=1e-6, workers=8,
                   desc="Poisson mix of elastic/thermal/J2 solves, N log-uniform 32..256 (rounded), residual 1e-6"),
 }
@@ -232,12 +235,143 @@ def cpu_reference_batch(w, steps, warmup, threads):
                        f"first load case, stopped after 2 sweeps (set-up included), FP64")
 
 
+def disc_rve_2d(N, vf=0.20, seed=0):
+    """Seeded 2-D microstructure: overlapping discs of radius N/32 at
+    inclusion fraction vf (phase 1 = matrix, 0 = inclusion)."""
+    rng = np.random.default_rng(seed)
+    g = np.ones((N, N), np.int32)
+    r = N / 32.0
+    X, Y = np.meshgrid(np.arange(N), np.arange(N), indexing="ij")
+    while (g == 0).mean() < vf:
+        cx, cy = rng.uniform(0, N, 2)
+        dx = (X - cx + N / 2) % N - N / 2
+        dy = (Y - cy + N / 2) % N - N / 2
+        g[dx * dx + dy * dy <= r * r] = 0
+    return g.ravel()
+
+
+def cpu_reference_2d(w, steps, warmup):
+    """The reference's FFT_Analysis2D (oracle/_ref) on the host: each step is
+    one full runAnalysis (25 iterations) of the same 2-D workload."""
+    from oracle import ref_lib
+    if not ref_lib.available():
+        return None
+    ref = ref_lib.RefLib()
+    N = w["N"]
+    rve = disc_rve_2d(N)
+    E = np.array([0, 0, 0.005], np.complex128)
+    secs = 0.0
+    for i in range(warmup + steps):
+        t0 = time.perf_counter()
+        ref.mech2d_run((N, N), np.array(w["props"]), rve, E)
+        if i >= warmup:
+            secs += time.perf_counter() - t0
+    its = steps * w["iterations"]
+    return dict(value=N * N * its / secs, seconds=secs,
+                sample=f"{steps} x reference runAnalysis of the full {N}^2 workload ({w['iterations']} iterations, "
+                       f"set-up included), FP64 complex, single thread")
+
+
+def run_2d(args, w, rank, world, local):
+    """2-D solver: a step is one runAnalysis (w["iterations"] iterations)."""
+    import torch
+    import torch.distributed as dist
+
+    import mat3d_b200 as m3d
+
+    N = w["N"]
+    rve = disc_rve_2d(N, seed=rank)
+    E = np.array([0, 0, 0.005], np.complex128)
+    s = m3d.Solver2D(N, N)
+    s.material(np.array(w["props"]), rve)
+    stream = torch.cuda.ExternalStream(s.stream_ptr())
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def reduce(x, op):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=op)
+        return float(t.item())
+
+    for _ in range(args.warmup):
+        s.set_load(E)
+        s.run(w["iterations"])
+    l0 = s.kernel_launches()
+    clk = ClockSampler(local)
+    clk.start()
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        s.set_load(E)
+        s.run(w["iterations"])
+    e1.record(stream)
+    barrier()
+    clocks = clk.stop()
+    ms = e0.elapsed_time(e1)
+    launches = s.kernel_launches() - l0
+    ms_max = reduce(ms, dist.ReduceOp.MAX if world > 1 else None)
+    vi = N * N * w["iterations"] * args.steps
+    value = reduce(float(vi), dist.ReduceOp.SUM if world > 1 else None) / (ms_max / 1000.0)
+    # e2e: material from the host, run, both fields copied back
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(max(1, args.steps // 2)):
+        s.material(np.array(w["props"]), rve)
+        s.set_load(E)
+        s.run(w["iterations"])
+        s.fields()
+    barrier()
+    esec = reduce(time.perf_counter() - t0, dist.ReduceOp.MAX if world > 1 else None)
+    e2e = reduce(float(N * N * w["iterations"] * max(1, args.steps // 2)),
+                 dist.ReduceOp.SUM if world > 1 else None) / esec
+    s.close()
+    peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    peak, peak_src = (json.load(open(peaks_path))["hbm_gbs"], "measured") if os.path.exists(peaks_path) \
+        else (6650.0, "fallback")
+    # algorithmic bytes per voxel-iteration: pointwise (read eps 48 B + phase 1 B, write
+    # sigma and tau 96 B) + three FFT passes reading and writing 3 complex FP64 (96 B each)
+    bpv = 48 + 1 + 96 + 3 * 96
+    achieved = bpv * vi / (ms / 1000.0) / 1e9
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_reference_2d(w, 1, 0)
+    if rank == 0:
+        line = {
+            "metric": "2-D voxel-iters/s (25-iteration basic scheme, FP64 complex)", "value": value,
+            "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "c128", "data": "synthetic",
+            "config": {"workload": args.workload, "desc": w["desc"], "grid": [N, N],
+                       "iterations": w["iterations"], "l2": "state (3 complex FP64 fields, 50 MB each) "
+                       "exceeds L2 in total; each pass streams 2-3 fields", "parallelism": f"replicas x{world}"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "traffic": None, "peak_source": peak_src, "bytes_per_voxel_iter": bpv,
+                         "kernel": "one iteration (pointwise + 3 generic FFT passes)"},
+            "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": N * N * 4 + 96,
+                    "d2h_bytes_per_step": 2 * 3 * 16 * N * N},
+            "gpu_launches": launches,
+            "clocks": clocks,
+        }
+        if cpu:
+            line["cpu_baseline"] = {"value": cpu["value"], "unit": UNIT, "cores": 1, "kind": "reference",
+                                    "sample": cpu["sample"]}
+        print(json.dumps(line))
+
+
 def run_reference_arm(args, w, rank, world):
     if rank != 0:
         return
     threads = os.cpu_count() or 1
     if w["kind"] == "batch":
         r = cpu_reference_batch(w, args.steps, args.warmup, threads)
+    elif w["kind"] == "2d":
+        r = cpu_reference_2d(w, args.steps, args.warmup)
     else:
         r = cpu_reference(w, args.steps, args.warmup, threads)
     if r is None:
@@ -532,8 +666,8 @@ def main():
     if world > 1:
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=120))
-    if w["kind"] in ("batch", "serve"):
-        (run_batch if w["kind"] == "batch" else run_serve)(args, w, rank, world, local)
+    if w["kind"] in ("batch", "serve", "2d"):
+        {"batch": run_batch, "serve": run_serve, "2d": run_2d}[w["kind"]](args, w, rank, world, local)
         if world > 1:
             dist.destroy_process_group()
         return
