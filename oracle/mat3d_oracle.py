@@ -25,6 +25,8 @@ ignored); numpy's 1/N normalisation equals the reference's ``/xyz``
 """
 from __future__ import annotations
 
+import math
+
 import numpy as np
 
 VOIGT_PAIRS = [(0, 0), (1, 1), (2, 2), (1, 2), (0, 2), (0, 1)]
@@ -732,3 +734,158 @@ class Mech2DOracle:
             sgH[:, w] = self.sig.real.sum(axis=1) / self.xy
         C = np.linalg.inv(epH) @ sgH
         return C, epH, sgH
+
+
+# ============================================================================
+# Microstructure reconstruction by phase retrieval, src/rec/reconstruction.cpp
+# (recon::recPlan from a two-point correlation function, runRec).
+# ============================================================================
+def _mix64(z):
+    z = z + np.uint64(0x9E3779B97F4A7C15)
+    z = (z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+    z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+    return z ^ (z >> np.uint64(31))
+
+
+def rand_pm1(seed, call, n):
+    """The seeded counter-based draws that stand in for Eigen's setRandom:
+    2 u - 1 with u = (mix(mix(seed * 0x100000001B3 + call) + i) >> 11) * 2^-53."""
+    with np.errstate(over="ignore"):
+        b = _mix64(np.uint64(seed) * np.uint64(0x100000001B3) + np.uint64(call))
+        v = _mix64(b + np.arange(n, dtype=np.uint64))
+    return 2.0 * ((v >> np.uint64(11)).astype(np.float64) * (1.0 / 9007199254740992.0)) - 1.0
+
+
+def tpcf_isotropic(N, A=25.0, Q=0.4, phi1=0.5):
+    """The example TPCF of example/reconst3d/main.cpp:37-80 (scaled
+    autocovariance f(r) = exp(-r/A) sin(Q r)/(Q r), S2 = f phi1 phi2 + phi1^2),
+    centred at (N/2, N/2, N/2), before the driver's ifftshift."""
+    m = N // 2
+    i = np.arange(N) - m
+    X, Y, Z = np.meshgrid(i, i, i, indexing="ij")
+    r = np.sqrt(X * X + Y * Y + Z * Z * 1.0)
+    with np.errstate(invalid="ignore", divide="ignore"):
+        fr = np.exp(-r / A) * np.sin(Q * r) / (Q * r)
+    fr[r == 0] = 1.0
+    phi2 = 1 - phi1
+    return (fr * phi1 * phi2 + phi1 * phi1).ravel()
+
+
+def ifftshift3(a, Nx, Ny, Nz):
+    """recon::ifftshift (:100-140): inverse of the centring shift, per axis
+    by floor(n/2) (even n) or floor(n/2)+1 (odd n)."""
+    return np.fft.ifftshift(np.asarray(a).reshape(Nx, Ny, Nz)).ravel()
+
+
+class RecOracle:
+    """recPlan(TPCF, Nx, Ny, Nz) (:213-240) and runRec(n, beta) (:283-400).
+
+    `fft(a, sign)` is the unnormalised 3-D complex transform (sign -1 forward,
+    +1 backward); numpy's by default.  The iteration is chaotic: a rounding
+    difference of one unit grows by a factor of about three per iteration, so
+    two implementations agree bit for bit only when they share every rounding
+    step -- `fft` lets the pin tests run this restatement on the reference's
+    own transform, and every other operation below keeps the reference's
+    order (sequential error sum, sqrt(re^2 + im^2), atan2, division by xyz).
+    """
+
+    def __init__(self, tpcf, Nx, Ny, Nz, fft=None, libm_atan2=False):
+        self.shape = (Nx, Ny, Nz)
+        # numpy's arctan2 rounds differently from the C library's atan2 (which
+        # std::arg calls) in a few ulps of cases; the pin tests take libm's
+        self.atan2 = np.frompyfunc(math.atan2, 2, 1) if libm_atan2 else np.arctan2
+        self.xyz = Nx * Ny * Nz
+        self.normC = np.sqrt(np.abs(np.asarray(tpcf, np.float64).ravel()) * self.xyz)
+        sh = self.shape
+        self.fft = fft or (lambda a, sign: (np.fft.fftn(a.reshape(sh)) if sign < 0 else
+                                            np.fft.ifftn(a.reshape(sh), norm="forward")).ravel())
+
+    def error(self, MT):
+        """funcNormC (include/reconstruction.hpp:37-44): mean |(|MTilda| - normC)|, summed in voxel order."""
+        a = np.abs(np.sqrt(MT.real * MT.real + MT.imag * MT.imag) - self.normC)
+        return float(np.add.accumulate(a)[-1]) / self.xyz
+
+    def start(self, seed):
+        """The state runRec starts from (:289-293): mTilda = (U + 1) / 2 from the first draw."""
+        st = dict(mT=((rand_pm1(seed, 0, self.xyz) + 1.0) * 0.5).astype(np.complex128), i=0, j=0, call=1,
+                  seed=seed)
+        return st
+
+    def step(self, st, beta):
+        """One pass of the runRec loop (:296-364) on state `st` (mTilda, i, j,
+        draw counter); returns the recorded error.  The caller checks i < n
+        before and err < 0.1 after, as the loop does."""
+        xyz = self.xyz
+        st["j"] += 1
+        MT = self.fft(st["mT"], -1)
+        err = self.error(MT)
+        st["MT"] = MT
+        if err < 0.1:
+            return err
+        at = lambda z: np.asarray(self.atan2(z.imag, z.real), np.float64)
+        ang = at(MT)
+        if np.remainder(st["i"] + 1, 150) == 0:  # restart the phases from a fresh draw
+            r = rand_pm1(st["seed"], st["call"], xyz)
+            st["call"] += 1
+            MH = self.fft(r.astype(np.complex128), -1)
+            ang = at(MH) * 0.3 + at(MT) * 0.7
+        MH = self.normC * np.cos(ang) + 1j * (self.normC * np.sin(ang))
+        mH = self.fft(MH, +1)
+        re, im = mH.real / xyz, mH.imag / xyz
+        mT = st["mT"]
+        if st["j"] < 100:  # hybrid input-output projection
+            k = re < 0
+            re[k] = mT.real[k] - beta * re[k]
+            im[k] = 0
+            k = re > 1
+            re[k] = mT.real[k] - beta * (re[k] - 1)
+            im[k] = 0
+            k = re > 1
+            re[k] = 1
+            im[k] = 0
+        else:  # plain box projection
+            k = re < 0
+            re[k] = 0
+            im[k] = 0
+            k = re > 1
+            re[k] = 1
+            im[k] = 0
+            if st["j"] > 200:
+                st["j"] = 0
+        st["mT"] = re + 1j * im
+        st["i"] += 1
+        return err
+
+    def threshold(self, field):
+        """The closing loop of runRec (:370-395): shift the 0.5 cut by 0.001 at a
+        time until the phase-1 fraction is within 1e-4 of normC[0] / xyz (at
+        most 202 tries)."""
+        xyz = self.xyz
+        ctr, x = 0, 0.0
+        while True:
+            b = np.where(field < 0.5 - x, 0.0, 1.0)
+            vol_dif = b.sum() / (1.0 * xyz) - self.normC[0] / (1.0 * xyz)
+            if vol_dif > 0:
+                x -= 0.001
+            else:
+                x += 0.001
+            if abs(vol_dif) < 0.0001 or ctr > 200:
+                break
+            ctr += 1
+        return b
+
+    def runRec(self, n, beta, seed):
+        st = self.start(seed)
+        err = np.zeros(n)
+        while True:
+            if st["i"] >= n:
+                break
+            i = st["i"]
+            err[i] = self.step(st, beta)
+            if err[i] < 0.1:
+                break
+        self.err = err
+        self.iterations = int(np.count_nonzero(err))
+        self.field = st["mT"].real.copy()
+        self.rve = self.threshold(self.field)
+        return self.rve

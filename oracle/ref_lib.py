@@ -124,3 +124,31 @@ class RefLib:
             raise RuntimeError(f"ref_2d_homog failed ({rc})")
         # Eigen storage is column-major
         return dict(C=C.reshape(3, 3).T, epHomo=ep.reshape(3, 3).T, sigHomo=sg.reshape(3, 3).T)
+
+    # ---- microstructure reconstruction (src/rec/reconstruction.cpp) -----------
+    def rec_run(self, shape, tpcf, n, beta, seed):
+        """recPlan(TPCF, Nx, Ny, Nz).runRec(n, beta) with the stand-in generator
+        seeded by `seed`: the binary field, the error track, iterations run."""
+        Nx, Ny, Nz = shape
+        t = np.ascontiguousarray(np.asarray(tpcf, np.float64).ravel())
+        rve, err = np.zeros(t.size), np.zeros(n)
+        self.L.ref_rec_run.restype = ctypes.c_int
+        its = self.L.ref_rec_run(Nx, Ny, Nz, _p(t), n, ctypes.c_double(beta), ctypes.c_ulonglong(seed), _p(rve),
+                                 _p(err))
+        return dict(rve=rve, err=err, iterations=its)
+
+    def ifftshift(self, a, shape):
+        Nx, Ny, Nz = shape
+        x = np.ascontiguousarray(np.asarray(a, np.float64).ravel())
+        out = np.zeros_like(x)
+        self.L.ref_ifftshift(_p(x), _p(out), Nx, Ny, Nz)
+        return out
+
+    def fft3(self, a, shape, sign):
+        """One unnormalised 3-D complex transform through the stand-in FFTW
+        plan the reconstruction runs on (sign -1 forward, +1 backward)."""
+        Nx, Ny, Nz = shape
+        x = np.ascontiguousarray(np.asarray(a, np.complex128).ravel())
+        out = np.zeros_like(x)
+        self.L.ref_fft3(ctypes.c_void_p(x.ctypes.data), ctypes.c_void_p(out.ctypes.data), Nx, Ny, Nz, sign)
+        return out

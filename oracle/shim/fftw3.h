@@ -324,6 +324,16 @@ inline fftw_plan fftw_plan_guru64_dft(int rank, const fftw_iodim64* dims, int ho
     return p;
 }
 
+/* row-major complex transforms (last index fastest), in -> out */
+inline fftw_plan fftw_plan_dft_3d(int n0, int n1, int n2, fftw_complex* in, fftw_complex* out, int sign, unsigned f) {
+    const fftw_iodim64 d[3] = {{n0, (std::ptrdiff_t)n1 * n2, (std::ptrdiff_t)n1 * n2}, {n1, n2, n2}, {n2, 1, 1}};
+    return fftw_plan_guru64_dft(3, d, 0, nullptr, in, out, sign, f);
+}
+inline fftw_plan fftw_plan_dft_2d(int n0, int n1, fftw_complex* in, fftw_complex* out, int sign, unsigned f) {
+    const fftw_iodim64 d[2] = {{n0, n1, n1}, {n1, 1, 1}};
+    return fftw_plan_guru64_dft(2, d, 0, nullptr, in, out, sign, f);
+}
+
 inline void fftw_execute(const fftw_plan p) { m3d_fftw_shim::execute(p); }
 inline void fftw_destroy_plan(fftw_plan p) { delete p; }
 
