@@ -324,6 +324,46 @@ int m3d2d_get_fields(m3d_solver2d* h, double* eps, double* sig);
 long long m3d2d_kernel_launches(const m3d_solver2d* h);
 void* m3d2d_get_stream(const m3d_solver2d* h);
 
+/* ---- microstructure reconstruction by phase retrieval ---------------------
+   Replaces recon::recPlan (include/reconstruction.hpp:46-96,
+   src/rec/reconstruction.cpp) built from a full two-point correlation
+   function: complex FP64 fields, voxel index z + Nz*(y + Ny*x).
+     m3drec_create        recPlan(TPCF, Nx, Ny, Nz)            src/rec/reconstruction.cpp:213-240
+                          (normC = sqrt(|TPCF| * xyz))
+     m3drec_seed          the seed of the random draws (Eigen setRandom in the
+                          reference): draw `call` of voxel v is 2u - 1 with
+                          u = (mix(mix(seed * 0x100000001B3 + call) + v) >> 11) * 2^-53,
+                          mix = the SplitMix64 finaliser; draw 0 makes the
+                          initial field, each restart pass takes the next
+     m3drec_run           runRec(n, beta)                      :283-400 (loop + threshold)
+     m3drec_get_field     the public member mTilda (real part) include/reconstruction.hpp:74
+     m3drec_get_error     the public member trackrealerrorA    include/reconstruction.hpp:73
+     m3drec_fftshift      recon::fftshift                      :47-90
+     m3drec_ifftshift     recon::ifftshift                     :97-140
+   Beyond the reference: m3drec_iterate continues the loop from the current
+   state without the closing threshold, m3drec_threshold applies it, and
+   m3drec_set_state / m3drec_get_state move the complete loop state (field as
+   xyz complex (re, im) pairs, counters i and j, draws taken) for checkpoints. */
+typedef struct m3d_rec m3d_rec;
+int m3drec_create(int Nx, int Ny, int Nz, const double* tpcf, int device, m3d_rec** out);
+int m3drec_destroy(m3d_rec* h);
+int m3drec_seed(m3d_rec* h, unsigned long long seed);
+int m3drec_run(m3d_rec* h, int n, double beta);
+int m3drec_iterate(m3d_rec* h, int iters, double beta);
+int m3drec_threshold(m3d_rec* h);
+int m3drec_set_state(m3d_rec* h, const double* field, int i, int j, unsigned long long call);
+int m3drec_get_state(m3d_rec* h, double* field, int* i, int* j, unsigned long long* call);
+int m3drec_get_field(m3d_rec* h, double* out);
+int m3drec_get_error(m3d_rec* h, double* out, int cap, int* count);
+/* Per-kernel event timing (host-driven passes instead of the graph) and the
+   summed times [restart transform, zfwd, yfwd, xturn, yinv, zinv] in ms. */
+int m3drec_set_profiling(m3d_rec* h, int on);
+int m3drec_profile(const m3d_rec* h, double* ms6, long long* passes);
+long long m3drec_kernel_launches(const m3d_rec* h);
+void* m3drec_get_stream(const m3d_rec* h);
+int m3drec_fftshift(const double* in, double* out, int Nx, int Ny, int Nz);
+int m3drec_ifftshift(const double* in, double* out, int Nx, int Ny, int Nz);
+
 /* The CUDA stream (cudaStream_t) all work of the handle is ordered on.
    m3d_set_stream replaces it with a caller-owned stream (NULL: the handle's own). */
 void* m3d_get_stream(const m3d_solver* h);

@@ -124,6 +124,9 @@ EXPORTS = [
     "m3d2d_get_fields", "m3d2d_kernel_launches", "m3d2d_get_stream",
     "m3d_serve_create", "m3d_serve_submit", "m3d_serve_poll", "m3d_serve_wait", "m3d_serve_get_field",
     "m3d_serve_get_stats", "m3d_serve_destroy",
+    "m3drec_create", "m3drec_destroy", "m3drec_seed", "m3drec_run", "m3drec_iterate", "m3drec_threshold",
+    "m3drec_set_state", "m3drec_get_state", "m3drec_get_field", "m3drec_get_error", "m3drec_set_profiling",
+    "m3drec_profile", "m3drec_kernel_launches", "m3drec_get_stream", "m3drec_fftshift", "m3drec_ifftshift",
 ]
 
 
@@ -154,7 +157,8 @@ def load_library(path: str | None = None):
     L.m3d_abi_version.restype = i
     for name in EXPORTS:
         if name not in ("m3d_status_string", "m3d_last_error", "m3d_get_stream", "m3d_footprint_bytes",
-                        "m3d2d_kernel_launches", "m3d2d_get_stream"):
+                        "m3d2d_kernel_launches", "m3d2d_get_stream", "m3drec_kernel_launches",
+                        "m3drec_get_stream"):
             getattr(L, name).restype = ctypes.c_int
     L.m3d_get_stream.restype = vp
     L.m3d_get_stream.argtypes = [vp]
@@ -195,6 +199,25 @@ def load_library(path: str | None = None):
     L.m3d_serve_destroy.argtypes = [vp]
     L.m3d_set_profiling.argtypes = [vp, i]
     L.m3d_get_profile.argtypes = [vp, ctypes.POINTER(Profile)]
+    u64, ip = ctypes.c_ulonglong, ctypes.POINTER(ctypes.c_int)
+    L.m3drec_create.argtypes = [i, i, i, vp, i, ctypes.POINTER(vp)]
+    L.m3drec_destroy.argtypes = [vp]
+    L.m3drec_seed.argtypes = [vp, u64]
+    L.m3drec_run.argtypes = [vp, i, d]
+    L.m3drec_iterate.argtypes = [vp, i, d]
+    L.m3drec_threshold.argtypes = [vp]
+    L.m3drec_set_state.argtypes = [vp, vp, i, i, u64]
+    L.m3drec_get_state.argtypes = [vp, vp, ip, ip, ctypes.POINTER(u64)]
+    L.m3drec_get_field.argtypes = [vp, vp]
+    L.m3drec_get_error.argtypes = [vp, vp, i, ip]
+    L.m3drec_set_profiling.argtypes = [vp, i]
+    L.m3drec_profile.argtypes = [vp, vp, ctypes.POINTER(ctypes.c_longlong)]
+    L.m3drec_kernel_launches.argtypes = [vp]
+    L.m3drec_kernel_launches.restype = ctypes.c_longlong
+    L.m3drec_get_stream.argtypes = [vp]
+    L.m3drec_get_stream.restype = vp
+    L.m3drec_fftshift.argtypes = [vp, vp, i, i, i]
+    L.m3drec_ifftshift.argtypes = [vp, vp, i, i, i]
     if path is None:
         _lib = L
     return L
@@ -674,3 +697,127 @@ class FFT_analysis3d_thermal:
 
     def stats(self):
         return self._s.stats()
+
+
+# ---- microstructure reconstruction (m3drec_*) -------------------------------
+def _shift(name, a, Nx, Ny, Nz):
+    L = load_library()
+    x = np.ascontiguousarray(np.asarray(a, np.float64).ravel())
+    if x.size != Nx * Ny * Nz:
+        raise ValueError("size does not match Nx * Ny * Nz")
+    out = np.empty_like(x)
+    _check(L, getattr(L, name)(_ptr(x), _ptr(out), Nx, Ny, Nz), name)
+    return out
+
+
+def fftshift(a, Nx, Ny, Nz):
+    """recon::fftshift (src/rec/reconstruction.cpp:47-90) of an Nx*Ny*Nz array."""
+    return _shift("m3drec_fftshift", a, Nx, Ny, Nz)
+
+
+def ifftshift(a, Nx, Ny, Nz):
+    """recon::ifftshift (src/rec/reconstruction.cpp:97-140)."""
+    return _shift("m3drec_ifftshift", a, Nx, Ny, Nz)
+
+
+class Reconstruction:
+    """Phase-retrieval reconstruction of a two-phase field from its two-point
+    correlation function on the GPU (m3drec_*)."""
+
+    def __init__(self, tpcf, Nx, Ny, Nz, device=0):
+        self.L = load_library()
+        self.Nx, self.Ny, self.Nz, self.xyz = Nx, Ny, Nz, Nx * Ny * Nz
+        t = np.ascontiguousarray(np.asarray(tpcf, np.float64).ravel())
+        if t.size != self.xyz:
+            raise ValueError("tpcf must hold Nx * Ny * Nz values")
+        h = ctypes.c_void_p()
+        _check(self.L, self.L.m3drec_create(Nx, Ny, Nz, _ptr(t), device, ctypes.byref(h)), "m3drec_create")
+        self.h = h
+
+    def seed(self, seed):
+        _check(self.L, self.L.m3drec_seed(self.h, int(seed)), "seed")
+
+    def run(self, n, beta):
+        _check(self.L, self.L.m3drec_run(self.h, int(n), float(beta)), "runRec")
+
+    def iterate(self, iters, beta):
+        _check(self.L, self.L.m3drec_iterate(self.h, int(iters), float(beta)), "iterate")
+
+    def threshold(self):
+        _check(self.L, self.L.m3drec_threshold(self.h), "threshold")
+
+    def set_state(self, field, i, j, call):
+        f = np.ascontiguousarray(np.asarray(field, np.complex128).ravel())
+        if f.size != self.xyz:
+            raise ValueError("field must hold Nx * Ny * Nz complex values")
+        _check(self.L, self.L.m3drec_set_state(self.h, _ptr(f), int(i), int(j), int(call)), "set_state")
+
+    def get_state(self):
+        f = np.zeros(self.xyz, np.complex128)
+        i, j, c = ctypes.c_int(), ctypes.c_int(), ctypes.c_ulonglong()
+        _check(self.L, self.L.m3drec_get_state(self.h, _ptr(f), ctypes.byref(i), ctypes.byref(j), ctypes.byref(c)),
+               "get_state")
+        return dict(field=f, i=i.value, j=j.value, call=c.value)
+
+    def field(self):
+        out = np.zeros(self.xyz)
+        _check(self.L, self.L.m3drec_get_field(self.h, _ptr(out)), "get_field")
+        return out
+
+    def errors(self):
+        n = ctypes.c_int()
+        _check(self.L, self.L.m3drec_get_error(self.h, None, 0, ctypes.byref(n)), "get_error")
+        out = np.zeros(n.value)
+        _check(self.L, self.L.m3drec_get_error(self.h, _ptr(out), n.value, ctypes.byref(n)), "get_error")
+        return out
+
+    def set_profiling(self, on):
+        _check(self.L, self.L.m3drec_set_profiling(self.h, 1 if on else 0), "set_profiling")
+
+    def profile(self):
+        ms = np.zeros(6)
+        n = ctypes.c_longlong()
+        _check(self.L, self.L.m3drec_profile(self.h, _ptr(ms), ctypes.byref(n)), "profile")
+        return ms, n.value
+
+    def kernel_launches(self):
+        return int(self.L.m3drec_kernel_launches(self.h))
+
+    def stream_ptr(self):
+        return self.L.m3drec_get_stream(self.h)
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.m3drec_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class recPlan:
+    """Drop-in mirror of ``recon::recPlan`` built from a two-point correlation
+    function (include/reconstruction.hpp:46-96): ``recPlan(TPCF, Nx, Ny, Nz)``,
+    ``runRec(n, b)``, the members ``mTilda`` (the reconstructed field, real
+    part; 0/1 after runRec) and ``trackrealerrorA`` (error of every pass run).
+    ``seed`` picks the random draws (the reference's come from std::rand)."""
+
+    def __init__(self, TPCF, Nx1, Ny1, Nz1, seed=1):
+        self.Nx, self.Ny, self.Nz = Nx1, Ny1, Nz1
+        self._r = Reconstruction(TPCF, Nx1, Ny1, Nz1)
+        self._r.seed(seed)
+        self.trackrealerrorA = np.zeros(0)
+        self.mTilda = None
+
+    def runRec(self, n, b):
+        self._r.run(n, b)
+        e = self._r.errors()
+        self.trackrealerrorA = np.zeros(n)
+        self.trackrealerrorA[:min(n, e.size)] = e[:n]
+        self.mTilda = self._r.field()
+
+    def close(self):
+        self._r.close()

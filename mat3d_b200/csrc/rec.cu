@@ -1,0 +1,851 @@
+// rec.cu -- microstructure reconstruction by phase retrieval (recon::recPlan,
+// src/rec/reconstruction.cpp) on the GPU.
+//
+// Given the modulus |M(k)| = normC = sqrt(|TPCF| * xyz) of the 3-D Fourier
+// transform of a two-phase field, runRec(n, beta) looks for a field m in
+// [0, 1] with that modulus (:283-400):
+//     m = (U + 1) / 2                                   (U uniform in [-1, 1))
+//     loop: M = FFT(m); err = mean | |M| - normC |; stop if err < 0.1 or i >= n
+//           ang = arg M   (every 150th pass: 0.3 arg FFT(U') + 0.7 arg M)
+//           m' = IFFT(normC e^{i ang}) / xyz
+//           j < 100:  hybrid input-output  m' < 0 -> m - beta m' ; m' > 1 -> m - beta (m' - 1) ; m' > 1 -> 1
+//           j >= 100: box projection       m' < 0 -> 0 ; m' > 1 -> 1 ; j > 200 -> j = 0
+//           (the imaginary part is zeroed only where a projection fired)
+//     threshold m at 0.5 - x, moving x by 0.001 until the phase-1 fraction is
+//     within 1e-4 of normC[0] / xyz (at most 202 tries).
+//
+// Layout: complex FP64 fields in the reference's voxel order v = z + Nz (y + Ny x).
+// One pass of the loop = 5 launches over the work buffer A:
+//   zfwd  (m -> A, z lines)  yfwd (y lines)  xturn (x FFT, error partials,
+//   modulus replacement, inverse x FFT; its last CTA reduces the error in a
+//   fixed order and advances the loop state)  yinv  zinv (z lines, 1/xyz,
+//   projection -> m).
+// A restart pass adds three launches before them that transform U' (drawn in
+// the z-pass load, never stored) and keep 0.3 arg FFT(U') in R.  Those three
+// return at once on other passes.  Everything the loop decides (i, j, the
+// draw counter, convergence) lives in a device control block, so the whole
+// loop is one CUDA graph with a conditional while node; the threshold walk is
+// a second while node (an integer count per try, so it is exact).
+//
+// Random draws: the reference calls Eigen's setRandom (std::rand underneath,
+// implementation defined).  Here draw number `call` (0 = the initial field,
+// then one per restart) of voxel v is 2 u - 1 with
+//   u = (mix(mix(seed * 0x100000001B3 + call) + v) >> 11) * 2^-53,
+// mix = the SplitMix64 finaliser: the CPU restatement and the stand-in Eigen
+// the reference is built against for testing use the same formula.
+//
+// Arithmetic that the reference writes as separate operations is kept
+// separate (__dmul_rn / __dadd_rn / __dsub_rn) so no fused multiply-add
+// changes its rounding; the transforms themselves round differently from any
+// CPU FFT, and the iteration amplifies such differences (about threefold per
+// pass), so long runs agree with the CPU statistically, not bit for bit.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/mat3d_b200.h"
+#include "fft_plan.hpp"
+#include "fft_smem.cuh"
+
+using namespace m3d;
+
+void m3d_internal_set_error(const std::string& msg);
+
+namespace {
+
+int failr(int code, const std::string& msg) {
+    m3d_internal_set_error(msg);
+    return code;
+}
+
+#define MR_CUDA(call)                                                                \
+    do {                                                                             \
+        cudaError_t e_ = (call);                                                     \
+        if (e_ != cudaSuccess) return failr(M3D_ERR_CUDA, cudaGetErrorString(e_)); \
+    } while (0)
+
+constexpr int kThreads = 256;
+constexpr int kRestartPeriod = 150;  // remainder(i + 1, 150) == 0 (:320)
+
+struct RecCtl {
+    int i, j, n, done;      // loop counters (:287-288), stop bound, 1 = converged
+    int hio, trips, ctr, thr_done;
+    unsigned int ticket, pad0;
+    unsigned long long seed, call;  // generator seed, draws taken so far
+    unsigned long long count_lt;    // threshold: voxels below the cut
+    double beta, x, cut;            // HIO beta; threshold offset and the cut last applied
+    double normC0;                  // normC[0]
+    long long xyz;
+};
+
+__device__ __forceinline__ unsigned long long mix64(unsigned long long z) {
+    z += 0x9E3779B97F4A7C15ULL;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+    return z ^ (z >> 31);
+}
+__device__ __forceinline__ unsigned long long draw_base(unsigned long long seed, unsigned long long call) {
+    return mix64(seed * 0x100000001B3ULL + call);
+}
+// 2 u - 1: both steps are exact in double (u has 53 bits, 2 u is a scaling)
+__device__ __forceinline__ double draw_pm1(unsigned long long base, unsigned long long v) {
+    const double u = (double)(mix64(base + v) >> 11) * (1.0 / 9007199254740992.0);
+    return __dsub_rn(__dmul_rn(2.0, u), 1.0);
+}
+
+__device__ __forceinline__ bool restart_pass(const RecCtl* c) { return !c->done && (c->i + 1) % kRestartPeriod == 0; }
+
+// initial field (:289-291): m = (U + 1) * 0.5 from draw 0
+__global__ void krec_init(double2* __restrict__ m, RecCtl* ctl, long long xyz) {
+    const unsigned long long base = draw_base(ctl->seed, 0);
+    for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < xyz; v += (long long)gridDim.x * blockDim.x)
+        m[v] = make_double2(__dmul_rn(__dadd_rn(draw_pm1(base, (unsigned long long)v), 1.0), 0.5), 0.0);
+}
+
+enum ZMode { Z_FWD = 0, Z_RAND = 1, Z_INV = 2 };
+
+// z lines (contiguous): G lines of length Nz per CTA.
+//   Z_FWD : A = FFT_z(m)
+//   Z_RAND: A = FFT_z(U') on restart passes (U' = draw `call`, real)
+//   Z_INV : m = projection(IFFT_z(A) / xyz, m) unless the pass converged
+template <int MODE>
+__global__ void __launch_bounds__(kThreads) krec_z(double2* __restrict__ A, double2* __restrict__ m,
+                                                    const double2* __restrict__ twz, LinePlan pz, int G,
+                                                    long long nlines, const RecCtl* __restrict__ ctl) {
+    if (MODE == Z_RAND && !restart_pass(ctl)) return;
+    if (MODE == Z_INV && ctl->done) return;
+    extern __shared__ __align__(16) char smem_raw[];
+    const int Nz = pz.n;
+    double2* tw = (double2*)smem_raw;
+    double2* S0 = tw + Nz;
+    double2* S1 = S0 + (size_t)G * Nz;
+    const long long l0 = (long long)blockIdx.x * G;
+    const long long xyz = ctl->xyz;
+    for (int t = threadIdx.x; t < Nz; t += blockDim.x) tw[t] = twz[t];
+    unsigned long long base = 0;
+    if (MODE == Z_RAND) base = draw_base(ctl->seed, ctl->call);
+    for (int t = threadIdx.x; t < G * Nz; t += blockDim.x) {
+        const long long l = l0 + t / Nz;
+        const long long v = l * Nz + t % Nz;
+        double2 w = make_double2(0, 0);
+        if (l < nlines) {
+            if (MODE == Z_FWD) w = m[v];
+            else if (MODE == Z_RAND) w = make_double2(draw_pm1(base, (unsigned long long)v), 0.0);
+            else w = A[v];
+        }
+        S0[t] = w;
+    }
+    __syncthreads();
+    LineLayout L{G, G, Nz, 0, 1, false};
+    double2* r = fft_lines(S0, S1, tw, pz, L, MODE == Z_INV ? +1 : -1);
+    if (MODE != Z_INV) {
+        for (int t = threadIdx.x; t < G * Nz; t += blockDim.x) {
+            const long long l = l0 + t / Nz;
+            if (l < nlines) A[l * Nz + t % Nz] = r[t];
+        }
+        return;
+    }
+    // temp = temp / xyz, then the projections (:345-364)
+    const double dxyz = (double)xyz;
+    const double beta = ctl->beta;
+    const bool hio = ctl->hio != 0;
+    for (int t = threadIdx.x; t < G * Nz; t += blockDim.x) {
+        const long long l = l0 + t / Nz;
+        if (l >= nlines) continue;
+        const long long v = l * Nz + t % Nz;
+        const double2 w = r[t];
+        double re = w.x / dxyz, im = w.y / dxyz;
+        if (hio) {
+            const double old = m[v].x;
+            if (re < 0) { re = __dsub_rn(old, __dmul_rn(beta, re)); im = 0; }
+            if (re > 1) { re = __dsub_rn(old, __dmul_rn(beta, __dsub_rn(re, 1.0))); im = 0; }
+            if (re > 1) { re = 1; im = 0; }
+        } else {
+            if (re < 0) { re = 0; im = 0; }
+            if (re > 1) { re = 1; im = 0; }
+        }
+        m[v] = make_double2(re, im);
+    }
+}
+
+// column passes (y or x lines): TZ consecutive z columns of one plane, N
+// elements each at `stride`; smem element e of column t at e * TZ + t.
+struct ColTile {
+    long long base;  // offset of element 0 of column 0
+    long long stride;
+    int nz;          // columns present in this tile
+};
+
+__device__ __forceinline__ void col_load(double2* S, const double2* __restrict__ A, const ColTile& c, int N, int TZ) {
+    for (int t = threadIdx.x; t < N * TZ; t += blockDim.x) {
+        const int tz = t % TZ, e = t / TZ;
+        S[t] = tz < c.nz ? A[c.base + e * c.stride + tz] : make_double2(0, 0);
+    }
+}
+__device__ __forceinline__ void col_store(double2* __restrict__ A, const double2* S, const ColTile& c, int N, int TZ) {
+    for (int t = threadIdx.x; t < N * TZ; t += blockDim.x) {
+        const int tz = t % TZ, e = t / TZ;
+        if (tz < c.nz) A[c.base + e * c.stride + tz] = S[t];
+    }
+}
+
+enum YMode { Y_FWD = 0, Y_RAND = 1, Y_INV = 2 };
+
+// y lines: CTA (x, z tile); in place on A
+template <int MODE>
+__global__ void __launch_bounds__(kThreads) krec_y(double2* __restrict__ A, const double2* __restrict__ twy,
+                                                    LinePlan py, int Nz, int TZ, int ntz, const RecCtl* __restrict__ ctl) {
+    if (MODE == Y_RAND && !restart_pass(ctl)) return;
+    if (MODE == Y_INV && ctl->done) return;
+    extern __shared__ __align__(16) char smem_raw[];
+    const int Ny = py.n;
+    double2* tw = (double2*)smem_raw;
+    double2* S0 = tw + Ny;
+    double2* S1 = S0 + (size_t)Ny * TZ;
+    const int x = blockIdx.x / ntz, z0 = (blockIdx.x % ntz) * TZ;
+    const ColTile c{(long long)x * Ny * Nz + z0, Nz, min(TZ, Nz - z0)};
+    for (int t = threadIdx.x; t < Ny; t += blockDim.x) tw[t] = twy[t];
+    col_load(S0, A, c, Ny, TZ);
+    __syncthreads();
+    LineLayout L{TZ, TZ, 1, 0, TZ, true};
+    const double2* r = fft_lines(S0, S1, tw, py, L, MODE == Y_INV ? +1 : -1);
+    col_store(A, r, c, Ny, TZ);
+}
+
+// x lines of a restart pass: R = 0.3 arg FFT(U') (:326-327)
+__global__ void __launch_bounds__(kThreads) krec_xrand(const double2* __restrict__ A, double* __restrict__ R,
+                                                        const double2* __restrict__ twx, LinePlan px, int Ny, int Nz,
+                                                        int TZ, int ntz, const RecCtl* __restrict__ ctl) {
+    if (!restart_pass(ctl)) return;
+    extern __shared__ __align__(16) char smem_raw[];
+    const int Nx = px.n;
+    double2* tw = (double2*)smem_raw;
+    double2* S0 = tw + Nx;
+    double2* S1 = S0 + (size_t)Nx * TZ;
+    const int y = blockIdx.x / ntz, z0 = (blockIdx.x % ntz) * TZ;
+    const ColTile c{(long long)y * Nz + z0, (long long)Ny * Nz, min(TZ, Nz - z0)};
+    for (int t = threadIdx.x; t < Nx; t += blockDim.x) tw[t] = twx[t];
+    col_load(S0, A, c, Nx, TZ);
+    __syncthreads();
+    LineLayout L{TZ, TZ, 1, 0, TZ, true};
+    const double2* r = fft_lines(S0, S1, tw, px, L, -1);
+    for (int t = threadIdx.x; t < Nx * TZ; t += blockDim.x) {
+        const int tz = t % TZ, e = t / TZ;
+        if (tz < c.nz) R[c.base + e * c.stride + tz] = __dmul_rn(atan2(r[t].y, r[t].x), 0.3);
+    }
+}
+
+// x turnaround: forward x FFT (M = FFT(m) complete), error partials
+// (funcNormC, include/reconstruction.hpp:37-44), modulus replacement
+// (:317-336), inverse x FFT.  The last CTA to finish reduces the partials in
+// a fixed order, records err[i] and advances the loop state (:300-314, :360-365).
+__global__ void __launch_bounds__(kThreads) krec_xturn(double2* __restrict__ A, const double* __restrict__ normC,
+                                                        const double* __restrict__ R, const double2* __restrict__ twx,
+                                                        LinePlan px, int Ny, int Nz, int TZ, int ntz,
+                                                        double* __restrict__ part, double* __restrict__ errs,
+                                                        RecCtl* ctl) {
+    extern __shared__ __align__(16) char smem_raw[];
+    __shared__ double red[kThreads / 32];
+    __shared__ bool last;
+    const int Nx = px.n;
+    double2* tw = (double2*)smem_raw;
+    double2* S0 = tw + Nx;
+    double2* S1 = S0 + (size_t)Nx * TZ;
+    const int y = blockIdx.x / ntz, z0 = (blockIdx.x % ntz) * TZ;
+    const ColTile c{(long long)y * Nz + z0, (long long)Ny * Nz, min(TZ, Nz - z0)};
+    const bool restart = restart_pass(ctl);
+    for (int t = threadIdx.x; t < Nx; t += blockDim.x) tw[t] = twx[t];
+    col_load(S0, A, c, Nx, TZ);
+    __syncthreads();
+    LineLayout L{TZ, TZ, 1, 0, TZ, true};
+    double2* r = fft_lines(S0, S1, tw, px, L, -1);
+    double2* o = (r == S0) ? S1 : S0;
+    double acc = 0;
+    for (int t = threadIdx.x; t < Nx * TZ; t += blockDim.x) {
+        const int tz = t % TZ, e = t / TZ;
+        if (tz >= c.nz) continue;  // padding columns stay zero through the inverse transform
+        const long long v = c.base + e * c.stride + tz;
+        const double2 w = r[t];
+        const double nc = normC[v];
+        acc += fabs(__dsub_rn(sqrt(__dadd_rn(__dmul_rn(w.x, w.x), __dmul_rn(w.y, w.y))), nc));
+        double ang = atan2(w.y, w.x);
+        if (restart) ang = __dadd_rn(R[v], __dmul_rn(ang, 0.7));
+        double s, co;
+        sincos(ang, &s, &co);
+        r[t] = make_double2(__dmul_rn(nc, co), __dmul_rn(nc, s));
+    }
+    // block partial in a fixed order: warp shuffle tree, then the warps in order
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, off);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    const double2* q = fft_lines(r, o, tw, px, L, +1);
+    col_store(A, q, c, Nx, TZ);
+    if (threadIdx.x == 0) {
+        double b = 0;
+        for (int w = 0; w < kThreads / 32; ++w) b += red[w];
+        part[blockIdx.x] = b;
+        __threadfence();
+        last = atomicAdd(&ctl->ticket, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!last || threadIdx.x >= 32) return;
+    __threadfence();
+    double s = 0;
+    for (int k = threadIdx.x; k < (int)gridDim.x; k += 32) s += __ldcg(part + k);
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) s += __shfl_down_sync(0xffffffffu, s, off);
+    if (threadIdx.x != 0) return;
+    const int i = ctl->i;
+    int j = ctl->j + 1;  // j += 1 at the top of the pass (:296)
+    const double err = s / (double)ctl->xyz;
+    errs[i] = err;
+    if (err < 0.1) {  // converged: the field stays as it is (:310-314)
+        ctl->done = 1;
+    } else {
+        if (restart) ctl->call += 1;
+        ctl->hio = j < 100;
+        if (j >= 100 && j > 200) j = 0;
+        ctl->i = i + 1;
+    }
+    ctl->j = j;
+    ctl->ticket = 0;
+}
+
+// loop condition: another pass while not converged, i < n, and (bound) at most n + 2 trips
+__global__ void krec_cond(cudaGraphConditionalHandle h, RecCtl* ctl) {
+    const int t = ++ctl->trips;
+    cudaGraphSetConditional(h, (!ctl->done && ctl->i < ctl->n && t <= ctl->n + 2) ? 1u : 0u);
+}
+
+// threshold walk (:370-395): one try = count voxels below 0.5 - x, then step x
+__global__ void krec_thr_count(const double2* __restrict__ m, RecCtl* ctl, long long xyz) {
+    __shared__ unsigned int red[kThreads / 32];
+    const double cut = __dsub_rn(0.5, ctl->x);
+    unsigned int cnt = 0;
+    for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < xyz; v += (long long)gridDim.x * blockDim.x)
+        cnt += m[v].x < cut ? 1u : 0u;
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) cnt += __shfl_down_sync(0xffffffffu, cnt, off);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = cnt;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned long long b = 0;
+        for (int w = 0; w < kThreads / 32; ++w) b += red[w];
+        if (b) atomicAdd(&ctl->count_lt, b);
+    }
+}
+
+__global__ void krec_thr_step(cudaGraphConditionalHandle h, RecCtl* ctl, int use_cond) {
+    const long long xyz = ctl->xyz;
+    const double ones = (double)(xyz - (long long)ctl->count_lt);  // ang.sum() of the 0/1 field
+    const double vol_dif = __dsub_rn(ones / (1.0 * xyz), ctl->normC0 / (1.0 * xyz));
+    ctl->cut = __dsub_rn(0.5, ctl->x);
+    if (vol_dif > 0) ctl->x = __dsub_rn(ctl->x, 0.001);
+    else ctl->x = __dadd_rn(ctl->x, 0.001);
+    const bool stop = fabs(vol_dif) < 0.0001 || ctl->ctr > 200;
+    if (!stop) ctl->ctr += 1;
+    ctl->thr_done = stop;
+    ctl->count_lt = 0;
+    const int t = ++ctl->trips;
+    if (use_cond) cudaGraphSetConditional(h, (!stop && t <= 203) ? 1u : 0u);
+}
+
+// the field after the walk: real part 0 / 1 at the last cut, imaginary part kept (:397)
+__global__ void krec_thr_apply(double2* __restrict__ m, const RecCtl* __restrict__ ctl, long long xyz) {
+    const double cut = ctl->cut;
+    for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < xyz; v += (long long)gridDim.x * blockDim.x)
+        m[v].x = m[v].x < cut ? 0.0 : 1.0;
+}
+
+__global__ void krec_real(const double2* __restrict__ m, double* __restrict__ out, long long xyz) {
+    for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < xyz; v += (long long)gridDim.x * blockDim.x)
+        out[v] = m[v].x;
+}
+
+cudaError_t add_while(cudaGraph_t graph, const cudaGraphNode_t* deps, size_t ndeps, cudaGraphConditionalHandle h,
+                      cudaGraphNode_t* node, cudaGraph_t* body) {
+    cudaGraphNodeParams p = {cudaGraphNodeTypeConditional};  // the remaining members are zero
+    p.conditional.handle = h;
+    p.conditional.type = cudaGraphCondTypeWhile;
+    p.conditional.size = 1;
+    cudaError_t e = cudaGraphAddNode(node, graph, deps, ndeps, &p);
+    if (e == cudaSuccess) *body = p.conditional.phGraph_out[0];
+    return e;
+}
+
+}  // namespace
+
+struct m3d_rec {
+    int Nx = 0, Ny = 0, Nz = 0;
+    long long xyz = 0;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    double2 *m = nullptr, *A = nullptr, *twx = nullptr, *twy = nullptr, *twz = nullptr;
+    double *R = nullptr, *normC = nullptr, *part = nullptr, *errs = nullptr, *real = nullptr;
+    int err_cap = 0;
+    RecCtl* d_ctl = nullptr;
+    RecCtl* h_ctl = nullptr;  // pinned mirror
+    LinePlan px{}, py{}, pz{};
+    int G = 1, TZ = 1, ntz = 1;
+    long long zlines = 0;
+    int nb_y = 0, nb_x = 0;
+    double normC0 = 0;
+    unsigned long long seed = 1;
+    bool started = false;   // a field exists (run, set_state)
+    int i = 0, j = 0;       // host copy of the loop state
+    unsigned long long call = 0;
+    int n_recorded = 0;
+    bool profiling = false;
+    double pass_ms[8] = {0};
+    long long pass_count[8] = {0};
+    cudaEvent_t ev[9] = {};
+    cudaGraphExec_t g_loop = nullptr, g_thr = nullptr;
+    long long launches = 0;
+
+    ~m3d_rec() {
+        if (g_loop) cudaGraphExecDestroy(g_loop);
+        if (g_thr) cudaGraphExecDestroy(g_thr);
+        for (auto& e : ev)
+            if (e) cudaEventDestroy(e);
+        cudaFree(m); cudaFree(A); cudaFree(twx); cudaFree(twy); cudaFree(twz);
+        cudaFree(R); cudaFree(normC); cudaFree(part); cudaFree(errs); cudaFree(real); cudaFree(d_ctl);
+        if (h_ctl) cudaFreeHost(h_ctl);
+        if (stream) cudaStreamDestroy(stream);
+    }
+    size_t z_smem() const { return (size_t)Nz * 16 + 2 * (size_t)G * Nz * 16; }
+    size_t y_smem() const { return (size_t)Ny * 16 + 2 * (size_t)Ny * TZ * 16; }
+    size_t x_smem() const { return (size_t)Nx * 16 + 2 * (size_t)Nx * TZ * 16; }
+    int grid1d() const { return (int)std::min<long long>(148 * 8, (xyz + kThreads - 1) / kThreads); }
+
+    // the kernels of one pass, in order; `prof` brackets each with events
+    int launch_pass(bool prof) {
+        const int nbz = (int)((zlines + G - 1) / G);
+        auto mark = [&](int k) { if (prof) cudaEventRecord(ev[k], stream); };
+        mark(0);
+        krec_z<Z_RAND><<<nbz, kThreads, z_smem(), stream>>>(A, m, twz, pz, G, zlines, d_ctl);
+        krec_y<Y_RAND><<<nb_y, kThreads, y_smem(), stream>>>(A, twy, py, Nz, TZ, ntz, d_ctl);
+        krec_xrand<<<nb_x, kThreads, x_smem(), stream>>>(A, R, twx, px, Ny, Nz, TZ, ntz, d_ctl);
+        mark(1);
+        krec_z<Z_FWD><<<nbz, kThreads, z_smem(), stream>>>(A, m, twz, pz, G, zlines, d_ctl);
+        mark(2);
+        krec_y<Y_FWD><<<nb_y, kThreads, y_smem(), stream>>>(A, twy, py, Nz, TZ, ntz, d_ctl);
+        mark(3);
+        krec_xturn<<<nb_x, kThreads, x_smem(), stream>>>(A, normC, R, twx, px, Ny, Nz, TZ, ntz, part, errs, d_ctl);
+        mark(4);
+        krec_y<Y_INV><<<nb_y, kThreads, y_smem(), stream>>>(A, twy, py, Nz, TZ, ntz, d_ctl);
+        mark(5);
+        krec_z<Z_INV><<<nbz, kThreads, z_smem(), stream>>>(A, m, twz, pz, G, zlines, d_ctl);
+        mark(6);
+        launches += 8;
+        MR_CUDA(cudaGetLastError());
+        return M3D_OK;
+    }
+
+    // grow the error track, keeping what it holds
+    int ensure_err(int n) {
+        if (n <= err_cap) return M3D_OK;
+        double* e = nullptr;
+        if (cudaMalloc(&e, (size_t)n * sizeof(double)) != cudaSuccess) {
+            (void)cudaGetLastError();
+            return failr(M3D_ERR_OOM, "device allocation failed");
+        }
+        MR_CUDA(cudaMemsetAsync(e, 0, (size_t)n * sizeof(double), stream));
+        if (err_cap > 0) MR_CUDA(cudaMemcpyAsync(e, errs, (size_t)err_cap * sizeof(double), cudaMemcpyDeviceToDevice, stream));
+        MR_CUDA(cudaStreamSynchronize(stream));
+        cudaFree(errs);
+        errs = e;
+        err_cap = n;
+        if (g_loop) { cudaGraphExecDestroy(g_loop); g_loop = nullptr; }  // the graph holds the old pointer
+        return M3D_OK;
+    }
+
+    int build_loop_graph() {
+        cudaGraph_t top = nullptr;
+        MR_CUDA(cudaGraphCreate(&top, 0));
+        cudaGraphConditionalHandle h;
+        cudaGraphNode_t node;
+        cudaGraph_t body = nullptr;
+        cudaError_t e = cudaGraphConditionalHandleCreate(&h, top, 1, cudaGraphCondAssignDefault);
+        if (e == cudaSuccess) e = add_while(top, nullptr, 0, h, &node, &body);
+        if (e == cudaSuccess) e = cudaStreamBeginCaptureToGraph(stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed);
+        if (e == cudaSuccess) {
+            const long long kl = launches;
+            launch_pass(false);
+            krec_cond<<<1, 1, 0, stream>>>(h, d_ctl);
+            launches = kl;
+            cudaGraph_t got = nullptr;
+            e = cudaGetLastError();
+            const cudaError_t e2 = cudaStreamEndCapture(stream, &got);
+            if (e == cudaSuccess) e = e2;
+        }
+        if (e == cudaSuccess) e = cudaGraphInstantiate(&g_loop, top, 0);
+        cudaGraphDestroy(top);
+        if (e != cudaSuccess) {
+            g_loop = nullptr;
+            (void)cudaGetLastError();
+            return failr(M3D_ERR_CUDA, std::string("reconstruction graph: ") + cudaGetErrorString(e));
+        }
+        return M3D_OK;
+    }
+
+    int build_thr_graph() {
+        cudaGraph_t top = nullptr;
+        MR_CUDA(cudaGraphCreate(&top, 0));
+        cudaGraphConditionalHandle h;
+        cudaGraphNode_t node;
+        cudaGraph_t body = nullptr;
+        cudaError_t e = cudaGraphConditionalHandleCreate(&h, top, 1, cudaGraphCondAssignDefault);
+        if (e == cudaSuccess) e = add_while(top, nullptr, 0, h, &node, &body);
+        if (e == cudaSuccess) e = cudaStreamBeginCaptureToGraph(stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed);
+        if (e == cudaSuccess) {
+            krec_thr_count<<<grid1d(), kThreads, 0, stream>>>(m, d_ctl, xyz);
+            krec_thr_step<<<1, 1, 0, stream>>>(h, d_ctl, 1);
+            cudaGraph_t got = nullptr;
+            e = cudaGetLastError();
+            const cudaError_t e2 = cudaStreamEndCapture(stream, &got);
+            if (e == cudaSuccess) e = e2;
+        }
+        if (e == cudaSuccess) e = cudaGraphInstantiate(&g_thr, top, 0);
+        cudaGraphDestroy(top);
+        if (e != cudaSuccess) {
+            g_thr = nullptr;
+            (void)cudaGetLastError();
+            return failr(M3D_ERR_CUDA, std::string("threshold graph: ") + cudaGetErrorString(e));
+        }
+        return M3D_OK;
+    }
+
+    int pull_ctl() {
+        MR_CUDA(cudaMemcpyAsync(h_ctl, d_ctl, sizeof(RecCtl), cudaMemcpyDeviceToHost, stream));
+        MR_CUDA(cudaStreamSynchronize(stream));
+        return M3D_OK;
+    }
+
+    // continue the loop until converged or i reaches n_stop
+    int iterate(int n_stop, double beta) {
+        if (n_stop > err_cap) {
+            const int rc = ensure_err(std::max(n_stop, 2 * err_cap));
+            if (rc) return rc;
+        }
+        // errors recorded before this call stay (the device array keeps them)
+        RecCtl c{};
+        c.i = i; c.j = j; c.n = n_stop; c.done = 0; c.hio = 1; c.trips = 0;
+        c.seed = seed; c.call = call; c.beta = beta; c.normC0 = normC0; c.xyz = xyz;
+        *h_ctl = c;
+        MR_CUDA(cudaMemcpyAsync(d_ctl, h_ctl, sizeof(RecCtl), cudaMemcpyHostToDevice, stream));
+        if (i < n_stop) {
+            if (profiling) {
+                for (int t = 0; t < n_stop - i + 1; ++t) {
+                    int rc = launch_pass(true);
+                    if (rc) return rc;
+                    rc = pull_ctl();
+                    if (rc) return rc;
+                    float ms;
+                    for (int k = 0; k < 6; ++k) {
+                        cudaEventElapsedTime(&ms, ev[k], ev[k + 1]);
+                        pass_ms[k] += ms;
+                        pass_count[k] += 1;
+                    }
+                    if (h_ctl->done || h_ctl->i >= n_stop) break;
+                }
+            } else {
+                if (!g_loop) {
+                    const int rc = build_loop_graph();
+                    if (rc) return rc;
+                }
+                MR_CUDA(cudaGraphLaunch(g_loop, stream));
+                launches += 1;
+                const int rc = pull_ctl();
+                if (rc) return rc;
+                launches += 9LL * h_ctl->trips;
+            }
+        }
+        const int rc = pull_ctl();
+        if (rc) return rc;
+        if (h_ctl->trips > n_stop + 2) return failr(M3D_ERR_CUDA, "reconstruction loop exceeded its trip bound");
+        i = h_ctl->i;
+        j = h_ctl->j;
+        call = h_ctl->call;
+        n_recorded = h_ctl->done ? i + 1 : i;
+        return M3D_OK;
+    }
+
+    int threshold() {
+        RecCtl c{};
+        c.normC0 = normC0; c.xyz = xyz; c.x = 0; c.ctr = 0; c.count_lt = 0; c.trips = 0;
+        c.i = i; c.j = j; c.seed = seed; c.call = call;
+        *h_ctl = c;
+        MR_CUDA(cudaMemcpyAsync(d_ctl, h_ctl, sizeof(RecCtl), cudaMemcpyHostToDevice, stream));
+        if (profiling) {
+            for (int t = 0; t < 203; ++t) {
+                krec_thr_count<<<grid1d(), kThreads, 0, stream>>>(m, d_ctl, xyz);
+                krec_thr_step<<<1, 1, 0, stream>>>(cudaGraphConditionalHandle{}, d_ctl, 0);
+                launches += 2;
+                MR_CUDA(cudaGetLastError());
+                const int rc = pull_ctl();
+                if (rc) return rc;
+                if (h_ctl->thr_done) break;
+            }
+        } else {
+            if (!g_thr) {
+                const int rc = build_thr_graph();
+                if (rc) return rc;
+            }
+            MR_CUDA(cudaGraphLaunch(g_thr, stream));
+            launches += 1;
+        }
+        krec_thr_apply<<<grid1d(), kThreads, 0, stream>>>(m, d_ctl, xyz);
+        launches += 1;
+        MR_CUDA(cudaGetLastError());
+        const int rc = pull_ctl();
+        if (rc) return rc;
+        if (!profiling) launches += 2LL * h_ctl->trips;
+        if (!h_ctl->thr_done) return failr(M3D_ERR_CUDA, "threshold walk did not finish");
+        return M3D_OK;
+    }
+};
+
+extern "C" {
+
+int m3drec_create(int Nx, int Ny, int Nz, const double* tpcf, int device, m3d_rec** out) {
+    if (!out) return failr(M3D_ERR_ARG, "out is NULL");
+    *out = nullptr;
+    if (!tpcf) return failr(M3D_ERR_ARG, "tpcf is NULL");
+    if (Nx < 1 || Ny < 1 || Nz < 1 || Nx > 2048 || Ny > 2048 || Nz > 2048)
+        return failr(M3D_ERR_ARG, "grid sizes must be in [1, 2048]");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return failr(M3D_ERR_CUDA, "no CUDA device");
+    if (device < 0 || device >= ndev) return failr(M3D_ERR_ARG, "device out of range");
+    MR_CUDA(cudaSetDevice(device));
+    m3d_rec* h = new m3d_rec();
+    h->Nx = Nx; h->Ny = Ny; h->Nz = Nz;
+    h->xyz = (long long)Nx * Ny * Nz;
+    h->device = device;
+    if (!make_plan(Nx, h->px) || !make_plan(Ny, h->py) || !make_plan(Nz, h->pz)) {
+        delete h;
+        return failr(M3D_ERR_UNSUPPORTED, "grid sizes need prime factors <= 32");
+    }
+    h->G = std::max(1, std::min(16, (int)(48 * 1024 / (32 * (size_t)Nz))));
+    const int nmax = std::max(Nx, Ny);
+    h->TZ = std::max(1, std::min(16, (int)(96 * 1024 / (32 * (size_t)nmax))));
+    h->TZ = std::min(h->TZ, Nz);
+    h->ntz = (Nz + h->TZ - 1) / h->TZ;
+    h->zlines = (long long)Nx * Ny;
+    h->nb_y = Nx * h->ntz;
+    h->nb_x = Ny * h->ntz;
+    if (h->z_smem() > 220 * 1024 || h->y_smem() > 220 * 1024 || h->x_smem() > 220 * 1024) {
+        delete h;
+        return failr(M3D_ERR_UNSUPPORTED, "grid too large for the shared-memory line FFTs");
+    }
+    const size_t c16 = (size_t)h->xyz * sizeof(double2), c8 = (size_t)h->xyz * sizeof(double);
+    if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaMalloc(&h->m, c16) != cudaSuccess || cudaMalloc(&h->A, c16) != cudaSuccess ||
+        cudaMalloc(&h->R, c8) != cudaSuccess || cudaMalloc(&h->normC, c8) != cudaSuccess ||
+        cudaMalloc(&h->part, (size_t)h->nb_x * sizeof(double)) != cudaSuccess ||
+        cudaMalloc(&h->twx, Nx * sizeof(double2)) != cudaSuccess ||
+        cudaMalloc(&h->twy, Ny * sizeof(double2)) != cudaSuccess ||
+        cudaMalloc(&h->twz, Nz * sizeof(double2)) != cudaSuccess ||
+        cudaMalloc(&h->d_ctl, sizeof(RecCtl)) != cudaSuccess ||
+        cudaMallocHost(&h->h_ctl, sizeof(RecCtl)) != cudaSuccess) {
+        delete h;
+        (void)cudaGetLastError();
+        return failr(M3D_ERR_OOM, "device allocation failed");
+    }
+    for (auto& e : h->ev)
+        if (cudaEventCreate(&e) != cudaSuccess) {
+            delete h;
+            return failr(M3D_ERR_CUDA, "event creation failed");
+        }
+    // normC = sqrt(|TPCF| * xyz) (:238-239)
+    std::vector<double> nc((size_t)h->xyz);
+    for (long long v = 0; v < h->xyz; ++v) nc[v] = std::sqrt(std::fabs(tpcf[v]) * (double)h->xyz);
+    h->normC0 = nc[0];
+    const auto tx = twiddles<double>(Nx), ty = twiddles<double>(Ny), tz = twiddles<double>(Nz);
+    cudaMemcpy(h->normC, nc.data(), c8, cudaMemcpyHostToDevice);
+    cudaMemcpy(h->twx, tx.data(), Nx * sizeof(double2), cudaMemcpyHostToDevice);
+    cudaMemcpy(h->twy, ty.data(), Ny * sizeof(double2), cudaMemcpyHostToDevice);
+    cudaMemcpy(h->twz, tz.data(), Nz * sizeof(double2), cudaMemcpyHostToDevice);
+    cudaMemset(h->m, 0, c16);
+    cudaMemset(h->R, 0, c8);
+    cudaMemset(h->d_ctl, 0, sizeof(RecCtl));
+    const int zs = (int)h->z_smem(), ys = (int)h->y_smem(), xs = (int)h->x_smem();
+    cudaFuncSetAttribute(krec_z<Z_FWD>, cudaFuncAttributeMaxDynamicSharedMemorySize, zs);
+    cudaFuncSetAttribute(krec_z<Z_RAND>, cudaFuncAttributeMaxDynamicSharedMemorySize, zs);
+    cudaFuncSetAttribute(krec_z<Z_INV>, cudaFuncAttributeMaxDynamicSharedMemorySize, zs);
+    cudaFuncSetAttribute(krec_y<Y_FWD>, cudaFuncAttributeMaxDynamicSharedMemorySize, ys);
+    cudaFuncSetAttribute(krec_y<Y_RAND>, cudaFuncAttributeMaxDynamicSharedMemorySize, ys);
+    cudaFuncSetAttribute(krec_y<Y_INV>, cudaFuncAttributeMaxDynamicSharedMemorySize, ys);
+    cudaFuncSetAttribute(krec_xrand, cudaFuncAttributeMaxDynamicSharedMemorySize, xs);
+    cudaFuncSetAttribute(krec_xturn, cudaFuncAttributeMaxDynamicSharedMemorySize, xs);
+    if (cudaDeviceSynchronize() != cudaSuccess || cudaGetLastError() != cudaSuccess) {
+        delete h;
+        return failr(M3D_ERR_CUDA, "device set-up failed");
+    }
+    *out = h;
+    return M3D_OK;
+}
+
+int m3drec_destroy(m3d_rec* h) {
+    if (h) {
+        cudaSetDevice(h->device);
+        cudaStreamSynchronize(h->stream);
+        delete h;
+    }
+    return M3D_OK;
+}
+
+int m3drec_seed(m3d_rec* h, unsigned long long seed) {
+    if (!h) return failr(M3D_ERR_ARG, "NULL handle");
+    h->seed = seed;
+    h->call = 0;
+    return M3D_OK;
+}
+
+// runRec(n, beta) :283-400: fresh random field, the loop, the threshold
+int m3drec_run(m3d_rec* h, int n, double beta) {
+    if (!h) return failr(M3D_ERR_ARG, "NULL handle");
+    if (n < 0 || n > 10000000) return failr(M3D_ERR_ARG, "n must be in [0, 1e7]");
+    MR_CUDA(cudaSetDevice(h->device));
+    RecCtl c{};
+    c.seed = h->seed;
+    *h->h_ctl = c;
+    MR_CUDA(cudaMemcpyAsync(h->d_ctl, h->h_ctl, sizeof(RecCtl), cudaMemcpyHostToDevice, h->stream));
+    krec_init<<<h->grid1d(), kThreads, 0, h->stream>>>(h->m, h->d_ctl, h->xyz);
+    h->launches += 1;
+    MR_CUDA(cudaGetLastError());
+    h->i = 0; h->j = 0; h->call = 1; h->n_recorded = 0;
+    h->started = true;
+    if (n > 0) {
+        int rc = h->ensure_err(n);
+        if (rc) return rc;
+        MR_CUDA(cudaMemsetAsync(h->errs, 0, (size_t)n * sizeof(double), h->stream));
+        rc = h->iterate(n, beta);
+        if (rc) return rc;
+    }
+    return h->threshold();
+}
+
+// more passes of the loop from the current state (no threshold): until
+// converged or `iters` further passes
+int m3drec_iterate(m3d_rec* h, int iters, double beta) {
+    if (!h) return failr(M3D_ERR_ARG, "NULL handle");
+    if (!h->started) return failr(M3D_ERR_STATE, "no field yet (run or set_state first)");
+    if (iters < 0 || iters > 10000000) return failr(M3D_ERR_ARG, "iters must be in [0, 1e7]");
+    MR_CUDA(cudaSetDevice(h->device));
+    return h->iterate(h->i + iters, beta);
+}
+
+int m3drec_threshold(m3d_rec* h) {
+    if (!h) return failr(M3D_ERR_ARG, "NULL handle");
+    if (!h->started) return failr(M3D_ERR_STATE, "no field yet (run or set_state first)");
+    MR_CUDA(cudaSetDevice(h->device));
+    return h->threshold();
+}
+
+int m3drec_set_state(m3d_rec* h, const double* field, int i, int j, unsigned long long call) {
+    if (!h || !field) return failr(M3D_ERR_ARG, "NULL argument");
+    if (i < 0 || j < 0 || j > 201) return failr(M3D_ERR_ARG, "need i >= 0 and 0 <= j <= 201");
+    MR_CUDA(cudaSetDevice(h->device));
+    MR_CUDA(cudaMemcpyAsync(h->m, field, (size_t)h->xyz * sizeof(double2), cudaMemcpyHostToDevice, h->stream));
+    const int rc = h->ensure_err(i + 1);
+    if (rc) return rc;
+    MR_CUDA(cudaMemsetAsync(h->errs, 0, (size_t)h->err_cap * sizeof(double), h->stream));
+    MR_CUDA(cudaStreamSynchronize(h->stream));
+    h->i = i; h->j = j; h->call = call;
+    h->n_recorded = i;
+    h->started = true;
+    return M3D_OK;
+}
+
+int m3drec_get_state(m3d_rec* h, double* field, int* i, int* j, unsigned long long* call) {
+    if (!h) return failr(M3D_ERR_ARG, "NULL handle");
+    MR_CUDA(cudaSetDevice(h->device));
+    if (field) {
+        MR_CUDA(cudaMemcpyAsync(field, h->m, (size_t)h->xyz * sizeof(double2), cudaMemcpyDeviceToHost, h->stream));
+        MR_CUDA(cudaStreamSynchronize(h->stream));
+    }
+    if (i) *i = h->i;
+    if (j) *j = h->j;
+    if (call) *call = h->call;
+    return M3D_OK;
+}
+
+// mTilda's real part (after run: the 0/1 phase field), xyz doubles
+int m3drec_get_field(m3d_rec* h, double* out) {
+    if (!h || !out) return failr(M3D_ERR_ARG, "NULL argument");
+    MR_CUDA(cudaSetDevice(h->device));
+    if (!h->real && cudaMalloc(&h->real, (size_t)h->xyz * sizeof(double)) != cudaSuccess) {
+        (void)cudaGetLastError();
+        h->real = nullptr;
+        return failr(M3D_ERR_OOM, "device allocation failed");
+    }
+    krec_real<<<h->grid1d(), kThreads, 0, h->stream>>>(h->m, h->real, h->xyz);
+    h->launches += 1;
+    MR_CUDA(cudaGetLastError());
+    MR_CUDA(cudaMemcpyAsync(out, h->real, (size_t)h->xyz * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    MR_CUDA(cudaStreamSynchronize(h->stream));
+    return M3D_OK;
+}
+
+// trackrealerrorA: the first min(cap, recorded) errors; *count = recorded
+int m3drec_get_error(m3d_rec* h, double* out, int cap, int* count) {
+    if (!h) return failr(M3D_ERR_ARG, "NULL handle");
+    MR_CUDA(cudaSetDevice(h->device));
+    const int k = std::min(std::max(cap, 0), h->n_recorded);
+    if (out && k > 0) {
+        MR_CUDA(cudaMemcpyAsync(out, h->errs, (size_t)k * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+        MR_CUDA(cudaStreamSynchronize(h->stream));
+    }
+    if (count) *count = h->n_recorded;
+    return M3D_OK;
+}
+
+int m3drec_set_profiling(m3d_rec* h, int on) {
+    if (!h) return failr(M3D_ERR_ARG, "NULL handle");
+    h->profiling = on != 0;
+    for (int k = 0; k < 8; ++k) { h->pass_ms[k] = 0; h->pass_count[k] = 0; }
+    return M3D_OK;
+}
+
+// summed event times of the host-driven passes: [restart (3 launches), zfwd, yfwd, xturn, yinv, zinv]
+int m3drec_profile(const m3d_rec* h, double* ms6, long long* passes) {
+    if (!h || !ms6) return failr(M3D_ERR_ARG, "NULL argument");
+    for (int k = 0; k < 6; ++k) ms6[k] = h->pass_ms[k];
+    if (passes) *passes = h->pass_count[1];
+    return M3D_OK;
+}
+
+long long m3drec_kernel_launches(const m3d_rec* h) { return h ? h->launches : 0; }
+void* m3drec_get_stream(const m3d_rec* h) { return h ? (void*)h->stream : nullptr; }
+
+// recon::fftshift / recon::ifftshift (:47-140): per axis, element k moves to
+// (k + s) mod n with s = floor(n / 2) for fftshift and s = floor((n + 1) / 2)
+// for ifftshift (the inverse permutation; the two differ for odd n only)
+static void shift3(const double* in, double* out, int Nx, int Ny, int Nz, bool inverse) {
+    auto sh = [&](int n) { return inverse ? (n + 1) / 2 : n / 2; };
+    const int sx = sh(Nx), sy = sh(Ny), sz = sh(Nz);
+    for (int x = 0; x < Nx; ++x)
+        for (int y = 0; y < Ny; ++y)
+            for (int z = 0; z < Nz; ++z)
+                out[((size_t)((x + sx) % Nx) * Ny + (y + sy) % Ny) * Nz + (z + sz) % Nz] =
+                    in[((size_t)x * Ny + y) * Nz + z];
+}
+
+int m3drec_fftshift(const double* in, double* out, int Nx, int Ny, int Nz) {
+    if (!in || !out || in == out || Nx < 1 || Ny < 1 || Nz < 1) return failr(M3D_ERR_ARG, "bad arguments");
+    shift3(in, out, Nx, Ny, Nz, false);
+    return M3D_OK;
+}
+
+int m3drec_ifftshift(const double* in, double* out, int Nx, int Ny, int Nz) {
+    if (!in || !out || in == out || Nx < 1 || Ny < 1 || Nz < 1) return failr(M3D_ERR_ARG, "bad arguments");
+    shift3(in, out, Nx, Ny, Nz, true);
+    return M3D_OK;
+}
+
+}  // extern "C"

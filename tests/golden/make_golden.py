@@ -1,8 +1,9 @@
 """Generate the golden fixtures in tests/golden/ from the reference's own solver.
 
 Runs oracle/_ref/libmat3d_ref.so -- the reference sources
-src/3d/FFT_analysis3D.cpp and src/3dTherm/FFT_thermal3D.cpp compiled
-unmodified by oracle/Makefile against stand-in FFTW/Eigen/VTK headers -- on
+src/3d/FFT_analysis3D.cpp, src/3dTherm/FFT_thermal3D.cpp, src/2d/FFT_analysis2D.cpp
+and src/rec/reconstruction.cpp compiled unmodified by oracle/Makefile against
+stand-in FFTW/Eigen/VTK headers -- on
 small seeded inputs and stores inputs and outputs as compressed .npz files.
 The reference project ships no tests or expected outputs of its own, so these
 fixtures are the parity pin for the numpy oracle (tests/test_oracle_golden.py)
@@ -93,6 +94,20 @@ def main():
         h = ref.mech2d_homog((N, N), props, rve, E)
         np.savez_compressed(os.path.join(HERE, f"mech2d_{N}.npz"), shape=(N, N), rve=rve, props=props, E=E,
                             eps=r["eps"], sig=r["sig"], C=h["C"], epHomo=h["epHomo"], sigHomo=h["sigHomo"])
+    # microstructure reconstruction (src/rec/reconstruction.cpp): the TPCF of
+    # example/reconst3d/main.cpp (f(r) = exp(-r/A) sin(Qr)/(Qr)), shifted to
+    # index 0 and transformed as the example does; 320 passes cover the
+    # hybrid input-output phase, the box projection (j >= 100), the restarts
+    # at i + 1 = 150 and 300 and the reset of j after 200
+    from oracle.mat3d_oracle import ifftshift3, tpcf_isotropic
+    for shape, seed, (A, Q, phi1) in (((8, 8, 8), 1, (3.0, 0.8, 0.4)), ((6, 8, 10), 2, (4.0, 0.6, 0.5))):
+        Nx, Ny, Nz = shape
+        t = tpcf_isotropic(max(shape), A, Q, phi1).reshape((max(shape),) * 3)[:Nx, :Ny, :Nz].ravel()
+        T = np.real(np.fft.fftn(ifftshift3(t, Nx, Ny, Nz).reshape(shape))).ravel()
+        n, beta = 320, 0.8
+        r = ref.rec_run(shape, T, n, beta, seed)
+        np.savez_compressed(os.path.join(HERE, f"rec_{Nx}x{Ny}x{Nz}.npz"), shape=shape, tpcf=T, seed=seed, n=n,
+                            beta=beta, err=r["err"], rve=r["rve"], iterations=r["iterations"])
     print("fixtures written to", HERE)
 
 

@@ -14,7 +14,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 def declared():
     txt = open(os.path.join(ROOT, "include", "mat3d_b200.h")).read()
     txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
-    return sorted(set(re.findall(r"\b(m3d(?:2d)?_[a-z_0-9]+)\s*\(", txt)))
+    return sorted(set(re.findall(r"\b(m3d(?:2d|rec)?_[a-z_0-9]+)\s*\(", txt)))
 
 
 @pytest.mark.skipif(not os.path.exists(m3d.LIB_PATH), reason="library not built")

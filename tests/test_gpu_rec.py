@@ -1,0 +1,221 @@
+"""Microstructure reconstruction on the GPU (m3drec_*) against the
+restatement of recon::recPlan / runRec (src/rec/reconstruction.cpp) and the
+reference's fixtures.
+
+The random draws and the threshold walk are exact (integer work and exact
+double steps), so the initial field and a thresholded field must be equal bit
+for bit.  The transforms round differently from numpy's, and the iteration
+amplifies a rounding difference about threefold per pass, so the loop is
+checked pass by pass from the same state (every branch: hybrid input-output,
+box projection, the restart at i + 1 = 150, the reset of j after 200,
+convergence) to 1e-9, short runs to 1e-8, and long runs through what they must
+achieve (error track of the reference's size, volume fraction on target)."""
+import numpy as np
+import pytest
+
+import mat3d_b200 as m3d
+from oracle import mat3d_oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def load(name):
+    import os
+    return np.load(os.path.join(os.path.dirname(__file__), "golden", f"{name}.npz"))
+
+
+def example_tpcf(shape, A=3.0, Q=0.8, phi1=0.4):
+    """The example's TPCF (example/reconst3d/main.cpp): centred S2, shifted to
+    index 0, real part of its transform."""
+    m = max(shape)
+    t = O.tpcf_isotropic(m, A, Q, phi1).reshape(m, m, m)[:shape[0], :shape[1], :shape[2]].ravel()
+    return np.real(np.fft.fftn(O.ifftshift3(t, *shape).reshape(shape))).ravel()
+
+
+def state_close(gpu, st, tol=1e-9):
+    f = gpu["field"]
+    assert gpu["i"] == st["i"] and gpu["j"] == st["j"] and gpu["call"] == st["call"]
+    d = np.abs(f - st["mT"]).max()
+    assert d < tol, d
+
+
+@pytest.mark.parametrize("shape", [(8, 8, 8), (6, 8, 10), (16, 12, 9)])
+def test_initial_field_and_threshold_exact(shape):
+    """n = 0: the initial draws (m = (U + 1) / 2) thresholded; both steps exact."""
+    T = example_tpcf(shape)
+    r = m3d.Reconstruction(T, *shape)
+    r.seed(11)
+    r.run(0, 0.8)
+    o = O.RecOracle(T, *shape)
+    st = o.start(11)
+    want = o.threshold(st["mT"].real)
+    assert np.array_equal(r.field(), want)
+    assert r.errors().size == 0
+    r.close()
+
+
+@pytest.mark.parametrize("name", ["rec_8x8x8", "rec_6x8x10"])
+def test_first_passes_vs_reference_fixture(name):
+    """The reference's recorded errors for the first passes (fixture made by
+    the reference itself) agree to 1e-9."""
+    g = load(name)
+    shape = tuple(int(v) for v in g["shape"])
+    r = m3d.Reconstruction(g["tpcf"], *shape)
+    r.seed(int(g["seed"]))
+    r.run(10, float(g["beta"]))
+    e = r.errors()
+    assert e.size == 10
+    assert np.abs(e - g["err"][:10]).max() / g["err"][0] < 1e-9
+    r.close()
+
+
+@pytest.mark.parametrize("shape,k", [((16, 16, 16), 12), ((12, 10, 14), 12), ((27, 20, 25), 8)])
+def test_short_run_state_vs_oracle(shape, k):
+    T = example_tpcf(shape)
+    r = m3d.Reconstruction(T, *shape)
+    r.seed(5)
+    r.run(k, 0.8)  # k passes then the threshold
+    o = O.RecOracle(T, *shape)
+    o.runRec(k, 0.8, 5)
+    assert np.abs(r.errors() - o.err).max() / o.err[0] < 1e-8
+    # the same passes without the threshold: the complex field itself
+    r.seed(5)
+    r.run(0, 0.8)
+    o2 = O.RecOracle(T, *shape)
+    st = o2.start(5)
+    r.set_state(st["mT"], 0, 0, 1)
+    r.iterate(k, 0.8)
+    for _ in range(k):
+        o2.step(st, 0.8)
+    state_close(r.get_state(), st, 1e-8)
+    r.close()
+
+
+@pytest.mark.parametrize("i,j", [(148, 149), (298, 99), (98, 99), (199, 200), (149, 0), (40, 150)])
+def test_branches_step_by_step(i, j):
+    """Two passes from the same state at the loop's branch points: restart
+    (i + 1 = 150, 300), the switch to the box projection (j = 100), the reset
+    of j after 200, and an ordinary box-projection pass."""
+    shape = (12, 12, 12)
+    T = example_tpcf(shape)
+    o = O.RecOracle(T, *shape)
+    st = o.start(3)
+    for _ in range(5):
+        o.step(st, 0.8)
+    st.update(i=i, j=j, call=1 + i // 150)  # draws taken: the initial one and one per earlier restart
+    r = m3d.Reconstruction(T, *shape)
+    r.seed(3)
+    r.set_state(st["mT"], i, j, st["call"])
+    r.iterate(2, 0.8)
+    e = [o.step(st, 0.8) for _ in range(2)]
+    state_close(r.get_state(), st)
+    got = r.errors()
+    assert got.size == i + 2
+    assert np.abs(got[i:] - np.array(e)).max() / e[0] < 1e-9
+    r.close()
+
+
+def test_converged_pass_leaves_field():
+    """A field whose transform already has the target modulus: the first pass
+    records err < 0.1 and stops without touching the field (:310-314)."""
+    shape = (8, 10, 12)
+    rng = np.random.default_rng(2)
+    m = (rng.random(shape) < 0.4).astype(np.float64)
+    M = np.fft.fftn(m)
+    T = (np.abs(M) ** 2 / m.size).ravel()  # normC = |M|
+    r = m3d.Reconstruction(T, *shape)
+    r.seed(1)
+    r.set_state(m.ravel().astype(np.complex128), 0, 0, 1)
+    r.iterate(50, 0.8)
+    s = r.get_state()
+    e = r.errors()
+    assert e.size == 1 and e[0] < 1e-12
+    assert s["i"] == 0 and s["j"] == 1
+    assert np.array_equal(s["field"], m.ravel().astype(np.complex128))
+    r.close()
+
+
+def test_threshold_exact_on_planted_field():
+    shape = (20, 20, 20)
+    T = example_tpcf(shape)
+    rng = np.random.default_rng(4)
+    f = rng.random(int(np.prod(shape))) * 1.2 - 0.1 + 1j * rng.random(int(np.prod(shape)))
+    r = m3d.Reconstruction(T, *shape)
+    r.set_state(f, 0, 0, 1)
+    r.threshold()
+    o = O.RecOracle(T, *shape)
+    got = r.get_state()["field"]
+    assert np.array_equal(got.real, o.threshold(f.real))
+    assert np.array_equal(got.imag, f.imag)  # the walk writes the real part only (:397)
+    r.close()
+
+
+def test_graph_equals_host_loop():
+    """The graph-captured loop and the host-driven loop (per-kernel timing)
+    launch the same kernels: identical errors, fields and counters."""
+    shape = (16, 16, 16)
+    T = example_tpcf(shape)
+    out = []
+    for prof in (False, True):
+        r = m3d.Reconstruction(T, *shape)
+        r.seed(9)
+        r.set_profiling(prof)
+        r.run(160, 0.8)  # crosses the restart at i + 1 = 150
+        out.append((r.errors(), r.field(), r.get_state()))
+        if prof:
+            ms, n = r.profile()
+            assert n == out[0][0].size and ms[3] > 0
+        r.close()
+    assert np.array_equal(out[0][0], out[1][0])
+    assert np.array_equal(out[0][1], out[1][1])
+    assert {k: out[0][2][k] for k in ("i", "j", "call")} == {k: out[1][2][k] for k in ("i", "j", "call")}
+
+
+@pytest.mark.parametrize("name", ["rec_8x8x8", "rec_6x8x10"])
+def test_long_run_properties(name):
+    """320 passes (every branch) on the reference's fixture input: the run
+    completes the same number of passes or converges as the reference did,
+    its error track stays at the reference's level, and the volume fraction
+    of the 0/1 field meets the walk's target like the reference's does."""
+    g = load(name)
+    shape = tuple(int(v) for v in g["shape"])
+    n = int(g["n"])
+    r = m3d.Reconstruction(g["tpcf"], *shape)
+    r.seed(int(g["seed"]))
+    r.run(n, float(g["beta"]))
+    e, f = r.errors(), r.field()
+    ref_e = g["err"][: int(g["iterations"])]
+    assert set(np.unique(f)) <= {0.0, 1.0}
+    assert 0 < e.size <= n
+    assert np.median(e[-50:]) < 2 * np.median(ref_e[-50:]) + 0.1
+    target = np.sqrt(abs(g["tpcf"][0]) * f.size) / f.size
+    assert abs(f.mean() - target) <= max(abs(g["rve"].mean() - target), 1e-4) + 0.01
+    r.close()
+
+
+def test_recplan_mirror():
+    shape = (16, 16, 16)
+    T = example_tpcf(shape, phi1=0.5)
+    a = m3d.recPlan(T, *shape, seed=2)
+    a.runRec(30, 0.8)
+    assert a.trackrealerrorA.shape == (30,)
+    assert a.mTilda.shape == (16 ** 3,)
+    assert set(np.unique(a.mTilda)) <= {0.0, 1.0}
+    o = O.RecOracle(T, *shape)
+    o.runRec(30, 0.8, 2)
+    assert np.abs(a.trackrealerrorA[:8] - o.err[:8]).max() / o.err[0] < 1e-9
+    a.close()
+
+
+def test_errors():
+    T = example_tpcf((8, 8, 8))
+    with pytest.raises(m3d.M3DError):
+        m3d.Reconstruction(np.ones(37 * 4 * 4), 37, 4, 4)  # prime factor 37
+    r = m3d.Reconstruction(T, 8, 8, 8)
+    with pytest.raises(m3d.M3DError):
+        r.iterate(3, 0.8)  # no field yet
+    with pytest.raises(m3d.M3DError):
+        r.run(-1, 0.8)
+    with pytest.raises(m3d.M3DError):
+        r.set_state(np.zeros(512, np.complex128), 0, 300, 0)
+    r.close()
