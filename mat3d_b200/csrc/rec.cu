@@ -475,11 +475,11 @@ struct m3d_rec {
         if (e == cudaSuccess) e = cudaStreamBeginCaptureToGraph(stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed);
         if (e == cudaSuccess) {
             const long long kl = launches;
-            launch_pass(false);
+            const int rc = launch_pass(false);
             krec_cond<<<1, 1, 0, stream>>>(h, d_ctl);
             launches = kl;
             cudaGraph_t got = nullptr;
-            e = cudaGetLastError();
+            e = rc ? cudaErrorLaunchFailure : cudaGetLastError();
             const cudaError_t e2 = cudaStreamEndCapture(stream, &got);
             if (e == cudaSuccess) e = e2;
         }
