@@ -9,7 +9,15 @@ amplifies a rounding difference about threefold per pass, so the loop is
 checked pass by pass from the same state (every branch: hybrid input-output,
 box projection, the restart at i + 1 = 150, the reset of j after 200,
 convergence) to 1e-9, short runs to 1e-8, and long runs through what they must
-achieve (error track of the reference's size, volume fraction on target)."""
+achieve (error track of the reference's size, volume fraction on target).
+
+Grids with an even length are avoided where transforms are compared: the
+transform of a real field (the initial field, the restart draws) has real
+coefficients at the Nyquist frequencies, and where such a coefficient is
+negative its phase is +pi or -pi by the sign of a rounding-level imaginary
+part -- a choice that differs between FFT implementations (numpy's, the GPU's)
+and changes the next field by O(1).  With odd lengths only the zero frequency
+is self-conjugate, and its imaginary part is an exact +0 everywhere."""
 import numpy as np
 import pytest
 
@@ -54,7 +62,7 @@ def test_initial_field_and_threshold_exact(shape):
     r.close()
 
 
-@pytest.mark.parametrize("name", ["rec_8x8x8", "rec_6x8x10"])
+@pytest.mark.parametrize("name", ["rec_9x9x9", "rec_7x9x11"])
 def test_first_passes_vs_reference_fixture(name):
     """The reference's recorded errors for the first passes (fixture made by
     the reference itself) agree to 1e-9."""
@@ -69,7 +77,7 @@ def test_first_passes_vs_reference_fixture(name):
     r.close()
 
 
-@pytest.mark.parametrize("shape,k", [((16, 16, 16), 12), ((12, 10, 14), 12), ((27, 20, 25), 8)])
+@pytest.mark.parametrize("shape,k", [((15, 15, 15), 12), ((11, 13, 9), 12), ((27, 21, 25), 8)])
 def test_short_run_state_vs_oracle(shape, k):
     T = example_tpcf(shape)
     r = m3d.Reconstruction(T, *shape)
@@ -96,7 +104,7 @@ def test_branches_step_by_step(i, j):
     """Two passes from the same state at the loop's branch points: restart
     (i + 1 = 150, 300), the switch to the box projection (j = 100), the reset
     of j after 200, and an ordinary box-projection pass."""
-    shape = (12, 12, 12)
+    shape = (11, 13, 15)
     T = example_tpcf(shape)
     o = O.RecOracle(T, *shape)
     st = o.start(3)
@@ -171,7 +179,7 @@ def test_graph_equals_host_loop():
     assert {k: out[0][2][k] for k in ("i", "j", "call")} == {k: out[1][2][k] for k in ("i", "j", "call")}
 
 
-@pytest.mark.parametrize("name", ["rec_8x8x8", "rec_6x8x10"])
+@pytest.mark.parametrize("name", ["rec_9x9x9", "rec_7x9x11"])
 def test_long_run_properties(name):
     """320 passes (every branch) on the reference's fixture input: the run
     completes the same number of passes or converges as the reference did,
@@ -194,12 +202,12 @@ def test_long_run_properties(name):
 
 
 def test_recplan_mirror():
-    shape = (16, 16, 16)
+    shape = (15, 15, 15)
     T = example_tpcf(shape, phi1=0.5)
     a = m3d.recPlan(T, *shape, seed=2)
     a.runRec(30, 0.8)
     assert a.trackrealerrorA.shape == (30,)
-    assert a.mTilda.shape == (16 ** 3,)
+    assert a.mTilda.shape == (15 ** 3,)
     assert set(np.unique(a.mTilda)) <= {0.0, 1.0}
     o = O.RecOracle(T, *shape)
     o.runRec(30, 0.8, 2)

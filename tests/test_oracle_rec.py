@@ -14,7 +14,7 @@ import pytest
 from oracle import mat3d_oracle as O
 from oracle import ref_lib
 
-GOLDEN = ["rec_8x8x8", "rec_6x8x10"]
+GOLDEN = ["rec_9x9x9", "rec_7x9x11"]
 have_ref = pytest.mark.skipif(not ref_lib.available(), reason="oracle/_ref/libmat3d_ref.so not built")
 
 
