@@ -22,6 +22,9 @@ Workloads (synthetic, seeded; the reference project has no dataset):
               nu .2; matrix 3 GPa, .35); 6 unit load cases each -> full C_eff;
               FP32 sweeps + FP64 refinement to residual 1e-6; one graph launch
               per grid size (a step is the whole batch)
+  rec171      microstructure reconstruction (recPlan + runRec(100, 0.8)) on the
+              example's 171^3 grid and TPCF; a step is one runRec; value =
+              voxels x phase-retrieval passes / device time
   serve       Poisson arrivals of elastic, thermal and J2 solves (1/3 each), N
               log-uniform on [32, 256] rounded to the nearest of {32, 48, 64, 96,
               128, 256} in log scale; elastic as elastic64 (FP32+refine), thermal
@@ -99,6 +102,10 @@ WORKLOADS = {
     "elastic2d": dict(kind="2d", N=1024, iterations=25, props=(68.9e9, 0.35, 400e9, 0.23),
                       desc="2-D plane elastic (FFT_Analysis2D), 1024^2, discs at 20%, E 68.9/400 GPa, "
                            "E12 = 0.005, 25 basic-scheme iterations, complex FP64"),
+    "rec171": dict(kind="rec", N=171, n=100, beta=0.8, A=25.0, Q=0.4, phi1=0.5, seed=1,
+                   desc="microstructure reconstruction (recPlan from a TPCF + runRec(100, 0.8)) on the example's "
+                        "171^3 grid and isotropic TPCF f(r) = exp(-r/25) sin(0.4 r)/(0.4 r), phi1 = 0.5; "
+                        "complex FP64"),
     "serve": dict(kind="serve", per_level=24, levels=(0.25, 0.5, 1.0, 1.5), tol=1e-6, workers=8,
                   desc="Poisson mix of elastic/thermal/J2 solves, N log-uniform 32..256 (rounded), residual 1e-6"),
 }
@@ -364,6 +371,149 @@ def run_2d(args, w, rank, world, local):
         print(json.dumps(line))
 
 
+# algorithmic bytes per voxel of each reconstruction pass kernel (complex FP64
+# field 16 B, normC 8 B): z forward reads m and writes A; the y passes read and
+# write A; the x turnaround reads A and normC and writes A; z inverse reads A and
+# the old m (hybrid input-output) and writes m
+REC_KERNELS = ("krec_z<Z_FWD>", "krec_y<Y_FWD>", "krec_xturn", "krec_y<Y_INV>", "krec_z<Z_INV>")
+REC_BYTES = (32, 32, 40, 32, 48)
+
+
+def cpu_reference_rec(w, budget_s=40.0):
+    """The reference's recPlan / runRec (oracle/_ref) on the host, on the full
+    grid: runRec(1) and runRec(3) give the cost of one pass and the fixed part
+    (plan set-up, initial field, threshold walk); the value is the rate of the
+    full runRec(n) those imply.  The reference transforms with 3 threads
+    (fftw_plan_with_nthreads(3))."""
+    from oracle import ref_lib
+    if not ref_lib.available():
+        return None
+    from mat3d_b200 import rve as R
+    N = w["N"]
+    T = R.reconstruction_input((N, N, N), w["A"], w["Q"], w["phi1"])
+    ref = ref_lib.RefLib()
+    t0 = time.perf_counter()
+    ref.rec_run((N, N, N), T, 1, w["beta"], w["seed"])
+    t1 = time.perf_counter()
+    ref.rec_run((N, N, N), T, 3, w["beta"], w["seed"])
+    t3 = time.perf_counter() - t1
+    t1 = t1 - t0
+    per_pass = max((t3 - t1) / 2, 1e-9)
+    fixed = max(t1 - per_pass, 0.0)
+    total = fixed + w["n"] * per_pass
+    return dict(value=N ** 3 * w["n"] / total, seconds=total, per_pass=per_pass, fixed=fixed,
+                sample=f"reference runRec(1) and runRec(3) on the full {N}^3 grid ({t1 + t3:.1f} s): "
+                       f"{per_pass:.2f} s per pass, {fixed:.2f} s fixed (set-up + threshold walk), "
+                       f"extrapolated to runRec({w['n']})")
+
+
+def run_rec(args, w, rank, world, local):
+    """Reconstruction: a step is one runRec(n, beta) (fresh random field, the
+    loop, the threshold walk) on the resident TPCF."""
+    import torch
+    import torch.distributed as dist
+
+    import mat3d_b200 as m3d
+    from mat3d_b200 import rve as R
+
+    N, n, beta = w["N"], w["n"], w["beta"]
+    shape = (N, N, N)
+    xyz = N ** 3
+    T = R.reconstruction_input(shape, w["A"], w["Q"], w["phi1"])
+    r = m3d.Reconstruction(T, *shape)
+    r.seed(w["seed"] + rank)
+    stream = torch.cuda.ExternalStream(r.stream_ptr())
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def reduce(x, op):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=op)
+        return float(t.item())
+
+    for _ in range(args.warmup):
+        r.run(n, beta)
+    l0 = r.kernel_launches()
+    clk = ClockSampler(local)
+    clk.start()
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    passes = 0
+    e0.record(stream)
+    for _ in range(args.steps):
+        r.run(n, beta)
+        passes += r.errors().size
+    e1.record(stream)
+    barrier()
+    clocks = clk.stop()
+    ms = e0.elapsed_time(e1)
+    launches = r.kernel_launches() - l0
+    ms_max = reduce(ms, dist.ReduceOp.MAX if world > 1 else None)
+    vp = float(xyz) * passes
+    value = reduce(vp, dist.ReduceOp.SUM if world > 1 else None) / (ms_max / 1000.0)
+    # per-kernel event times from one host-driven run (same kernels, no graph)
+    r.set_profiling(True)
+    r.run(n, beta)
+    pms, npass = r.profile()
+    r.set_profiling(False)
+    per_kernel = {REC_KERNELS[k]: 1000.0 * pms[k + 1] / npass for k in range(5)}  # us per launch
+    dom = max(range(5), key=lambda k: pms[k + 1])
+    dom_us = 1000.0 * pms[dom + 1] / npass
+    r.close()
+    # e2e: the TPCF from host memory into a new plan, runRec, the field back
+    barrier()
+    t0 = time.perf_counter()
+    e2e_steps = max(1, args.steps // 2)
+    ep = 0
+    for _ in range(e2e_steps):
+        r2 = m3d.Reconstruction(T, *shape)
+        r2.seed(w["seed"] + rank)
+        r2.run(n, beta)
+        ep += r2.errors().size
+        r2.field()
+        r2.close()
+    barrier()
+    esec = reduce(time.perf_counter() - t0, dist.ReduceOp.MAX if world > 1 else None)
+    e2e = reduce(float(xyz) * ep, dist.ReduceOp.SUM if world > 1 else None) / esec
+    peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    peak, peak_src = (json.load(open(peaks_path))["hbm_gbs"], "measured") if os.path.exists(peaks_path) \
+        else (6650.0, "fallback")
+    achieved = REC_BYTES[dom] * xyz / (dom_us * 1e-6) / 1e9
+    pass_us = sum(per_kernel.values())
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_reference_rec(w)
+    if rank == 0:
+        line = {
+            "metric": "reconstruction voxel-passes/s (runRec: phase-retrieval passes x voxels, FP64 complex)",
+            "value": value, "unit": "voxel-pass/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "c128", "data": "synthetic",
+            "config": {"workload": args.workload, "desc": w["desc"], "grid": list(shape), "n": n, "beta": beta,
+                       "passes_per_step": passes / args.steps,
+                       "l2": "working set m + A (80 MB each) + normC (40 MB) exceeds L2; each pass streams them",
+                       "parallelism": f"replicas x{world}"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "traffic": None, "peak_source": peak_src, "kernel": REC_KERNELS[dom],
+                         "bytes_per_voxel": REC_BYTES[dom], "kernel_us": dom_us, "per_kernel_us": per_kernel,
+                         "pass_us": pass_us,
+                         "pass_frac": sum(REC_BYTES) * xyz / (pass_us * 1e-6) / 1e9 / peak},
+            "e2e": {"value": e2e, "unit": "voxel-pass/s", "h2d_bytes_per_step": 8 * xyz,
+                    "d2h_bytes_per_step": 8 * xyz},
+            "gpu_launches": launches,
+            "clocks": clocks,
+        }
+        if cpu:
+            line["cpu_baseline"] = {"value": cpu["value"], "unit": "voxel-pass/s", "cores": 3, "kind": "reference",
+                                    "sample": cpu["sample"]}
+        print(json.dumps(line))
+
+
 def run_reference_arm(args, w, rank, world):
     if rank != 0:
         return
@@ -372,6 +522,21 @@ def run_reference_arm(args, w, rank, world):
         r = cpu_reference_batch(w, args.steps, args.warmup, threads)
     elif w["kind"] == "2d":
         r = cpu_reference_2d(w, args.steps, args.warmup)
+    elif w["kind"] == "rec":
+        r = cpu_reference_rec(w)
+        if r is not None:
+            line = {
+                "impl": "reference", "metric": "reconstruction voxel-passes/s (runRec: phase-retrieval passes x "
+                "voxels, FP64 complex)", "value": r["value"], "unit": "voxel-pass/s", "n_gpus": args.gpus,
+                "steps": 1, "warmup": 0, "ms_per_step": 1000 * r["seconds"], "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "c128", "data": "synthetic",
+                "config": {"workload": args.workload, "desc": w["desc"]},
+                "cpu_baseline": {"value": r["value"], "unit": "voxel-pass/s", "cores": 3, "kind": "reference",
+                                 "sample": r["sample"]},
+                "e2e": {"value": r["value"], "unit": "voxel-pass/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            }
+            print(json.dumps(line))
+            return
     else:
         r = cpu_reference(w, args.steps, args.warmup, threads)
     if r is None:
@@ -666,8 +831,8 @@ def main():
     if world > 1:
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=120))
-    if w["kind"] in ("batch", "serve", "2d"):
-        {"batch": run_batch, "serve": run_serve, "2d": run_2d}[w["kind"]](args, w, rank, world, local)
+    if w["kind"] in ("batch", "serve", "2d", "rec"):
+        {"batch": run_batch, "serve": run_serve, "2d": run_2d, "rec": run_rec}[w["kind"]](args, w, rank, world, local)
         if world > 1:
             dist.destroy_process_group()
         return

@@ -169,3 +169,25 @@ MAT_ELASTIC_SPHERES = np.array([[70e9, 0.2, 1e30, 0.0, 1.0, 0.0, 1e30],   # incl
                                 [3e9, 0.35, 1e30, 0.0, 1.0, 0.0, 1e30]])  # matrix (phase 1)
 MAT_J2_PARTICLES = np.array([[400e9, 0.2, 1e30, 0.0, 1.0, 0.0, 1e30],      # elastic particles
                              [70e9, 0.33, 100e6, 1e9, 1.0, 0.0, 1e30]])    # J2 matrix, linear hardening
+
+
+def tpcf_isotropic(shape, A=25.0, Q=0.4, phi1=0.5):
+    """Two-point correlation function S2 of a statistically isotropic two-phase
+    medium, centred on (Nx/2, Ny/2, Nz/2), as example/reconst3d/main.cpp
+    builds it: S2 = f(r) phi1 phi2 + phi1^2 with the scaled autocovariance
+    f(r) = exp(-r/A) sin(Q r) / (Q r) (f(0) = 1), r the distance from the centre."""
+    Nx, Ny, Nz = shape
+    X, Y, Z = np.meshgrid(np.arange(Nx) - Nx // 2, np.arange(Ny) - Ny // 2, np.arange(Nz) - Nz // 2, indexing="ij")
+    r = np.sqrt(X * X + Y * Y + Z * Z * 1.0)
+    with np.errstate(invalid="ignore", divide="ignore"):
+        fr = np.exp(-r / A) * np.sin(Q * r) / (Q * r)
+    fr[r == 0] = 1.0
+    return (fr * phi1 * (1 - phi1) + phi1 * phi1).ravel()
+
+
+def reconstruction_input(shape, A=25.0, Q=0.4, phi1=0.5):
+    """What the example hands to recPlan: the centred S2 moved to index 0
+    (recon::ifftshift) and replaced by the real part of its 3-D transform."""
+    import mat3d_b200 as m3d
+    t = m3d.ifftshift(tpcf_isotropic(shape, A, Q, phi1), *shape)
+    return np.ascontiguousarray(np.real(np.fft.fftn(t.reshape(shape))).ravel())
