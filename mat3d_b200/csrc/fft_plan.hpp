@@ -8,15 +8,20 @@
 
 namespace m3d {
 
-// radix schedule 8, 4, 2, then odd primes up to kMaxGenericRadix; false if a factor is larger
+// radix schedule: odd primes up to kMaxGenericRadix, largest first (the
+// first stage needs no twiddle multiplications, so the costliest butterfly
+// goes there), then 8, 4, 2; false if a factor is larger
 inline bool make_plan(int n, LinePlan& p) {
-    std::vector<int> f;
+    std::vector<int> f, odd;
     int m = n;
-    while (m % 8 == 0) { f.push_back(8); m /= 8; }
-    while (m % 4 == 0) { f.push_back(4); m /= 4; }
-    while (m % 2 == 0) { f.push_back(2); m /= 2; }
+    int p2 = 0;
+    while (m % 2 == 0) { ++p2; m /= 2; }
     for (int q = 3; q <= m; q += 2)
-        while (m % q == 0) { f.push_back(q); m /= q; }
+        while (m % q == 0) { odd.push_back(q); m /= q; }
+    for (auto it = odd.rbegin(); it != odd.rend(); ++it) f.push_back(*it);
+    for (; p2 >= 3; p2 -= 3) f.push_back(8);
+    if (p2 == 2) f.push_back(4);
+    if (p2 == 1) f.push_back(2);
     if (f.empty()) f.push_back(1);
     if ((int)f.size() > kMaxStages) return false;
     for (int r : f)

@@ -56,6 +56,27 @@ template <typename C2> __device__ __forceinline__ C2 twid(const C2* tw, int m, i
     return w;
 }
 
+// x / d for 0 <= x, 1 <= d with x * d < 2^32 (always true for indices of a
+// shared-memory tile): round-up reciprocal m = ceil(2^32 / d), q = hi32(x m).
+// The error of x m / 2^32 against x / d is below x / 2^32 < 1 / d, too small
+// to carry the quotient past the next integer.
+struct FastDiv {
+    unsigned m;
+    int d;
+    __device__ __forceinline__ void init(int dd) {
+        d = dd;
+        m = dd > 1 ? 0xFFFFFFFFu / (unsigned)dd + 1u : 0u;
+    }
+    __device__ __forceinline__ int div(int x) const { return d == 1 ? x : (int)__umulhi((unsigned)x, m); }
+};
+
+// per-stage constants shared by every butterfly of a Stockham stage
+struct StageIdx {
+    int nb;    // n / R: butterflies per line, and the input stride
+    int Ns;    // product of the earlier radices
+    int step;  // n / (Ns R): twiddle index step
+};
+
 template <typename C2, int R>
 __device__ __forceinline__ void dft_small(C2 (&v)[R], const C2* tw, int n, int sign) {
     typedef decltype(C2().x) T;
@@ -131,39 +152,92 @@ __device__ __forceinline__ void dft_small(C2 (&v)[R], const C2* tw, int n, int s
     }
 }
 
+// butterfly j of a stage: inputs j + r nb, twiddles w^(k r step) with
+// j = g Ns + k, outputs g Ns R + k + r Ns
 template <typename C2, int R>
-__device__ __forceinline__ void butterfly(const C2* __restrict__ src, C2* __restrict__ dst, int j, int n, int Ns,
-                                          int es, const C2* tw, int sign) {
-    const int nb = n / R;
+__device__ __forceinline__ void butterfly(const C2* __restrict__ src, C2* __restrict__ dst, int j, int g, int k,
+                                          const StageIdx& S, int es, const C2* tw, int sign) {
     C2 v[R];
 #pragma unroll
-    for (int r = 0; r < R; ++r) v[r] = src[(j + r * nb) * es];
-    const int k = j % Ns;
-    if (Ns > 1) {
-        const int step = n / (Ns * R);
+    for (int r = 0; r < R; ++r) v[r] = src[(j + r * S.nb) * es];
+    if (S.Ns > 1) {
 #pragma unroll
-        for (int r = 1; r < R; ++r) v[r] = cmul(v[r], twid(tw, k * r * step, sign));
+        for (int r = 1; r < R; ++r) v[r] = cmul(v[r], twid(tw, k * r * S.step, sign));
     }
-    dft_small<C2, R>(v, tw, n, sign);
-    const int idx = (j / Ns) * Ns * R + k;
+    dft_small<C2, R>(v, tw, S.nb * R, sign);
+    const int idx = g * S.Ns * R + k;
 #pragma unroll
-    for (int r = 0; r < R; ++r) dst[(idx + r * Ns) * es] = v[r];
+    for (int r = 0; r < R; ++r) dst[(idx + r * S.Ns) * es] = v[r];
+}
+
+// Odd radix R >= 5, compile time: inputs j and R-j are paired
+// (a_j = x_j + x_{R-j}, b_j = x_j - x_{R-j}) so outputs k and R-k share one set
+// of products:
+//   y_k, y_{R-k} = x_0 + sum_j a_j cos(2 pi jk/R) +- i sign sum_j b_j sin(2 pi jk/R)
+// -- (R-1)^2 real multiply-adds per butterfly instead of the 4 R^2 of a direct
+// DFT.  Outputs go straight to `dst`, so only a, b and the h = (R-1)/2 cosines
+// and sines (from the table: tw[m n/R] = (cos, -sin) of 2 pi m/R) live in
+// registers.
+template <typename C2, int R>
+__device__ __forceinline__ void butterfly_odd(const C2* __restrict__ src, C2* __restrict__ dst, int j, int g, int k0,
+                                              const StageIdx& S, int es, const C2* tw, int sign) {
+    typedef decltype(C2().x) T;
+    constexpr int h = (R - 1) / 2;
+    const int nb = S.nb, Ns = S.Ns, step = S.step;
+    const C2 x0 = src[j * es];
+    C2 a[h], b[h];
+#pragma unroll
+    for (int q = 1; q <= h; ++q) {
+        C2 u = src[(j + q * nb) * es], w = src[(j + (R - q) * nb) * es];
+        if (Ns > 1) {
+            u = cmul(u, twid(tw, k0 * q * step, sign));
+            w = cmul(w, twid(tw, k0 * (R - q) * step, sign));
+        }
+        a[q - 1] = cadd(u, w);
+        b[q - 1] = csub(u, w);
+    }
+    T c[h], sn[h];
+#pragma unroll
+    for (int m = 1; m <= h; ++m) {
+        const C2 w = tw[m * nb];
+        c[m - 1] = w.x;
+        sn[m - 1] = sign < 0 ? w.y : -w.y;  // sign * sin(2 pi m / R)
+    }
+    const int idx = g * Ns * R + k0;
+    C2 y0 = x0;
+#pragma unroll
+    for (int q = 0; q < h; ++q) y0 = cadd(y0, a[q]);
+    dst[idx * es] = y0;
+#pragma unroll
+    for (int k = 1; k <= h; ++k) {
+        T px = x0.x, py = x0.y, qx = 0, qy = 0;
+#pragma unroll
+        for (int q = 1; q <= h; ++q) {
+            const int m = (q * k) % R;
+            const T cc = m <= h ? c[m - 1] : c[R - m - 1];
+            const T ss = m <= h ? sn[m - 1] : -sn[R - m - 1];
+            px += a[q - 1].x * cc;
+            py += a[q - 1].y * cc;
+            qx += b[q - 1].x * ss;
+            qy += b[q - 1].y * ss;
+        }
+        dst[(idx + k * Ns) * es] = mk<C2>(px - qy, py + qx);
+        dst[(idx + (R - k) * Ns) * es] = mk<C2>(px + qy, py - qx);
+    }
 }
 
 // generic-radix butterfly (any R up to kMaxGenericRadix), run-time R
 constexpr int kMaxGenericRadix = 32;
 template <typename C2>
-__device__ __noinline__ void butterfly_generic(const C2* __restrict__ src, C2* __restrict__ dst, int R, int j, int n,
-                                               int Ns, int es, const C2* tw, int sign) {
+__device__ __noinline__ void butterfly_generic(const C2* __restrict__ src, C2* __restrict__ dst, int R, int j, int g,
+                                               int k, StageIdx S, int es, const C2* tw, int sign) {
     typedef decltype(C2().x) T;
-    const int nb = n / R;
+    const int nb = S.nb, Ns = S.Ns, step = S.step;
     C2 v[kMaxGenericRadix];
     for (int r = 0; r < R; ++r) v[r] = src[(j + r * nb) * es];
-    const int k = j % Ns;
-    const int step = n / (Ns * R);
     for (int r = 1; r < R; ++r) v[r] = cmul(v[r], twid(tw, k * r * step, sign));
-    const int st = n / R;
-    const int idx = (j / Ns) * Ns * R + k;
+    const int st = nb;
+    const int idx = g * Ns * R + k;
     for (int s = 0; s < R; ++s) {
         C2 acc = v[0];
         for (int q = 1; q < R; ++q) acc = cadd(acc, cmul(v[q], twid(tw, ((q * s) % R) * st, sign)));
@@ -183,29 +257,64 @@ struct LineLayout {
 
 // Transforms every line; returns the buffer (a or b) that holds the result.
 // Must be called by all threads of the CTA; ends with __syncthreads().
-template <typename C2>
+// Radices 2, 3, 4, 5, 8 are compile-time butterflies; odd primes 7..MaxR are
+// compile-time too when MaxR reaches them (each adds registers to the
+// kernel, so callers pick the smallest MaxR their lengths need); any other
+// radix runs the run-time generic butterfly.
+// one Stockham stage of radix R over every line of the tile (R fixed at
+// compile time, so the loop body is one straight-line butterfly); KIND 0 =
+// butterfly (2, 3, 4, 8), 1 = butterfly_odd, 2 = run-time generic
+template <typename C2, int R, int KIND>
+__device__ __forceinline__ void run_stage(const C2* a, C2* b, const C2* tw, const StageIdx& S, int Rrt,
+                                          const LineLayout& L, const FastDiv& dl, const FastDiv& dg, int sign) {
+    FastDiv dnb, dns;
+    dnb.init(S.nb);
+    dns.init(S.Ns);
+    const int total = S.nb * L.nlines;
+    const int es = L.estride;
+    for (int w = threadIdx.x; w < total; w += blockDim.x) {
+        int line, j;
+        if (L.lines_fast) { j = dl.div(w); line = w - j * L.nlines; }
+        else { line = dnb.div(w); j = w - line * S.nb; }
+        const int grp = dg.div(line);
+        const int base = grp * L.gstride + (line - grp * L.lpg) * L.lstride;
+        const int g = dns.div(j), k = j - g * S.Ns;
+        if constexpr (KIND == 0) butterfly<C2, R>(a + base, b + base, j, g, k, S, es, tw, sign);
+        else if constexpr (KIND == 1) butterfly_odd<C2, R>(a + base, b + base, j, g, k, S, es, tw, sign);
+        else butterfly_generic<C2>(a + base, b + base, Rrt, j, g, k, S, es, tw, sign);
+    }
+}
+
+template <typename C2, int MaxR = 5>
 __device__ C2* fft_lines(C2* a, C2* b, const C2* tw, const LinePlan& p, const LineLayout& L, int sign) {
     const int n = p.n;
+    FastDiv dl, dg;  // by the lines of the tile, by the lines of a group
+    dl.init(L.nlines);
+    dg.init(L.lpg);
     int Ns = 1;
     for (int s = 0; s < p.nstages; ++s) {
         const int R = p.radix[s];
-        const int nb = n / R;
-        const int total = nb * L.nlines;
-        for (int w = threadIdx.x; w < total; w += blockDim.x) {
-            int line, j;
-            if (L.lines_fast) { line = w % L.nlines; j = w / L.nlines; }
-            else { j = w % nb; line = w / nb; }
-            const int base = (line / L.lpg) * L.gstride + (line % L.lpg) * L.lstride;
-            const C2* src = a + base;
-            C2* dst = b + base;
-            switch (R) {
-                case 2: butterfly<C2, 2>(src, dst, j, n, Ns, L.estride, tw, sign); break;
-                case 3: butterfly<C2, 3>(src, dst, j, n, Ns, L.estride, tw, sign); break;
-                case 4: butterfly<C2, 4>(src, dst, j, n, Ns, L.estride, tw, sign); break;
-                case 5: butterfly<C2, 5>(src, dst, j, n, Ns, L.estride, tw, sign); break;
-                case 8: butterfly<C2, 8>(src, dst, j, n, Ns, L.estride, tw, sign); break;
-                default: butterfly_generic<C2>(src, dst, R, j, n, Ns, L.estride, tw, sign); break;
-            }
+        StageIdx S;
+        S.nb = n / R;
+        S.Ns = Ns;
+        S.step = S.nb / Ns;
+        switch (R) {
+            case 2: run_stage<C2, 2, 0>(a, b, tw, S, R, L, dl, dg, sign); break;
+            case 3: run_stage<C2, 3, 0>(a, b, tw, S, R, L, dl, dg, sign); break;
+            case 4: run_stage<C2, 4, 0>(a, b, tw, S, R, L, dl, dg, sign); break;
+            case 5: run_stage<C2, 5, 1>(a, b, tw, S, R, L, dl, dg, sign); break;
+            case 8: run_stage<C2, 8, 0>(a, b, tw, S, R, L, dl, dg, sign); break;
+            default:
+                if constexpr (MaxR >= 7) if (R == 7) { run_stage<C2, 7, 1>(a, b, tw, S, R, L, dl, dg, sign); break; }
+                if constexpr (MaxR >= 11) if (R == 11) { run_stage<C2, 11, 1>(a, b, tw, S, R, L, dl, dg, sign); break; }
+                if constexpr (MaxR >= 13) if (R == 13) { run_stage<C2, 13, 1>(a, b, tw, S, R, L, dl, dg, sign); break; }
+                if constexpr (MaxR >= 17) if (R == 17) { run_stage<C2, 17, 1>(a, b, tw, S, R, L, dl, dg, sign); break; }
+                if constexpr (MaxR >= 19) if (R == 19) { run_stage<C2, 19, 1>(a, b, tw, S, R, L, dl, dg, sign); break; }
+                if constexpr (MaxR >= 23) if (R == 23) { run_stage<C2, 23, 1>(a, b, tw, S, R, L, dl, dg, sign); break; }
+                if constexpr (MaxR >= 29) if (R == 29) { run_stage<C2, 29, 1>(a, b, tw, S, R, L, dl, dg, sign); break; }
+                if constexpr (MaxR >= 31) if (R == 31) { run_stage<C2, 31, 1>(a, b, tw, S, R, L, dl, dg, sign); break; }
+                run_stage<C2, 1, 2>(a, b, tw, S, R, L, dl, dg, sign);
+                break;
         }
         __syncthreads();
         C2* t = a; a = b; b = t;

@@ -7,6 +7,7 @@
 //     m = (U + 1) / 2                                   (U uniform in [-1, 1))
 //     loop: M = FFT(m); err = mean | |M| - normC |; stop if err < 0.1 or i >= n
 //           ang = arg M   (every 150th pass: 0.3 arg FFT(U') + 0.7 arg M)
+//           (on other passes normC e^{i ang} is formed as M normC / |M|)
 //           m' = IFFT(normC e^{i ang}) / xyz
 //           j < 100:  hybrid input-output  m' < 0 -> m - beta m' ; m' > 1 -> m - beta (m' - 1) ; m' > 1 -> 1
 //           j >= 100: box projection       m' < 0 -> 0 ; m' > 1 -> 1 ; j > 200 -> j = 0
@@ -68,7 +69,7 @@ int failr(int code, const std::string& msg) {
         if (e_ != cudaSuccess) return failr(M3D_ERR_CUDA, cudaGetErrorString(e_)); \
     } while (0)
 
-constexpr int kThreads = 256;
+constexpr int kThreads = 128;
 constexpr int kRestartPeriod = 150;  // remainder(i + 1, 150) == 0 (:320)
 
 struct RecCtl {
@@ -106,70 +107,107 @@ __global__ void krec_init(double2* __restrict__ m, RecCtl* ctl, long long xyz) {
         m[v] = make_double2(__dmul_rn(__dadd_rn(draw_pm1(base, (unsigned long long)v), 1.0), 0.5), 0.0);
 }
 
+// 16-byte global -> shared copies that complete asynchronously (zero-filled
+// when !valid; the source is then not read)
+__device__ __forceinline__ void cp_async16(void* sdst, const void* gsrc, bool valid) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(sdst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(sa), "l"(gsrc), "r"(valid ? 16 : 0) : "memory");
+}
+__device__ __forceinline__ void cp_async8(void* sdst, const void* gsrc, bool valid) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(sdst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(sa), "l"(gsrc), "r"(valid ? 8 : 0) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
 enum ZMode { Z_FWD = 0, Z_RAND = 1, Z_INV = 2 };
 
-// z lines (contiguous): G lines of length Nz per CTA.
+// z lines (contiguous): tiles of G lines of length Nz, walked by persistent
+// CTAs with three shared buffers (the next tile streams in by cp.async while
+// the current one is transformed).
 //   Z_FWD : A = FFT_z(m)
 //   Z_RAND: A = FFT_z(U') on restart passes (U' = draw `call`, real)
 //   Z_INV : m = projection(IFFT_z(A) / xyz, m) unless the pass converged
-template <int MODE>
+template <int MODE, int MaxR>
 __global__ void __launch_bounds__(kThreads) krec_z(double2* __restrict__ A, double2* __restrict__ m,
                                                     const double2* __restrict__ twz, LinePlan pz, int G,
-                                                    long long nlines, const RecCtl* __restrict__ ctl) {
+                                                    long long nlines, int ntiles, const RecCtl* __restrict__ ctl) {
     if (MODE == Z_RAND && !restart_pass(ctl)) return;
     if (MODE == Z_INV && ctl->done) return;
     extern __shared__ __align__(16) char smem_raw[];
     const int Nz = pz.n;
+    const int tsz = G * Nz;
     double2* tw = (double2*)smem_raw;
-    double2* S0 = tw + Nz;
-    double2* S1 = S0 + (size_t)G * Nz;
-    const long long l0 = (long long)blockIdx.x * G;
+    double2* B[3];
+    B[0] = tw + Nz;
+    B[1] = B[0] + tsz;
+    B[2] = B[1] + tsz;
+    double* MB[2];  // Z_INV: the old field's real part of the tile, double-buffered
+    MB[0] = (double*)(B[2] + tsz);
+    MB[1] = MB[0] + tsz;
     const long long xyz = ctl->xyz;
-    for (int t = threadIdx.x; t < Nz; t += blockDim.x) tw[t] = twz[t];
     unsigned long long base = 0;
     if (MODE == Z_RAND) base = draw_base(ctl->seed, ctl->call);
-    for (int t = threadIdx.x; t < G * Nz; t += blockDim.x) {
-        const long long l = l0 + t / Nz;
-        const long long v = l * Nz + t % Nz;
-        double2 w = make_double2(0, 0);
-        if (l < nlines) {
-            if (MODE == Z_FWD) w = m[v];
-            else if (MODE == Z_RAND) w = make_double2(draw_pm1(base, (unsigned long long)v), 0.0);
-            else w = A[v];
+    const double2* src = MODE == Z_FWD ? m : A;
+    // a tile's G lines are one contiguous run of voxels: v0 = tile G Nz ..
+    auto valid_of = [&](int tile) { return (int)(min((long long)G, nlines - (long long)tile * G) * Nz); };
+    auto fetch = [&](double2* S, double* MS, int tile) {
+        const long long v0 = (long long)tile * tsz;
+        const int valid = valid_of(tile);
+#pragma unroll 4
+        for (int t = threadIdx.x; t < tsz; t += blockDim.x) {
+            if (MODE == Z_RAND) S[t] = t < valid ? make_double2(draw_pm1(base, (unsigned long long)(v0 + t)), 0.0)
+                                                 : make_double2(0, 0);
+            else cp_async16(S + t, t < valid ? src + v0 + t : src, t < valid);
+            if (MODE == Z_INV) cp_async8(MS + t, t < valid ? &m[v0 + t].x : &m[0].x, t < valid);
         }
-        S0[t] = w;
-    }
-    __syncthreads();
-    LineLayout L{G, G, Nz, 0, 1, false};
-    double2* r = fft_lines(S0, S1, tw, pz, L, MODE == Z_INV ? +1 : -1);
-    if (MODE != Z_INV) {
-        for (int t = threadIdx.x; t < G * Nz; t += blockDim.x) {
-            const long long l = l0 + t / Nz;
-            if (l < nlines) A[l * Nz + t % Nz] = r[t];
-        }
-        return;
-    }
-    // temp = temp / xyz, then the projections (:345-364)
+    };
+    int tile = blockIdx.x;
+    if (tile < ntiles) fetch(B[0], MB[0], tile);
+    cp_async_commit();
+    for (int t = threadIdx.x; t < Nz; t += blockDim.x) tw[t] = twz[t];
+    const LineLayout L{G, G, Nz, 0, 1, false};
     const double dxyz = (double)xyz;
-    const double beta = ctl->beta;
-    const bool hio = ctl->hio != 0;
-    for (int t = threadIdx.x; t < G * Nz; t += blockDim.x) {
-        const long long l = l0 + t / Nz;
-        if (l >= nlines) continue;
-        const long long v = l * Nz + t % Nz;
-        const double2 w = r[t];
-        double re = w.x / dxyz, im = w.y / dxyz;
-        if (hio) {
-            const double old = m[v].x;
-            if (re < 0) { re = __dsub_rn(old, __dmul_rn(beta, re)); im = 0; }
-            if (re > 1) { re = __dsub_rn(old, __dmul_rn(beta, __dsub_rn(re, 1.0))); im = 0; }
-            if (re > 1) { re = 1; im = 0; }
+    const double beta = MODE == Z_INV ? ctl->beta : 0.0;
+    const bool hio = MODE == Z_INV && ctl->hio != 0;
+    int d = 0, mbi = 0;
+    for (; tile < ntiles; tile += gridDim.x) {
+        cp_async_wait_all();
+        __syncthreads();
+        const int f = d == 0 ? 2 : d - 1;
+        const int nxt = tile + gridDim.x;
+        if (nxt < ntiles) fetch(B[f], MB[mbi ^ 1], nxt);
+        cp_async_commit();
+        double2* r = fft_lines<double2, MaxR>(B[d], B[d == 2 ? 0 : d + 1], tw, pz, L, MODE == Z_INV ? +1 : -1);
+        const double* old = MB[mbi];
+        const long long v0 = (long long)tile * tsz;
+        const int valid = valid_of(tile);
+        if (MODE != Z_INV) {
+#pragma unroll 4
+            for (int t = threadIdx.x; t < valid; t += blockDim.x) A[v0 + t] = r[t];
         } else {
-            if (re < 0) { re = 0; im = 0; }
-            if (re > 1) { re = 1; im = 0; }
+            // temp = temp / xyz, then the projections (:345-364) against the
+            // old field (prefetched with the tile)
+#pragma unroll 2
+            for (int t = threadIdx.x; t < valid; t += blockDim.x) {
+                const long long v = v0 + t;
+                const double2 w = r[t];
+                double re = w.x / dxyz, im = w.y / dxyz;
+                if (hio) {
+                    if (re < 0) { re = __dsub_rn(old[t], __dmul_rn(beta, re)); im = 0; }
+                    if (re > 1) { re = __dsub_rn(old[t], __dmul_rn(beta, __dsub_rn(re, 1.0))); im = 0; }
+                    if (re > 1) { re = 1; im = 0; }
+                } else {
+                    if (re < 0) { re = 0; im = 0; }
+                    if (re > 1) { re = 1; im = 0; }
+                }
+                m[v] = make_double2(re, im);
+            }
         }
-        m[v] = make_double2(re, im);
+        d = f;
+        mbi ^= 1;
     }
+    cp_async_wait_all();
 }
 
 // column passes (y or x lines): TZ consecutive z columns of one plane, N
@@ -180,111 +218,212 @@ struct ColTile {
     int nz;          // columns present in this tile
 };
 
-__device__ __forceinline__ void col_load(double2* S, const double2* __restrict__ A, const ColTile& c, int N, int TZ) {
+__device__ __forceinline__ void col_store(double2* __restrict__ A, const double2* S, const ColTile& c, int N, int TZ,
+                                          const FastDiv& dz) {
+#pragma unroll 4
     for (int t = threadIdx.x; t < N * TZ; t += blockDim.x) {
-        const int tz = t % TZ, e = t / TZ;
-        S[t] = tz < c.nz ? A[c.base + e * c.stride + tz] : make_double2(0, 0);
+        const int e = dz.div(t), tz = t - e * TZ;
+        if (tz < c.nz) A[c.base + e * c.stride + tz] = S[t];
     }
 }
-__device__ __forceinline__ void col_store(double2* __restrict__ A, const double2* S, const ColTile& c, int N, int TZ) {
+
+__device__ __forceinline__ void col_fetch(double2* S, const double2* __restrict__ A, const ColTile& c, int N, int TZ,
+                                          const FastDiv& dz) {
+#pragma unroll 4
     for (int t = threadIdx.x; t < N * TZ; t += blockDim.x) {
-        const int tz = t % TZ, e = t / TZ;
-        if (tz < c.nz) A[c.base + e * c.stride + tz] = S[t];
+        const int e = dz.div(t), tz = t - e * TZ;
+        const bool ok = tz < c.nz;
+        cp_async16(S + t, ok ? A + c.base + e * c.stride + tz : A, ok);
     }
 }
 
 enum YMode { Y_FWD = 0, Y_RAND = 1, Y_INV = 2 };
 
-// y lines: CTA (x, z tile); in place on A
-template <int MODE>
+// y lines, in place on A: tiles (x, z range of TZ columns).  Persistent CTAs
+// walk the tiles with three shared buffers: while one tile is transformed in
+// two of them, the next tile streams into the third (cp.async), so the load
+// of a tile overlaps the arithmetic of the one before.
+template <int MODE, int MaxR>
 __global__ void __launch_bounds__(kThreads) krec_y(double2* __restrict__ A, const double2* __restrict__ twy,
-                                                    LinePlan py, int Nz, int TZ, int ntz, const RecCtl* __restrict__ ctl) {
+                                                    LinePlan py, int Nz, int TZ, int ntz, int ntiles,
+                                                    const RecCtl* __restrict__ ctl) {
     if (MODE == Y_RAND && !restart_pass(ctl)) return;
     if (MODE == Y_INV && ctl->done) return;
     extern __shared__ __align__(16) char smem_raw[];
     const int Ny = py.n;
     double2* tw = (double2*)smem_raw;
-    double2* S0 = tw + Ny;
-    double2* S1 = S0 + (size_t)Ny * TZ;
-    const int x = blockIdx.x / ntz, z0 = (blockIdx.x % ntz) * TZ;
-    const ColTile c{(long long)x * Ny * Nz + z0, Nz, min(TZ, Nz - z0)};
+    double2* B[3];
+    B[0] = tw + Ny;
+    B[1] = B[0] + (size_t)Ny * TZ;
+    B[2] = B[1] + (size_t)Ny * TZ;
+    FastDiv dz, dt;
+    dz.init(TZ);
+    dt.init(ntz);
+    auto tile_of = [&](int tile) {
+        const int x = dt.div(tile), z0 = (tile - x * ntz) * TZ;
+        return ColTile{(long long)x * Ny * Nz + z0, Nz, min(TZ, Nz - z0)};
+    };
+    int tile = blockIdx.x;
+    if (tile < ntiles) col_fetch(B[0], A, tile_of(tile), Ny, TZ, dz);
+    cp_async_commit();
     for (int t = threadIdx.x; t < Ny; t += blockDim.x) tw[t] = twy[t];
-    col_load(S0, A, c, Ny, TZ);
-    __syncthreads();
-    LineLayout L{TZ, TZ, 1, 0, TZ, true};
-    const double2* r = fft_lines(S0, S1, tw, py, L, MODE == Y_INV ? +1 : -1);
-    col_store(A, r, c, Ny, TZ);
+    const LineLayout L{TZ, TZ, 1, 0, TZ, true};
+    int d = 0;
+    for (; tile < ntiles; tile += gridDim.x) {
+        cp_async_wait_all();
+        __syncthreads();  // tile data landed; the previous tile's stores are done with its buffers
+        const int f = d == 0 ? 2 : d - 1;  // the buffer this tile does not use
+        const int nxt = tile + gridDim.x;
+        if (nxt < ntiles) col_fetch(B[f], A, tile_of(nxt), Ny, TZ, dz);
+        cp_async_commit();
+        const double2* r = fft_lines<double2, MaxR>(B[d], B[d == 2 ? 0 : d + 1], tw, py, L, MODE == Y_INV ? +1 : -1);
+        col_store(A, r, tile_of(tile), Ny, TZ, dz);
+        d = f;
+    }
+    cp_async_wait_all();
 }
 
-// x lines of a restart pass: R = 0.3 arg FFT(U') (:326-327)
+// x lines of a restart pass: R = 0.3 arg FFT(U') (:326-327); persistent CTAs
+// as the y passes
+template <int MaxR>
 __global__ void __launch_bounds__(kThreads) krec_xrand(const double2* __restrict__ A, double* __restrict__ R,
                                                         const double2* __restrict__ twx, LinePlan px, int Ny, int Nz,
-                                                        int TZ, int ntz, const RecCtl* __restrict__ ctl) {
+                                                        int TZ, int ntz, int ntiles, const RecCtl* __restrict__ ctl) {
     if (!restart_pass(ctl)) return;
     extern __shared__ __align__(16) char smem_raw[];
     const int Nx = px.n;
     double2* tw = (double2*)smem_raw;
-    double2* S0 = tw + Nx;
-    double2* S1 = S0 + (size_t)Nx * TZ;
-    const int y = blockIdx.x / ntz, z0 = (blockIdx.x % ntz) * TZ;
-    const ColTile c{(long long)y * Nz + z0, (long long)Ny * Nz, min(TZ, Nz - z0)};
+    double2* B[3];
+    B[0] = tw + Nx;
+    B[1] = B[0] + (size_t)Nx * TZ;
+    B[2] = B[1] + (size_t)Nx * TZ;
+    FastDiv dz, dt;
+    dz.init(TZ);
+    dt.init(ntz);
+    auto tile_of = [&](int tile) {
+        const int y = dt.div(tile), z0 = (tile - y * ntz) * TZ;
+        return ColTile{(long long)y * Nz + z0, (long long)Ny * Nz, min(TZ, Nz - z0)};
+    };
+    int tile = blockIdx.x;
+    if (tile < ntiles) col_fetch(B[0], A, tile_of(tile), Nx, TZ, dz);
+    cp_async_commit();
     for (int t = threadIdx.x; t < Nx; t += blockDim.x) tw[t] = twx[t];
-    col_load(S0, A, c, Nx, TZ);
-    __syncthreads();
-    LineLayout L{TZ, TZ, 1, 0, TZ, true};
-    const double2* r = fft_lines(S0, S1, tw, px, L, -1);
-    for (int t = threadIdx.x; t < Nx * TZ; t += blockDim.x) {
-        const int tz = t % TZ, e = t / TZ;
-        if (tz < c.nz) R[c.base + e * c.stride + tz] = __dmul_rn(atan2(r[t].y, r[t].x), 0.3);
+    const LineLayout L{TZ, TZ, 1, 0, TZ, true};
+    int d = 0;
+    for (; tile < ntiles; tile += gridDim.x) {
+        cp_async_wait_all();
+        __syncthreads();
+        const int f = d == 0 ? 2 : d - 1;
+        const int nxt = tile + gridDim.x;
+        if (nxt < ntiles) col_fetch(B[f], A, tile_of(nxt), Nx, TZ, dz);
+        cp_async_commit();
+        const double2* r = fft_lines<double2, MaxR>(B[d], B[d == 2 ? 0 : d + 1], tw, px, L, -1);
+        const ColTile c = tile_of(tile);
+        for (int t = threadIdx.x; t < Nx * TZ; t += blockDim.x) {
+            const int e = dz.div(t), tz = t - e * TZ;
+            if (tz < c.nz) R[c.base + e * c.stride + tz] = __dmul_rn(atan2(r[t].y, r[t].x), 0.3);
+        }
+        d = f;
     }
+    cp_async_wait_all();
 }
 
 // x turnaround: forward x FFT (M = FFT(m) complete), error partials
 // (funcNormC, include/reconstruction.hpp:37-44), modulus replacement
-// (:317-336), inverse x FFT.  The last CTA to finish reduces the partials in
-// a fixed order, records err[i] and advances the loop state (:300-314, :360-365).
+// (:317-336), inverse x FFT.  Persistent CTAs with three field buffers and
+// two normC buffers (the next tile's field and modulus stream in while the
+// current tile is worked on).  Each CTA sums its error terms in a fixed
+// order; the last CTA to finish reduces the partials in a fixed order,
+// records err[i] and advances the loop state (:300-314, :360-365).
+template <int MaxR>
 __global__ void __launch_bounds__(kThreads) krec_xturn(double2* __restrict__ A, const double* __restrict__ normC,
                                                         const double* __restrict__ R, const double2* __restrict__ twx,
-                                                        LinePlan px, int Ny, int Nz, int TZ, int ntz,
+                                                        LinePlan px, int Ny, int Nz, int TZ, int ntz, int ntiles,
                                                         double* __restrict__ part, double* __restrict__ errs,
                                                         RecCtl* ctl) {
     extern __shared__ __align__(16) char smem_raw[];
     __shared__ double red[kThreads / 32];
     __shared__ bool last;
     const int Nx = px.n;
+    const int tsz = Nx * TZ;
     double2* tw = (double2*)smem_raw;
-    double2* S0 = tw + Nx;
-    double2* S1 = S0 + (size_t)Nx * TZ;
-    const int y = blockIdx.x / ntz, z0 = (blockIdx.x % ntz) * TZ;
-    const ColTile c{(long long)y * Nz + z0, (long long)Ny * Nz, min(TZ, Nz - z0)};
+    double2* B[3];
+    B[0] = tw + Nx;
+    B[1] = B[0] + tsz;
+    B[2] = B[1] + tsz;
+    double* NB[2];
+    NB[0] = (double*)(B[2] + tsz);
+    NB[1] = NB[0] + tsz;
+    FastDiv dz, dt;
+    dz.init(TZ);
+    dt.init(ntz);
+    auto tile_of = [&](int tile) {
+        const int y = dt.div(tile), z0 = (tile - y * ntz) * TZ;
+        return ColTile{(long long)y * Nz + z0, (long long)Ny * Nz, min(TZ, Nz - z0)};
+    };
+    auto fetch = [&](double2* S, double* NS, int tile) {
+        const ColTile c = tile_of(tile);
+        col_fetch(S, A, c, Nx, TZ, dz);
+#pragma unroll 4
+        for (int t = threadIdx.x; t < tsz; t += blockDim.x) {
+            const int e = dz.div(t), tz = t - e * TZ;
+            const bool ok = tz < c.nz;
+            cp_async8(NS + t, ok ? normC + c.base + e * c.stride + tz : normC, ok);
+        }
+    };
     const bool restart = restart_pass(ctl);
+    int tile = blockIdx.x;
+    if (tile < ntiles) fetch(B[0], NB[0], tile);
+    cp_async_commit();
     for (int t = threadIdx.x; t < Nx; t += blockDim.x) tw[t] = twx[t];
-    col_load(S0, A, c, Nx, TZ);
-    __syncthreads();
-    LineLayout L{TZ, TZ, 1, 0, TZ, true};
-    double2* r = fft_lines(S0, S1, tw, px, L, -1);
-    double2* o = (r == S0) ? S1 : S0;
+    const LineLayout L{TZ, TZ, 1, 0, TZ, true};
     double acc = 0;
-    for (int t = threadIdx.x; t < Nx * TZ; t += blockDim.x) {
-        const int tz = t % TZ, e = t / TZ;
-        if (tz >= c.nz) continue;  // padding columns stay zero through the inverse transform
-        const long long v = c.base + e * c.stride + tz;
-        const double2 w = r[t];
-        const double nc = normC[v];
-        acc += fabs(__dsub_rn(sqrt(__dadd_rn(__dmul_rn(w.x, w.x), __dmul_rn(w.y, w.y))), nc));
-        double ang = atan2(w.y, w.x);
-        if (restart) ang = __dadd_rn(R[v], __dmul_rn(ang, 0.7));
-        double s, co;
-        sincos(ang, &s, &co);
-        r[t] = make_double2(__dmul_rn(nc, co), __dmul_rn(nc, s));
+    int d = 0, nbi = 0;
+    for (; tile < ntiles; tile += gridDim.x) {
+        cp_async_wait_all();
+        __syncthreads();
+        const int f = d == 0 ? 2 : d - 1;
+        const int nxt = tile + gridDim.x;
+        if (nxt < ntiles) fetch(B[f], NB[nbi ^ 1], nxt);
+        cp_async_commit();
+        double2* r = fft_lines<double2, MaxR>(B[d], B[d == 2 ? 0 : d + 1], tw, px, L, -1);
+        double2* o = (r == B[d]) ? B[d == 2 ? 0 : d + 1] : B[d];
+        const ColTile c = tile_of(tile);
+        const double* nct = NB[nbi];
+#pragma unroll 2
+        for (int t = threadIdx.x; t < tsz; t += blockDim.x) {
+            const int e = dz.div(t), tz = t - e * TZ;
+            if (tz >= c.nz) continue;  // padding columns stay zero through the inverse transform
+            const double2 w = r[t];
+            const double nc = nct[t];
+            const double mod = sqrt(__dadd_rn(__dmul_rn(w.x, w.x), __dmul_rn(w.y, w.y)));
+            acc += fabs(__dsub_rn(mod, nc));
+            if (restart) {
+                const double ang = __dadd_rn(R[c.base + e * c.stride + tz], __dmul_rn(atan2(w.y, w.x), 0.7));
+                double sn, co;
+                sincos(ang, &sn, &co);
+                r[t] = make_double2(__dmul_rn(nc, co), __dmul_rn(nc, sn));
+            } else if (mod > 0) {
+                // normC e^{i arg M} = M normC / |M|: the same quantity as
+                // normC (cos(atan2), sin(atan2)) without the three transcendentals
+                const double fct = nc / mod;
+                r[t] = make_double2(w.x * fct, w.y * fct);
+            } else {
+                r[t] = make_double2(nc, 0.0);  // arg 0 = 0
+            }
+        }
+        __syncthreads();
+        const double2* q = fft_lines<double2, MaxR>(r, o, tw, px, L, +1);
+        col_store(A, q, c, Nx, TZ, dz);
+        d = f;
+        nbi ^= 1;
     }
-    // block partial in a fixed order: warp shuffle tree, then the warps in order
+    cp_async_wait_all();
+    // CTA partial in a fixed order: warp shuffle tree, then the warps in order
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, off);
     if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
     __syncthreads();
-    const double2* q = fft_lines(r, o, tw, px, L, +1);
-    col_store(A, q, c, Nx, TZ);
     if (threadIdx.x == 0) {
         double b = 0;
         for (int w = 0; w < kThreads / 32; ++w) b += red[w];
@@ -394,6 +533,7 @@ struct m3d_rec {
     int G = 1, TZ = 1, ntz = 1;
     long long zlines = 0;
     int nb_y = 0, nb_x = 0;
+    int grid_y = 1, grid_z = 1, grid_zi = 1, grid_x = 1, grid_xr = 1;  // persistent CTAs per pass
     double normC0 = 0;
     unsigned long long seed = 1;
     bool started = false;   // a field exists (run, set_state)
@@ -417,33 +557,81 @@ struct m3d_rec {
         if (h_ctl) cudaFreeHost(h_ctl);
         if (stream) cudaStreamDestroy(stream);
     }
-    size_t z_smem() const { return (size_t)Nz * 16 + 2 * (size_t)G * Nz * 16; }
-    size_t y_smem() const { return (size_t)Ny * 16 + 2 * (size_t)Ny * TZ * 16; }
-    size_t x_smem() const { return (size_t)Nx * 16 + 2 * (size_t)Nx * TZ * 16; }
+    size_t z_smem() const { return (size_t)Nz * 16 + 3 * (size_t)G * Nz * 16; }
+    size_t zi_smem() const { return z_smem() + 2 * (size_t)G * Nz * 8; }
+    size_t y_smem() const { return (size_t)Ny * 16 + 3 * (size_t)Ny * TZ * 16; }
+    size_t x_smem() const { return (size_t)Nx * 16 + 3 * (size_t)Nx * TZ * 16 + 2 * (size_t)Nx * TZ * 8; }
+    size_t xr_smem() const { return (size_t)Nx * 16 + 3 * (size_t)Nx * TZ * 16; }
     int grid1d() const { return (int)std::min<long long>(148 * 8, (xyz + kThreads - 1) / kThreads); }
 
     // the kernels of one pass, in order; `prof` brackets each with events
-    int launch_pass(bool prof) {
+    template <int MaxR>
+    int launch_pass_t(bool prof) {
         const int nbz = (int)((zlines + G - 1) / G);
         auto mark = [&](int k) { if (prof) cudaEventRecord(ev[k], stream); };
         mark(0);
-        krec_z<Z_RAND><<<nbz, kThreads, z_smem(), stream>>>(A, m, twz, pz, G, zlines, d_ctl);
-        krec_y<Y_RAND><<<nb_y, kThreads, y_smem(), stream>>>(A, twy, py, Nz, TZ, ntz, d_ctl);
-        krec_xrand<<<nb_x, kThreads, x_smem(), stream>>>(A, R, twx, px, Ny, Nz, TZ, ntz, d_ctl);
+        krec_z<Z_RAND, MaxR><<<grid_z, kThreads, z_smem(), stream>>>(A, m, twz, pz, G, zlines, nbz, d_ctl);
+        krec_y<Y_RAND, MaxR><<<grid_y, kThreads, y_smem(), stream>>>(A, twy, py, Nz, TZ, ntz, nb_y, d_ctl);
+        krec_xrand<MaxR><<<grid_xr, kThreads, xr_smem(), stream>>>(A, R, twx, px, Ny, Nz, TZ, ntz, nb_x, d_ctl);
         mark(1);
-        krec_z<Z_FWD><<<nbz, kThreads, z_smem(), stream>>>(A, m, twz, pz, G, zlines, d_ctl);
+        krec_z<Z_FWD, MaxR><<<grid_z, kThreads, z_smem(), stream>>>(A, m, twz, pz, G, zlines, nbz, d_ctl);
         mark(2);
-        krec_y<Y_FWD><<<nb_y, kThreads, y_smem(), stream>>>(A, twy, py, Nz, TZ, ntz, d_ctl);
+        krec_y<Y_FWD, MaxR><<<grid_y, kThreads, y_smem(), stream>>>(A, twy, py, Nz, TZ, ntz, nb_y, d_ctl);
         mark(3);
-        krec_xturn<<<nb_x, kThreads, x_smem(), stream>>>(A, normC, R, twx, px, Ny, Nz, TZ, ntz, part, errs, d_ctl);
+        krec_xturn<MaxR><<<grid_x, kThreads, x_smem(), stream>>>(A, normC, R, twx, px, Ny, Nz, TZ, ntz, nb_x, part, errs, d_ctl);
         mark(4);
-        krec_y<Y_INV><<<nb_y, kThreads, y_smem(), stream>>>(A, twy, py, Nz, TZ, ntz, d_ctl);
+        krec_y<Y_INV, MaxR><<<grid_y, kThreads, y_smem(), stream>>>(A, twy, py, Nz, TZ, ntz, nb_y, d_ctl);
         mark(5);
-        krec_z<Z_INV><<<nbz, kThreads, z_smem(), stream>>>(A, m, twz, pz, G, zlines, d_ctl);
+        krec_z<Z_INV, MaxR><<<grid_zi, kThreads, zi_smem(), stream>>>(A, m, twz, pz, G, zlines, nbz, d_ctl);
         mark(6);
         launches += 8;
         MR_CUDA(cudaGetLastError());
         return M3D_OK;
+    }
+    template <int MaxR>
+    void set_smem_t() {
+        const int zs = (int)z_smem(), ys = (int)y_smem(), xs = (int)x_smem();
+        cudaFuncSetAttribute(krec_z<Z_FWD, MaxR>, cudaFuncAttributeMaxDynamicSharedMemorySize, zs);
+        cudaFuncSetAttribute(krec_z<Z_RAND, MaxR>, cudaFuncAttributeMaxDynamicSharedMemorySize, zs);
+        cudaFuncSetAttribute(krec_z<Z_INV, MaxR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)zi_smem());
+        cudaFuncSetAttribute(krec_y<Y_FWD, MaxR>, cudaFuncAttributeMaxDynamicSharedMemorySize, ys);
+        cudaFuncSetAttribute(krec_y<Y_RAND, MaxR>, cudaFuncAttributeMaxDynamicSharedMemorySize, ys);
+        cudaFuncSetAttribute(krec_y<Y_INV, MaxR>, cudaFuncAttributeMaxDynamicSharedMemorySize, ys);
+        cudaFuncSetAttribute(krec_xrand<MaxR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)xr_smem());
+        cudaFuncSetAttribute(krec_xturn<MaxR>, cudaFuncAttributeMaxDynamicSharedMemorySize, xs);
+        int sms = 0;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+        sms = std::max(1, sms);
+        auto fill = [&](auto kern, size_t smem, int tiles) {
+            int per_sm = 0;
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kThreads, smem);
+            return std::max(1, std::min(tiles, std::max(1, per_sm) * sms));
+        };
+        grid_y = fill(krec_y<Y_FWD, MaxR>, (size_t)ys, nb_y);
+        grid_z = fill(krec_z<Z_FWD, MaxR>, (size_t)zs, (int)((zlines + G - 1) / G));
+        grid_zi = fill(krec_z<Z_INV, MaxR>, zi_smem(), (int)((zlines + G - 1) / G));
+        grid_x = fill(krec_xturn<MaxR>, (size_t)xs, nb_x);
+        grid_xr = fill(krec_xrand<MaxR>, xr_smem(), nb_x);
+    }
+    // kernels are instantiated for the largest odd radix of the grid's plans
+    // in buckets, so a grid of small factors does not pay the registers of a
+    // 31-point butterfly
+    int maxr = 5;
+    int launch_pass(bool prof) {
+        switch (maxr) {
+            case 5: return launch_pass_t<5>(prof);
+            case 13: return launch_pass_t<13>(prof);
+            case 19: return launch_pass_t<19>(prof);
+            default: return launch_pass_t<31>(prof);
+        }
+    }
+    void set_smem() {
+        switch (maxr) {
+            case 5: set_smem_t<5>(); break;
+            case 13: set_smem_t<13>(); break;
+            case 19: set_smem_t<19>(); break;
+            default: set_smem_t<31>(); break;
+        }
     }
 
     // grow the error track, keeping what it holds
@@ -630,15 +818,17 @@ int m3drec_create(int Nx, int Ny, int Nz, const double* tpcf, int device, m3d_re
         delete h;
         return failr(M3D_ERR_UNSUPPORTED, "grid sizes need prime factors <= 32");
     }
+    // ~48 KB of shared memory per CTA (two buffers of 16-byte elements) so
+    // that several CTAs share an SM
     h->G = std::max(1, std::min(16, (int)(48 * 1024 / (32 * (size_t)Nz))));
     const int nmax = std::max(Nx, Ny);
-    h->TZ = std::max(1, std::min(16, (int)(96 * 1024 / (32 * (size_t)nmax))));
+    h->TZ = std::max(1, std::min(16, (int)(48 * 1024 / (32 * (size_t)nmax))));
     h->TZ = std::min(h->TZ, Nz);
     h->ntz = (Nz + h->TZ - 1) / h->TZ;
     h->zlines = (long long)Nx * Ny;
     h->nb_y = Nx * h->ntz;
     h->nb_x = Ny * h->ntz;
-    if (h->z_smem() > 220 * 1024 || h->y_smem() > 220 * 1024 || h->x_smem() > 220 * 1024) {
+    if (h->zi_smem() > 220 * 1024 || h->y_smem() > 220 * 1024 || h->x_smem() > 220 * 1024) {
         delete h;
         return failr(M3D_ERR_UNSUPPORTED, "grid too large for the shared-memory line FFTs");
     }
@@ -673,15 +863,11 @@ int m3drec_create(int Nx, int Ny, int Nz, const double* tpcf, int device, m3d_re
     cudaMemset(h->m, 0, c16);
     cudaMemset(h->R, 0, c8);
     cudaMemset(h->d_ctl, 0, sizeof(RecCtl));
-    const int zs = (int)h->z_smem(), ys = (int)h->y_smem(), xs = (int)h->x_smem();
-    cudaFuncSetAttribute(krec_z<Z_FWD>, cudaFuncAttributeMaxDynamicSharedMemorySize, zs);
-    cudaFuncSetAttribute(krec_z<Z_RAND>, cudaFuncAttributeMaxDynamicSharedMemorySize, zs);
-    cudaFuncSetAttribute(krec_z<Z_INV>, cudaFuncAttributeMaxDynamicSharedMemorySize, zs);
-    cudaFuncSetAttribute(krec_y<Y_FWD>, cudaFuncAttributeMaxDynamicSharedMemorySize, ys);
-    cudaFuncSetAttribute(krec_y<Y_RAND>, cudaFuncAttributeMaxDynamicSharedMemorySize, ys);
-    cudaFuncSetAttribute(krec_y<Y_INV>, cudaFuncAttributeMaxDynamicSharedMemorySize, ys);
-    cudaFuncSetAttribute(krec_xrand, cudaFuncAttributeMaxDynamicSharedMemorySize, xs);
-    cudaFuncSetAttribute(krec_xturn, cudaFuncAttributeMaxDynamicSharedMemorySize, xs);
+    int mr = 5;
+    for (const LinePlan* pl : {&h->px, &h->py, &h->pz})
+        for (int k = 0; k < pl->nstages; ++k) mr = std::max(mr, pl->radix[k] == 8 ? 5 : pl->radix[k]);
+    h->maxr = mr <= 5 ? 5 : mr <= 13 ? 13 : mr <= 19 ? 19 : 31;
+    h->set_smem();
     if (cudaDeviceSynchronize() != cudaSuccess || cudaGetLastError() != cudaSuccess) {
         delete h;
         return failr(M3D_ERR_CUDA, "device set-up failed");
