@@ -461,13 +461,24 @@ __global__ void krec_cond(cudaGraphConditionalHandle h, RecCtl* ctl) {
     cudaGraphSetConditional(h, (!ctl->done && ctl->i < ctl->n && t <= ctl->n + 2) ? 1u : 0u);
 }
 
-// threshold walk (:370-395): one try = count voxels below 0.5 - x, then step x
-__global__ void krec_thr_count(const double2* __restrict__ m, RecCtl* ctl, long long xyz) {
+// threshold walk (:370-395).  The real parts are first copied to a
+// contiguous array (40 MB at 171^3, so it stays in L2 across the tries); one
+// try = one launch that counts the voxels below 0.5 - x (integer counts, so
+// the order does not matter) and whose last CTA steps x exactly as the
+// reference does and sets the loop condition.
+__global__ void krec_thr_prep(const double2* __restrict__ m, double* __restrict__ re, long long xyz) {
+    for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < xyz; v += (long long)gridDim.x * blockDim.x)
+        re[v] = m[v].x;
+}
+
+__global__ void krec_thr_try(const double* __restrict__ re, RecCtl* ctl, long long xyz,
+                             cudaGraphConditionalHandle h, int use_cond) {
     __shared__ unsigned int red[kThreads / 32];
+    __shared__ bool last;
     const double cut = __dsub_rn(0.5, ctl->x);
     unsigned int cnt = 0;
     for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < xyz; v += (long long)gridDim.x * blockDim.x)
-        cnt += m[v].x < cut ? 1u : 0u;
+        cnt += re[v] < cut ? 1u : 0u;
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) cnt += __shfl_down_sync(0xffffffffu, cnt, off);
     if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = cnt;
@@ -476,20 +487,23 @@ __global__ void krec_thr_count(const double2* __restrict__ m, RecCtl* ctl, long 
         unsigned long long b = 0;
         for (int w = 0; w < kThreads / 32; ++w) b += red[w];
         if (b) atomicAdd(&ctl->count_lt, b);
+        __threadfence();
+        last = atomicAdd(&ctl->ticket, 1u) == gridDim.x - 1;
     }
-}
-
-__global__ void krec_thr_step(cudaGraphConditionalHandle h, RecCtl* ctl, int use_cond) {
-    const long long xyz = ctl->xyz;
-    const double ones = (double)(xyz - (long long)ctl->count_lt);  // ang.sum() of the 0/1 field
+    __syncthreads();
+    if (!last || threadIdx.x != 0) return;
+    __threadfence();
+    const unsigned long long below = atomicAdd(&ctl->count_lt, 0ull);
+    const double ones = (double)(xyz - (long long)below);  // ang.sum() of the 0/1 field
     const double vol_dif = __dsub_rn(ones / (1.0 * xyz), ctl->normC0 / (1.0 * xyz));
-    ctl->cut = __dsub_rn(0.5, ctl->x);
+    ctl->cut = cut;
     if (vol_dif > 0) ctl->x = __dsub_rn(ctl->x, 0.001);
     else ctl->x = __dadd_rn(ctl->x, 0.001);
     const bool stop = fabs(vol_dif) < 0.0001 || ctl->ctr > 200;
     if (!stop) ctl->ctr += 1;
     ctl->thr_done = stop;
     ctl->count_lt = 0;
+    ctl->ticket = 0;
     const int t = ++ctl->trips;
     if (use_cond) cudaGraphSetConditional(h, (!stop && t <= 203) ? 1u : 0u);
 }
@@ -691,8 +705,7 @@ struct m3d_rec {
         if (e == cudaSuccess) e = add_while(top, nullptr, 0, h, &node, &body);
         if (e == cudaSuccess) e = cudaStreamBeginCaptureToGraph(stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed);
         if (e == cudaSuccess) {
-            krec_thr_count<<<grid1d(), kThreads, 0, stream>>>(m, d_ctl, xyz);
-            krec_thr_step<<<1, 1, 0, stream>>>(h, d_ctl, 1);
+            krec_thr_try<<<grid1d(), kThreads, 0, stream>>>(R, d_ctl, xyz, h, 1);
             cudaGraph_t got = nullptr;
             e = cudaGetLastError();
             const cudaError_t e2 = cudaStreamEndCapture(stream, &got);
@@ -769,11 +782,12 @@ struct m3d_rec {
         c.i = i; c.j = j; c.seed = seed; c.call = call;
         *h_ctl = c;
         MR_CUDA(cudaMemcpyAsync(d_ctl, h_ctl, sizeof(RecCtl), cudaMemcpyHostToDevice, stream));
+        krec_thr_prep<<<grid1d(), kThreads, 0, stream>>>(m, R, xyz);  // R is free between passes
+        launches += 1;
         if (profiling) {
             for (int t = 0; t < 203; ++t) {
-                krec_thr_count<<<grid1d(), kThreads, 0, stream>>>(m, d_ctl, xyz);
-                krec_thr_step<<<1, 1, 0, stream>>>(cudaGraphConditionalHandle{}, d_ctl, 0);
-                launches += 2;
+                krec_thr_try<<<grid1d(), kThreads, 0, stream>>>(R, d_ctl, xyz, cudaGraphConditionalHandle{}, 0);
+                launches += 1;
                 MR_CUDA(cudaGetLastError());
                 const int rc = pull_ctl();
                 if (rc) return rc;
@@ -792,7 +806,7 @@ struct m3d_rec {
         MR_CUDA(cudaGetLastError());
         const int rc = pull_ctl();
         if (rc) return rc;
-        if (!profiling) launches += 2LL * h_ctl->trips;
+        if (!profiling) launches += h_ctl->trips;
         if (!h_ctl->thr_done) return failr(M3D_ERR_CUDA, "threshold walk did not finish");
         return M3D_OK;
     }
