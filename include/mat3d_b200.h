@@ -340,6 +340,13 @@ void* m3d2d_get_stream(const m3d_solver2d* h);
      m3drec_get_error     the public member trackrealerrorA    include/reconstruction.hpp:73
      m3drec_fftshift      recon::fftshift                      :47-90
      m3drec_ifftshift     recon::ifftshift                     :97-140
+     m3drec_create_from_sections
+                          recPlan(CImg c1, CImg c2)            :145-206 (8-bit sections, x fastest;
+                                                                         both of one size, grid w x h x h)
+     m3drec_estimate_norm estimateNormFFT_RVE()                :245-281
+     m3drec_save_images   saveRecImages(folder)                :403-432 (PNG slices, rve_rec.txt, err.txt)
+     m3drec_write_vti     vtiWriter(file, tpcf)                :435-470
+     m3drec_fft3          the example's fftw_plan_dft_3d + fftw_execute (example/reconst3d/main.cpp:85-107)
    Beyond the reference: m3drec_iterate continues the loop from the current
    state without the closing threshold, m3drec_threshold applies it, and
    m3drec_set_state / m3drec_get_state move the complete loop state (field as
@@ -361,6 +368,13 @@ int m3drec_set_profiling(m3d_rec* h, int on);
 int m3drec_profile(const m3d_rec* h, double* ms6, long long* passes);
 long long m3drec_kernel_launches(const m3d_rec* h);
 void* m3drec_get_stream(const m3d_rec* h);
+int m3drec_create_from_sections(const unsigned char* c1, int w1, int h1, const unsigned char* c2, int w2, int h2,
+                                int device, m3d_rec** out);
+int m3drec_estimate_norm(m3d_rec* h);
+int m3drec_get_norm(m3d_rec* h, double* out);
+int m3drec_save_images(m3d_rec* h, const char* folder);
+int m3drec_write_vti(m3d_rec* h, const char* file, const double* tpcf);
+int m3drec_fft3(const double* in, double* out, int Nx, int Ny, int Nz, int sign, int device);
 int m3drec_fftshift(const double* in, double* out, int Nx, int Ny, int Nz);
 int m3drec_ifftshift(const double* in, double* out, int Nx, int Ny, int Nz);
 

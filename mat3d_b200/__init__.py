@@ -127,6 +127,8 @@ EXPORTS = [
     "m3drec_create", "m3drec_destroy", "m3drec_seed", "m3drec_run", "m3drec_iterate", "m3drec_threshold",
     "m3drec_set_state", "m3drec_get_state", "m3drec_get_field", "m3drec_get_error", "m3drec_set_profiling",
     "m3drec_profile", "m3drec_kernel_launches", "m3drec_get_stream", "m3drec_fftshift", "m3drec_ifftshift",
+    "m3drec_create_from_sections", "m3drec_estimate_norm", "m3drec_get_norm", "m3drec_save_images",
+    "m3drec_write_vti", "m3drec_fft3",
 ]
 
 
@@ -218,6 +220,12 @@ def load_library(path: str | None = None):
     L.m3drec_get_stream.restype = vp
     L.m3drec_fftshift.argtypes = [vp, vp, i, i, i]
     L.m3drec_ifftshift.argtypes = [vp, vp, i, i, i]
+    L.m3drec_create_from_sections.argtypes = [vp, i, i, vp, i, i, i, ctypes.POINTER(vp)]
+    L.m3drec_estimate_norm.argtypes = [vp]
+    L.m3drec_get_norm.argtypes = [vp, vp]
+    L.m3drec_save_images.argtypes = [vp, ctypes.c_char_p]
+    L.m3drec_write_vti.argtypes = [vp, ctypes.c_char_p, vp]
+    L.m3drec_fft3.argtypes = [vp, vp, i, i, i, i, i]
     if path is None:
         _lib = L
     return L
@@ -720,19 +728,52 @@ def ifftshift(a, Nx, Ny, Nz):
     return _shift("m3drec_ifftshift", a, Nx, Ny, Nz)
 
 
+def fft3(a, shape, sign=-1, device=0):
+    """One unnormalised 3-D complex transform on the GPU (m3drec_fft3)."""
+    L = load_library()
+    x = np.ascontiguousarray(np.asarray(a, np.complex128).ravel())
+    out = np.empty_like(x)
+    _check(L, L.m3drec_fft3(_ptr(x), _ptr(out), *shape, int(sign), device), "m3drec_fft3")
+    return out
+
+
 class Reconstruction:
     """Phase-retrieval reconstruction of a two-phase field from its two-point
-    correlation function on the GPU (m3drec_*)."""
+    correlation function on the GPU (m3drec_*).  ``sections=(c1, c2)`` (2-D
+    uint8 arrays indexed [y, x], i.e. images of height x width) builds the
+    plan from two cut sections instead; call ``estimate_norm`` before ``run``."""
 
-    def __init__(self, tpcf, Nx, Ny, Nz, device=0):
+    def __init__(self, tpcf, Nx=None, Ny=None, Nz=None, device=0, sections=None):
         self.L = load_library()
-        self.Nx, self.Ny, self.Nz, self.xyz = Nx, Ny, Nz, Nx * Ny * Nz
-        t = np.ascontiguousarray(np.asarray(tpcf, np.float64).ravel())
-        if t.size != self.xyz:
-            raise ValueError("tpcf must hold Nx * Ny * Nz values")
         h = ctypes.c_void_p()
-        _check(self.L, self.L.m3drec_create(Nx, Ny, Nz, _ptr(t), device, ctypes.byref(h)), "m3drec_create")
+        if sections is not None:
+            c1, c2 = (np.ascontiguousarray(np.asarray(c, np.uint8)) for c in sections)
+            (h1, w1), (h2, w2) = c1.shape, c2.shape
+            _check(self.L, self.L.m3drec_create_from_sections(_ptr(c1), w1, h1, _ptr(c2), w2, h2, device,
+                                                              ctypes.byref(h)), "m3drec_create_from_sections")
+            Nx, Ny, Nz = w1, h1, h2
+        else:
+            t = np.ascontiguousarray(np.asarray(tpcf, np.float64).ravel())
+            if t.size != Nx * Ny * Nz:
+                raise ValueError("tpcf must hold Nx * Ny * Nz values")
+            _check(self.L, self.L.m3drec_create(Nx, Ny, Nz, _ptr(t), device, ctypes.byref(h)), "m3drec_create")
+        self.Nx, self.Ny, self.Nz, self.xyz = Nx, Ny, Nz, Nx * Ny * Nz
         self.h = h
+
+    def estimate_norm(self):
+        _check(self.L, self.L.m3drec_estimate_norm(self.h), "estimateNormFFT_RVE")
+
+    def norm(self):
+        out = np.zeros(self.xyz)
+        _check(self.L, self.L.m3drec_get_norm(self.h, _ptr(out)), "get_norm")
+        return out
+
+    def save_images(self, folder):
+        _check(self.L, self.L.m3drec_save_images(self.h, str(folder).encode()), "saveRecImages")
+
+    def write_vti(self, path, tpcf):
+        t = np.ascontiguousarray(np.asarray(tpcf, np.float64).ravel())
+        _check(self.L, self.L.m3drec_write_vti(self.h, str(path).encode(), _ptr(t)), "vtiWriter")
 
     def seed(self, seed):
         _check(self.L, self.L.m3drec_seed(self.h, int(seed)), "seed")
@@ -812,12 +853,32 @@ class recPlan:
         self.trackrealerrorA = np.zeros(0)
         self.mTilda = None
 
+    @classmethod
+    def from_sections(cls, c1, c2, seed=1):
+        """recPlan(CImg c1, CImg c2): two cut sections (uint8, [y, x])."""
+        self = cls.__new__(cls)
+        self._r = Reconstruction(None, sections=(c1, c2))
+        self._r.seed(seed)
+        self.Nx, self.Ny, self.Nz = self._r.Nx, self._r.Ny, self._r.Nz
+        self.trackrealerrorA = np.zeros(0)
+        self.mTilda = None
+        return self
+
+    def estimateNormFFT_RVE(self):
+        self._r.estimate_norm()
+
     def runRec(self, n, b):
         self._r.run(n, b)
         e = self._r.errors()
         self.trackrealerrorA = np.zeros(n)
         self.trackrealerrorA[:min(n, e.size)] = e[:n]
         self.mTilda = self._r.field()
+
+    def saveRecImages(self, locFldr):
+        self._r.save_images(locFldr)
+
+    def vtiWriter(self, fileName, tpcf):
+        self._r.write_vti(fileName, tpcf)
 
     def close(self):
         self._r.close()

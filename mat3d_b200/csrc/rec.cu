@@ -42,9 +42,13 @@
 // pass), so long runs agree with the CPU statistically, not bit for bit.
 #include <cuda_runtime.h>
 
+#include <sys/stat.h>
+
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
 #include <cstring>
+#include <fstream>
 #include <string>
 #include <vector>
 
@@ -120,7 +124,7 @@ __device__ __forceinline__ void cp_async8(void* sdst, const void* gsrc, bool val
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 
-enum ZMode { Z_FWD = 0, Z_RAND = 1, Z_INV = 2 };
+enum ZMode { Z_FWD = 0, Z_RAND = 1, Z_INV = 2, Z_BWD = 3 };
 
 // z lines (contiguous): tiles of G lines of length Nz, walked by persistent
 // CTAs with three shared buffers (the next tile streams in by cp.async while
@@ -128,6 +132,7 @@ enum ZMode { Z_FWD = 0, Z_RAND = 1, Z_INV = 2 };
 //   Z_FWD : A = FFT_z(m)
 //   Z_RAND: A = FFT_z(U') on restart passes (U' = draw `call`, real)
 //   Z_INV : m = projection(IFFT_z(A) / xyz, m) unless the pass converged
+//   Z_BWD : A = unnormalised inverse FFT_z(m) (plain transforms)
 template <int MODE, int MaxR>
 __global__ void __launch_bounds__(kThreads) krec_z(double2* __restrict__ A, double2* __restrict__ m,
                                                     const double2* __restrict__ twz, LinePlan pz, int G,
@@ -148,7 +153,7 @@ __global__ void __launch_bounds__(kThreads) krec_z(double2* __restrict__ A, doub
     const long long xyz = ctl->xyz;
     unsigned long long base = 0;
     if (MODE == Z_RAND) base = draw_base(ctl->seed, ctl->call);
-    const double2* src = MODE == Z_FWD ? m : A;
+    const double2* src = (MODE == Z_FWD || MODE == Z_BWD) ? m : A;
     // a tile's G lines are one contiguous run of voxels: v0 = tile G Nz ..
     auto valid_of = [&](int tile) { return (int)(min((long long)G, nlines - (long long)tile * G) * Nz); };
     auto fetch = [&](double2* S, double* MS, int tile) {
@@ -178,7 +183,8 @@ __global__ void __launch_bounds__(kThreads) krec_z(double2* __restrict__ A, doub
         const int nxt = tile + gridDim.x;
         if (nxt < ntiles) fetch(B[f], MB[mbi ^ 1], nxt);
         cp_async_commit();
-        double2* r = fft_lines<double2, MaxR>(B[d], B[d == 2 ? 0 : d + 1], tw, pz, L, MODE == Z_INV ? +1 : -1);
+        double2* r = fft_lines<double2, MaxR>(B[d], B[d == 2 ? 0 : d + 1], tw, pz, L,
+                                              (MODE == Z_INV || MODE == Z_BWD) ? +1 : -1);
         const double* old = MB[mbi];
         const long long v0 = (long long)tile * tsz;
         const int valid = valid_of(tile);
@@ -283,13 +289,17 @@ __global__ void __launch_bounds__(kThreads) krec_y(double2* __restrict__ A, cons
     cp_async_wait_all();
 }
 
-// x lines of a restart pass: R = 0.3 arg FFT(U') (:326-327); persistent CTAs
-// as the y passes
-template <int MaxR>
-__global__ void __launch_bounds__(kThreads) krec_xrand(const double2* __restrict__ A, double* __restrict__ R,
-                                                        const double2* __restrict__ twx, LinePlan px, int Ny, int Nz,
-                                                        int TZ, int ntz, int ntiles, const RecCtl* __restrict__ ctl) {
-    if (!restart_pass(ctl)) return;
+// x lines with an element-wise output, persistent CTAs as the y passes:
+//   XO_ANGLE: restart passes only, R = 0.3 arg FFT(U') (:326-327)
+//   XO_COPY : A = the transform (plain transforms, sign as given)
+//   XO_NORM : R = sqrt(sqrt(re^2 + im^2)) of the transform (estimateNormFFT_RVE :276-277)
+enum XOut { XO_ANGLE = 0, XO_COPY = 1, XO_NORM = 2 };
+template <int OUT, int MaxR>
+__global__ void __launch_bounds__(kThreads) krec_xout(double2* __restrict__ A, double* __restrict__ R,
+                                                       const double2* __restrict__ twx, LinePlan px, int Ny, int Nz,
+                                                       int TZ, int ntz, int ntiles, int sign,
+                                                       const RecCtl* __restrict__ ctl) {
+    if (OUT == XO_ANGLE && !restart_pass(ctl)) return;
     extern __shared__ __align__(16) char smem_raw[];
     const int Nx = px.n;
     double2* tw = (double2*)smem_raw;
@@ -317,11 +327,19 @@ __global__ void __launch_bounds__(kThreads) krec_xrand(const double2* __restrict
         const int nxt = tile + gridDim.x;
         if (nxt < ntiles) col_fetch(B[f], A, tile_of(nxt), Nx, TZ, dz);
         cp_async_commit();
-        const double2* r = fft_lines<double2, MaxR>(B[d], B[d == 2 ? 0 : d + 1], tw, px, L, -1);
+        const double2* r = fft_lines<double2, MaxR>(B[d], B[d == 2 ? 0 : d + 1], tw, px, L, sign);
         const ColTile c = tile_of(tile);
-        for (int t = threadIdx.x; t < Nx * TZ; t += blockDim.x) {
-            const int e = dz.div(t), tz = t - e * TZ;
-            if (tz < c.nz) R[c.base + e * c.stride + tz] = __dmul_rn(atan2(r[t].y, r[t].x), 0.3);
+        if (OUT == XO_COPY) {
+            col_store(A, r, c, Nx, TZ, dz);
+        } else {
+            for (int t = threadIdx.x; t < Nx * TZ; t += blockDim.x) {
+                const int e = dz.div(t), tz = t - e * TZ;
+                if (tz >= c.nz) continue;
+                const double2 w = r[t];
+                R[c.base + e * c.stride + tz] =
+                    OUT == XO_ANGLE ? __dmul_rn(atan2(w.y, w.x), 0.3)
+                                    : sqrt(sqrt(__dadd_rn(__dmul_rn(w.x, w.x), __dmul_rn(w.y, w.y))));
+            }
         }
         d = f;
     }
@@ -551,6 +569,10 @@ struct m3d_rec {
     double normC0 = 0;
     unsigned long long seed = 1;
     bool started = false;   // a field exists (run, set_state)
+    bool norm_set = false;  // normC holds the target modulus
+    std::vector<int> cc1, cc2;  // the cut sections as 0/1 (section constructor)
+    int Nzz = 0;
+    int last_n = 0;         // n of the last runRec (numloops)
     int i = 0, j = 0;       // host copy of the loop state
     unsigned long long call = 0;
     int n_recorded = 0;
@@ -586,7 +608,7 @@ struct m3d_rec {
         mark(0);
         krec_z<Z_RAND, MaxR><<<grid_z, kThreads, z_smem(), stream>>>(A, m, twz, pz, G, zlines, nbz, d_ctl);
         krec_y<Y_RAND, MaxR><<<grid_y, kThreads, y_smem(), stream>>>(A, twy, py, Nz, TZ, ntz, nb_y, d_ctl);
-        krec_xrand<MaxR><<<grid_xr, kThreads, xr_smem(), stream>>>(A, R, twx, px, Ny, Nz, TZ, ntz, nb_x, d_ctl);
+        krec_xout<XO_ANGLE, MaxR><<<grid_xr, kThreads, xr_smem(), stream>>>(A, R, twx, px, Ny, Nz, TZ, ntz, nb_x, -1, d_ctl);
         mark(1);
         krec_z<Z_FWD, MaxR><<<grid_z, kThreads, z_smem(), stream>>>(A, m, twz, pz, G, zlines, nbz, d_ctl);
         mark(2);
@@ -602,6 +624,35 @@ struct m3d_rec {
         MR_CUDA(cudaGetLastError());
         return M3D_OK;
     }
+    // one plain 3-D transform of m (sign -1 forward, +1 inverse, unnormalised):
+    // into A (out_norm false) or sqrt|.| into R (out_norm true)
+    template <int MaxR>
+    int transform_t(int sign, bool out_norm) {
+        const int nbz = (int)((zlines + G - 1) / G);
+        if (sign < 0) krec_z<Z_FWD, MaxR><<<grid_z, kThreads, z_smem(), stream>>>(A, m, twz, pz, G, zlines, nbz, d_ctl);
+        else krec_z<Z_BWD, MaxR><<<grid_z, kThreads, z_smem(), stream>>>(A, m, twz, pz, G, zlines, nbz, d_ctl);
+        if (sign < 0) krec_y<Y_FWD, MaxR><<<grid_y, kThreads, y_smem(), stream>>>(A, twy, py, Nz, TZ, ntz, nb_y, d_ctl);
+        else krec_y<Y_INV, MaxR><<<grid_y, kThreads, y_smem(), stream>>>(A, twy, py, Nz, TZ, ntz, nb_y, d_ctl);
+        if (out_norm)
+            krec_xout<XO_NORM, MaxR><<<grid_xr, kThreads, xr_smem(), stream>>>(A, R, twx, px, Ny, Nz, TZ, ntz, nb_x, sign, d_ctl);
+        else
+            krec_xout<XO_COPY, MaxR><<<grid_xr, kThreads, xr_smem(), stream>>>(A, R, twx, px, Ny, Nz, TZ, ntz, nb_x, sign, d_ctl);
+        launches += 3;
+        MR_CUDA(cudaGetLastError());
+        return M3D_OK;
+    }
+    int transform(int sign, bool out_norm) {
+        RecCtl c{};  // i = 0, not done: the pass kernels' early exits stay closed
+        c.xyz = xyz;
+        *h_ctl = c;
+        MR_CUDA(cudaMemcpyAsync(d_ctl, h_ctl, sizeof(RecCtl), cudaMemcpyHostToDevice, stream));
+        switch (maxr) {
+            case 5: return transform_t<5>(sign, out_norm);
+            case 13: return transform_t<13>(sign, out_norm);
+            case 19: return transform_t<19>(sign, out_norm);
+            default: return transform_t<31>(sign, out_norm);
+        }
+    }
     template <int MaxR>
     void set_smem_t() {
         const int zs = (int)z_smem(), ys = (int)y_smem(), xs = (int)x_smem();
@@ -611,7 +662,10 @@ struct m3d_rec {
         cudaFuncSetAttribute(krec_y<Y_FWD, MaxR>, cudaFuncAttributeMaxDynamicSharedMemorySize, ys);
         cudaFuncSetAttribute(krec_y<Y_RAND, MaxR>, cudaFuncAttributeMaxDynamicSharedMemorySize, ys);
         cudaFuncSetAttribute(krec_y<Y_INV, MaxR>, cudaFuncAttributeMaxDynamicSharedMemorySize, ys);
-        cudaFuncSetAttribute(krec_xrand<MaxR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)xr_smem());
+        cudaFuncSetAttribute(krec_xout<XO_ANGLE, MaxR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)xr_smem());
+        cudaFuncSetAttribute(krec_xout<XO_COPY, MaxR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)xr_smem());
+        cudaFuncSetAttribute(krec_xout<XO_NORM, MaxR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)xr_smem());
+        cudaFuncSetAttribute(krec_z<Z_BWD, MaxR>, cudaFuncAttributeMaxDynamicSharedMemorySize, zs);
         cudaFuncSetAttribute(krec_xturn<MaxR>, cudaFuncAttributeMaxDynamicSharedMemorySize, xs);
         int sms = 0;
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
@@ -625,7 +679,7 @@ struct m3d_rec {
         grid_z = fill(krec_z<Z_FWD, MaxR>, (size_t)zs, (int)((zlines + G - 1) / G));
         grid_zi = fill(krec_z<Z_INV, MaxR>, zi_smem(), (int)((zlines + G - 1) / G));
         grid_x = fill(krec_xturn<MaxR>, (size_t)xs, nb_x);
-        grid_xr = fill(krec_xrand<MaxR>, xr_smem(), nb_x);
+        grid_xr = fill(krec_xout<XO_ANGLE, MaxR>, xr_smem(), nb_x);
     }
     // kernels are instantiated for the largest odd radix of the grid's plans
     // in buckets, so a grid of small factors does not pay the registers of a
@@ -814,10 +868,11 @@ struct m3d_rec {
 
 extern "C" {
 
-int m3drec_create(int Nx, int Ny, int Nz, const double* tpcf, int device, m3d_rec** out) {
-    if (!out) return failr(M3D_ERR_ARG, "out is NULL");
+}  // extern "C"
+
+// a handle of the given grid with every buffer allocated; normC not set
+static int rec_alloc(int Nx, int Ny, int Nz, int device, m3d_rec** out) {
     *out = nullptr;
-    if (!tpcf) return failr(M3D_ERR_ARG, "tpcf is NULL");
     if (Nx < 1 || Ny < 1 || Nz < 1 || Nx > 2048 || Ny > 2048 || Nz > 2048)
         return failr(M3D_ERR_ARG, "grid sizes must be in [1, 2048]");
     int ndev = 0;
@@ -865,12 +920,8 @@ int m3drec_create(int Nx, int Ny, int Nz, const double* tpcf, int device, m3d_re
             delete h;
             return failr(M3D_ERR_CUDA, "event creation failed");
         }
-    // normC = sqrt(|TPCF| * xyz) (:238-239)
-    std::vector<double> nc((size_t)h->xyz);
-    for (long long v = 0; v < h->xyz; ++v) nc[v] = std::sqrt(std::fabs(tpcf[v]) * (double)h->xyz);
-    h->normC0 = nc[0];
     const auto tx = twiddles<double>(Nx), ty = twiddles<double>(Ny), tz = twiddles<double>(Nz);
-    cudaMemcpy(h->normC, nc.data(), c8, cudaMemcpyHostToDevice);
+    cudaMemset(h->normC, 0, c8);
     cudaMemcpy(h->twx, tx.data(), Nx * sizeof(double2), cudaMemcpyHostToDevice);
     cudaMemcpy(h->twy, ty.data(), Ny * sizeof(double2), cudaMemcpyHostToDevice);
     cudaMemcpy(h->twz, tz.data(), Nz * sizeof(double2), cudaMemcpyHostToDevice);
@@ -888,6 +939,223 @@ int m3drec_create(int Nx, int Ny, int Nz, const double* tpcf, int device, m3d_re
     }
     *out = h;
     return M3D_OK;
+}
+
+// host complex array (xyz (re, im) pairs) -> m; transform; A -> host
+static int rec_fft_host(m3d_rec* h, const double* in, double* out, int sign) {
+    const size_t c16 = (size_t)h->xyz * sizeof(double2);
+    MR_CUDA(cudaMemcpyAsync(h->m, in, c16, cudaMemcpyHostToDevice, h->stream));
+    int rc = h->transform(sign, false);
+    if (rc) return rc;
+    MR_CUDA(cudaMemcpyAsync(out, h->A, c16, cudaMemcpyDeviceToHost, h->stream));
+    MR_CUDA(cudaStreamSynchronize(h->stream));
+    return M3D_OK;
+}
+
+// two's-complement wrap of an int product, as the reference's int arithmetic
+static double int_product(long long a, long long b, long long c, long long d) {
+    const unsigned long long u = (unsigned long long)a * (unsigned long long)b * (unsigned long long)c *
+                                 (unsigned long long)d;
+    return (double)(int)(unsigned)(u & 0xFFFFFFFFull);
+}
+
+// writers -----------------------------------------------------------------
+static unsigned crc32_of(const unsigned char* p, size_t n, unsigned crc = 0xFFFFFFFFu) {
+    static unsigned table[256];
+    static bool init = false;
+    if (!init) {
+        for (unsigned i = 0; i < 256; ++i) {
+            unsigned c = i;
+            for (int k = 0; k < 8; ++k) c = (c & 1) ? 0xEDB88320u ^ (c >> 1) : c >> 1;
+            table[i] = c;
+        }
+        init = true;
+    }
+    for (size_t i = 0; i < n; ++i) crc = table[(crc ^ p[i]) & 0xFF] ^ (crc >> 8);
+    return crc;
+}
+
+// 8-bit greyscale PNG (zlib stream of stored deflate blocks: no compression library needed)
+static bool write_png_gray(const std::string& path, int w, int h, const unsigned char* px) {
+    std::vector<unsigned char> raw;
+    raw.reserve((size_t)(w + 1) * h);
+    for (int y = 0; y < h; ++y) {
+        raw.push_back(0);  // filter: none
+        raw.insert(raw.end(), px + (size_t)y * w, px + (size_t)(y + 1) * w);
+    }
+    std::vector<unsigned char> z = {0x78, 0x01};
+    unsigned a = 1, b = 0;
+    for (unsigned char c : raw) { a = (a + c) % 65521u; b = (b + a) % 65521u; }
+    for (size_t off = 0; off < raw.size() || off == 0;) {
+        const size_t len = std::min<size_t>(65535, raw.size() - off);
+        const bool final = off + len >= raw.size();
+        z.push_back(final ? 1 : 0);
+        z.push_back(len & 0xFF); z.push_back(len >> 8);
+        z.push_back(~len & 0xFF); z.push_back((~len >> 8) & 0xFF);
+        z.insert(z.end(), raw.begin() + off, raw.begin() + off + len);
+        off += len;
+        if (final) break;
+    }
+    const unsigned ad = (b << 16) | a;
+    for (int k = 3; k >= 0; --k) z.push_back((ad >> (8 * k)) & 0xFF);
+    FILE* f = std::fopen(path.c_str(), "wb");
+    if (!f) return false;
+    auto be32 = [](unsigned v, unsigned char* o) { o[0] = v >> 24; o[1] = v >> 16; o[2] = v >> 8; o[3] = v; };
+    auto chunk = [&](const char* type, const std::vector<unsigned char>& data) {
+        unsigned char hdr[8];
+        be32((unsigned)data.size(), hdr);
+        std::memcpy(hdr + 4, type, 4);
+        std::fwrite(hdr, 1, 8, f);
+        if (!data.empty()) std::fwrite(data.data(), 1, data.size(), f);
+        unsigned crc = crc32_of((const unsigned char*)type, 4);
+        crc = crc32_of(data.data(), data.size(), crc) ^ 0xFFFFFFFFu;
+        unsigned char c4[4];
+        be32(crc, c4);
+        std::fwrite(c4, 1, 4, f);
+    };
+    static const unsigned char sig[8] = {0x89, 'P', 'N', 'G', 0x0D, 0x0A, 0x1A, 0x0A};
+    std::fwrite(sig, 1, 8, f);
+    std::vector<unsigned char> ihdr(13);
+    be32(w, ihdr.data());
+    be32(h, ihdr.data() + 4);
+    ihdr[8] = 8; ihdr[9] = 0; ihdr[10] = 0; ihdr[11] = 0; ihdr[12] = 0;  // 8-bit grey, no interlace
+    chunk("IHDR", ihdr);
+    chunk("IDAT", z);
+    chunk("IEND", {});
+    return std::fclose(f) == 0;
+}
+
+extern "C" {
+
+int m3drec_create(int Nx, int Ny, int Nz, const double* tpcf, int device, m3d_rec** out) {
+    if (!out) return failr(M3D_ERR_ARG, "out is NULL");
+    *out = nullptr;
+    if (!tpcf) return failr(M3D_ERR_ARG, "tpcf is NULL");
+    m3d_rec* h = nullptr;
+    int rc = rec_alloc(Nx, Ny, Nz, device, &h);
+    if (rc) return rc;
+    // normC = sqrt(|TPCF| * xyz) (:238-239)
+    std::vector<double> nc((size_t)h->xyz);
+    for (long long v = 0; v < h->xyz; ++v) nc[v] = std::sqrt(std::fabs(tpcf[v]) * (double)h->xyz);
+    h->normC0 = nc[0];
+    if (cudaMemcpy(h->normC, nc.data(), nc.size() * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess) {
+        delete h;
+        return failr(M3D_ERR_CUDA, "normC upload failed");
+    }
+    h->norm_set = true;
+    *out = h;
+    return M3D_OK;
+}
+
+// recPlan(CImg c1, CImg c2) :145-206: two perpendicular cut sections, 8-bit
+// images stored x fastest (CImg's layout: pixel (x, y) at x + width * y).
+// The grid is width1 x height1 x height2.  Each section becomes 0/1 by the
+// reference's integer division pixel / max(pixel).  The reference fills the
+// second section's array over the first one's extent, so both must have the
+// same size (other sizes overrun its arrays); an all-zero section divides by
+// zero there -- both are rejected here.
+int m3drec_create_from_sections(const unsigned char* c1, int w1, int h1, const unsigned char* c2, int w2, int h2,
+                                int device, m3d_rec** out) {
+    if (!out) return failr(M3D_ERR_ARG, "out is NULL");
+    *out = nullptr;
+    if (!c1 || !c2) return failr(M3D_ERR_ARG, "NULL section");
+    if (w1 != w2 || h1 != h2) return failr(M3D_ERR_ARG, "the two sections must have the same size");
+    int max1 = 0, max2 = 0;
+    for (int i = 0; i < w1; ++i)
+        for (int j = 0; j < h1; ++j) {
+            max1 = std::max(max1, (int)c1[i + (size_t)w1 * j]);
+            max2 = std::max(max2, (int)c2[i + (size_t)w2 * j]);
+        }
+    if (max1 == 0 || max2 == 0) return failr(M3D_ERR_ARG, "a section has no nonzero pixel");
+    m3d_rec* h = nullptr;
+    int rc = rec_alloc(w1, h1, h2, device, &h);
+    if (rc) return rc;
+    h->Nzz = w2;
+    h->cc1.resize((size_t)w1 * h1);
+    h->cc2.resize((size_t)w1 * h1);
+    for (int j = 0; j < w1; ++j)
+        for (int k = 0; k < h1; ++k) {
+            h->cc1[k + (size_t)j * h1] = (int)c1[j + (size_t)w1 * k] / max1;
+            h->cc2[k + (size_t)j * h1] = (int)c2[j + (size_t)w2 * k] / max2;
+        }
+    *out = h;
+    return M3D_OK;
+}
+
+// estimateNormFFT_RVE :245-281: the sections' autocorrelations by 2-D
+// transforms, the separable two-point estimate, normC = sqrt|FFT3(estimate)|
+int m3drec_estimate_norm(m3d_rec* h) {
+    if (!h) return failr(M3D_ERR_ARG, "NULL handle");
+    if (h->cc1.empty()) return failr(M3D_ERR_STATE, "the handle was not made from cut sections");
+    MR_CUDA(cudaSetDevice(h->device));
+    const int Nx = h->Nx, Ny = h->Ny, Nz = h->Nz, Nzz = h->Nzz;
+    auto autocorr = [&](const std::vector<int>& cc, int a, int b, std::vector<double>& res) -> int {
+        m3d_rec* t = nullptr;
+        int rc = rec_alloc(a, b, 1, h->device, &t);
+        if (rc) return rc;
+        const size_t n = (size_t)a * b;
+        std::vector<double> in(2 * n), sp(2 * n);
+        for (size_t i = 0; i < n; ++i) { in[2 * i] = (double)cc[i]; in[2 * i + 1] = 0; }
+        rc = rec_fft_host(t, in.data(), sp.data(), -1);
+        const double den = int_product(a, b, a, b);
+        for (size_t i = 0; i < n && !rc; ++i) {
+            in[2 * i] = (sp[2 * i] * sp[2 * i] + sp[2 * i + 1] * sp[2 * i + 1]) / den;
+            in[2 * i + 1] = 0;
+        }
+        res.resize(2 * n);
+        if (!rc) rc = rec_fft_host(t, in.data(), res.data(), +1);
+        m3drec_destroy(t);
+        return rc;
+    };
+    std::vector<double> cc3, cc4;
+    int rc = autocorr(h->cc1, Nx, Ny, cc3);
+    if (!rc) rc = autocorr(h->cc2, Nz, Nzz, cc4);
+    if (rc) return rc;
+    const double f1 = cc3[0];
+    const double dxyz = (double)h->xyz;
+    std::vector<double> mh(2 * (size_t)h->xyz);
+    for (int i = 0; i < Nx; ++i)
+        for (int j = 0; j < Ny; ++j) {
+            const double c3 = cc3[2 * ((size_t)i * Ny + j)];
+            for (int k = 0; k < Nz; ++k) {
+                const double c4 = cc4[2 * (size_t)k];
+                const double a = c3 * c4 / f1;
+                const double b = (f1 - c3) * (f1 - c4) / (1 - f1);
+                const size_t v = k + (size_t)j * Nz + (size_t)i * Nz * Ny;
+                mh[2 * v] = (a + b) * dxyz;
+                mh[2 * v + 1] = 0;
+            }
+        }
+    MR_CUDA(cudaMemcpyAsync(h->m, mh.data(), mh.size() * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    rc = h->transform(-1, true);  // R = sqrt(sqrt(|MHat|^2))
+    if (rc) return rc;
+    MR_CUDA(cudaMemcpyAsync(h->normC, h->R, (size_t)h->xyz * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+    MR_CUDA(cudaMemcpyAsync(&h->normC0, h->normC, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    MR_CUDA(cudaStreamSynchronize(h->stream));
+    h->norm_set = true;
+    return M3D_OK;
+}
+
+// the modulus the loop targets (xyz doubles)
+int m3drec_get_norm(m3d_rec* h, double* out) {
+    if (!h || !out) return failr(M3D_ERR_ARG, "NULL argument");
+    MR_CUDA(cudaSetDevice(h->device));
+    MR_CUDA(cudaMemcpyAsync(out, h->normC, (size_t)h->xyz * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    MR_CUDA(cudaStreamSynchronize(h->stream));
+    return M3D_OK;
+}
+
+// one unnormalised 3-D complex transform of host arrays on the GPU (sign -1
+// forward, +1 inverse; xyz (re, im) pairs, index z + Nz (y + Ny x))
+int m3drec_fft3(const double* in, double* out, int Nx, int Ny, int Nz, int sign, int device) {
+    if (!in || !out) return failr(M3D_ERR_ARG, "NULL argument");
+    if (sign != -1 && sign != 1) return failr(M3D_ERR_ARG, "sign must be -1 or +1");
+    m3d_rec* t = nullptr;
+    int rc = rec_alloc(Nx, Ny, Nz, device, &t);
+    if (rc) return rc;
+    rc = rec_fft_host(t, in, out, sign);
+    m3drec_destroy(t);
+    return rc;
 }
 
 int m3drec_destroy(m3d_rec* h) {
@@ -910,6 +1178,8 @@ int m3drec_seed(m3d_rec* h, unsigned long long seed) {
 int m3drec_run(m3d_rec* h, int n, double beta) {
     if (!h) return failr(M3D_ERR_ARG, "NULL handle");
     if (n < 0 || n > 10000000) return failr(M3D_ERR_ARG, "n must be in [0, 1e7]");
+    if (!h->norm_set) return failr(M3D_ERR_STATE, "no target modulus (estimate_norm first)");
+    h->last_n = n;
     MR_CUDA(cudaSetDevice(h->device));
     RecCtl c{};
     c.seed = h->seed;
@@ -934,6 +1204,7 @@ int m3drec_run(m3d_rec* h, int n, double beta) {
 // converged or `iters` further passes
 int m3drec_iterate(m3d_rec* h, int iters, double beta) {
     if (!h) return failr(M3D_ERR_ARG, "NULL handle");
+    if (!h->norm_set) return failr(M3D_ERR_STATE, "no target modulus (estimate_norm first)");
     if (!h->started) return failr(M3D_ERR_STATE, "no field yet (run or set_state first)");
     if (iters < 0 || iters > 10000000) return failr(M3D_ERR_ARG, "iters must be in [0, 1e7]");
     MR_CUDA(cudaSetDevice(h->device));
@@ -1034,6 +1305,69 @@ static void shift3(const double* in, double* out, int Nx, int Ny, int Nz, bool i
             for (int z = 0; z < Nz; ++z)
                 out[((size_t)((x + sx) % Nx) * Ny + (y + sy) % Ny) * Nz + (z + sz) % Nz] =
                     in[((size_t)x * Ny + y) * Nz + z];
+}
+
+// saveRecImages :403-432: folder/<i+1>.png for every x slice (pixel (j, k) =
+// 255 m(x = i, y = j, z = k), an Ny x Nz image -- the reference's Nx x Ny image
+// for cubic grids), folder/rve_rec.txt (the field, one value per line) and
+// folder/err.txt ("voloum fraction= " + mean, then the errors of passes
+// 0 .. numloops-2, 0 past the last pass run)
+int m3drec_save_images(m3d_rec* h, const char* folder) {
+    if (!h || !folder) return failr(M3D_ERR_ARG, "NULL argument");
+    std::vector<double> f((size_t)h->xyz);
+    int rc = m3drec_get_field(h, f.data());
+    if (rc) return rc;
+    std::vector<double> e((size_t)std::max(h->last_n, 0), 0.0);
+    int cnt = 0;
+    rc = m3drec_get_error(h, e.data(), (int)e.size(), &cnt);
+    if (rc) return rc;
+    const std::string dir(folder);
+    mkdir(dir.c_str(), 0775);
+    const int Nx = h->Nx, Ny = h->Ny, Nz = h->Nz;
+    std::vector<unsigned char> img((size_t)Ny * Nz);
+    for (int i = 0; i < Nx; ++i) {
+        for (int j = 0; j < Ny; ++j)
+            for (int k = 0; k < Nz; ++k)
+                img[j + (size_t)Ny * k] = (unsigned char)(f[k + (size_t)j * Nz + (size_t)i * Ny * Nz] * 255);
+        if (!write_png_gray(dir + "/" + std::to_string(i + 1) + ".png", Ny, Nz, img.data()))
+            return failr(M3D_ERR_ARG, "cannot write " + dir + "/" + std::to_string(i + 1) + ".png");
+    }
+    std::ofstream op2(dir + "/rve_rec.txt");
+    double sum = 0;
+    for (long long v = 0; v < h->xyz; ++v) {
+        op2 << f[v] << std::endl;
+        sum += f[v];
+    }
+    sum = sum / h->xyz;
+    std::ofstream op1(dir + "/err.txt");
+    op1 << "voloum fraction= " << sum << std::endl;
+    for (int i = 0; i < h->last_n - 1; ++i) op1 << e[i] << std::endl;
+    if (!op1 || !op2) return failr(M3D_ERR_ARG, "cannot write into " + dir);
+    return M3D_OK;
+}
+
+// vtiWriter :435-470: VTK XML image data with two Float64 components per
+// point, (field, tpcf[len]), in flat index order (VTK's x-fastest loop over
+// the reference's flat arrays)
+int m3drec_write_vti(m3d_rec* h, const char* file, const double* tpcf) {
+    if (!h || !file || !tpcf) return failr(M3D_ERR_ARG, "NULL argument");
+    std::vector<double> f((size_t)h->xyz);
+    int rc = m3drec_get_field(h, f.data());
+    if (rc) return rc;
+    std::ofstream o(file);
+    if (!o) return failr(M3D_ERR_ARG, std::string("cannot open ") + file);
+    o << "<?xml version=\"1.0\"?>\n";
+    o << "<VTKFile type=\"ImageData\" version=\"0.1\" byte_order=\"LittleEndian\">\n";
+    o << "  <ImageData WholeExtent=\"0 " << h->Nx - 1 << " 0 " << h->Ny - 1 << " 0 " << h->Nz - 1
+      << "\" Origin=\"0 0 0\" Spacing=\"1 1 1\">\n";
+    o << "    <Piece Extent=\"0 " << h->Nx - 1 << " 0 " << h->Ny - 1 << " 0 " << h->Nz - 1 << "\">\n";
+    o << "      <PointData Scalars=\"ImageScalars\">\n";
+    o << "        <DataArray type=\"Float64\" Name=\"ImageScalars\" NumberOfComponents=\"2\" format=\"ascii\">\n";
+    o.precision(10);
+    for (long long v = 0; v < h->xyz; ++v) o << f[v] << " " << tpcf[v] << "\n";
+    o << "        </DataArray>\n      </PointData>\n      <CellData/>\n    </Piece>\n  </ImageData>\n</VTKFile>\n";
+    if (!o) return failr(M3D_ERR_ARG, std::string("write failed: ") + file);
+    return M3D_OK;
 }
 
 int m3drec_fftshift(const double* in, double* out, int Nx, int Ny, int Nz) {

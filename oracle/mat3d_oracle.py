@@ -800,6 +800,39 @@ class RecOracle:
         self.fft = fft or (lambda a, sign: (np.fft.fftn(a.reshape(sh)) if sign < 0 else
                                             np.fft.ifftn(a.reshape(sh), norm="forward")).ravel())
 
+    @classmethod
+    def from_sections(cls, c1, c2, fft=None, fft2=None):
+        """recPlan(CImg c1, CImg c2) (:145-206) + estimateNormFFT_RVE (:245-281).
+        c1, c2: 8-bit images indexed [y, x]; grid width1 x height1 x height2.
+        `fft2(a, (n0, n1), sign)` is the unnormalised 2-D complex transform."""
+        c1 = np.asarray(c1).astype(np.int64)
+        c2 = np.asarray(c2).astype(np.int64)
+        (Ny, Nx), (Nz, Nzz) = c1.shape, c2.shape
+        # CC1[k + j*Ny] = (int)C1(j, k) / Max, over j < Nx, k < Ny for both sections
+        cc1 = (c1.T // c1.max()).ravel().astype(np.float64)
+        cc2 = (c2[:Ny, :Nx].T // c2[:Ny, :Nx].max()).ravel().astype(np.float64)
+        f2 = fft2 or (lambda a, sh, sign: (np.fft.fft2(a.reshape(sh)) if sign < 0 else
+                                          np.fft.ifft2(a.reshape(sh), norm="forward")).ravel())
+
+        def autocorr(cc, sh):
+            sp = f2(cc.astype(np.complex128), sh, -1)
+            v = sh[0] * sh[1] * sh[0] * sh[1]  # int arithmetic in the reference: wraps past 2^31
+            den = float((v + 2 ** 31) % 2 ** 32 - 2 ** 31)
+            p = (sp.real * sp.real + sp.imag * sp.imag) / den
+            return f2(p.astype(np.complex128), sh, +1)
+
+        cc3 = autocorr(cc1, (Nx, Ny))
+        cc4 = autocorr(cc2, (Nz, Nzz))
+        xyz = Nx * Ny * Nz
+        f1 = cc3[0].real
+        c3 = cc3.real.reshape(Nx, Ny)[:, :, None]
+        c4 = cc4.real[:Nz][None, None, :]
+        mh = ((c3 * c4 / f1 + (f1 - c3) * (f1 - c4) / (1 - f1)) * xyz).ravel()
+        o = cls(np.zeros(xyz), Nx, Ny, Nz, fft=fft)
+        MH = o.fft(mh.astype(np.complex128), -1)
+        o.normC = np.sqrt(np.sqrt(MH.real * MH.real + MH.imag * MH.imag))
+        return o
+
     def error(self, MT):
         """funcNormC (include/reconstruction.hpp:37-44): mean |(|MTilda| - normC)|, summed in voxel order."""
         a = np.abs(np.sqrt(MT.real * MT.real + MT.imag * MT.imag) - self.normC)

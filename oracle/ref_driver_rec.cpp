@@ -8,11 +8,37 @@
 // reference's draws come from std::rand, which is implementation defined), so
 // the random initial field and restarts can be reproduced exactly elsewhere.
 
+#include <unistd.h>
+
 #include <cstdint>
+#include <cstdio>
+#include <fstream>
 #include <iostream>
 #include <streambuf>
 
+// Everything reconstruction.hpp includes, first, so that the access override
+// below reaches only the recPlan class (the section pin reads its private
+// normC after estimateNormFFT_RVE).  M3D_REF_CIMG is the reference's own
+// vendored CImg.h, the file reconstruction.hpp includes by a quoted path.
+#include <eigen/Eigen/Dense>
+#include "fftw3.h"
+#include M3D_REF_CIMG
+#include "omp.h"
+#include <vtkActor.h>
+#include <vtkImageData.h>
+#include <vtkImageDataGeometryFilter.h>
+#include <vtkPolyDataMapper.h>
+#include <vtkProperty.h>
+#include <vtkRenderWindow.h>
+#include <vtkRenderWindowInteractor.h>
+#include <vtkRenderer.h>
+#include <vtkSmartPointer.h>
+#include <vtkVersion.h>
+#include <vtkXMLImageDataReader.h>
+#include <vtkXMLImageDataWriter.h>
+#define private public
 #include "reconstruction.hpp"
+#undef private
 
 namespace {
 struct NullBuf : std::streambuf {
@@ -46,6 +72,30 @@ int ref_rec_run(int Nx, int Ny, int Nz, const double* tpcf, int n, double beta, 
         if (err_out[i] != 0) cnt = i + 1;
     }
     return cnt;
+}
+
+// recPlan(CImg c1, CImg c2) (:145-206) from 8-bit sections stored x fastest,
+// then estimateNormFFT_RVE() (:245-281); normC out (xyz = w1 * h1 * h2).
+// estimateNormFFT_RVE writes normc.txt into the working directory; it runs in
+// a scratch directory that is removed afterwards.
+int ref_rec_sections(const unsigned char* c1, int w1, int h1, const unsigned char* c2, int w2, int h2,
+                     double* normC_out) {
+    Quiet q;
+    cimg_library::CImg<unsigned char> C1(c1, w1, h1, 1, 1), C2(c2, w2, h2, 1, 1);
+    recon::recPlan a(C1, C2);
+    char cwd[4096];
+    if (!getcwd(cwd, sizeof(cwd))) return 1;
+    char tmpl[] = "/tmp/m3d_refrec_XXXXXX";
+    if (!mkdtemp(tmpl)) return 2;
+    if (chdir(tmpl) != 0) return 3;
+    a.estimateNormFFT_RVE();
+    if (chdir(cwd) != 0) return 4;
+    std::string f = std::string(tmpl) + "/normc.txt";
+    std::remove(f.c_str());
+    rmdir(tmpl);
+    const size_t xyz = (size_t)a.Nx * a.Ny * a.Nz;
+    for (size_t s = 0; s < xyz; ++s) normC_out[s] = a.normC[s];
+    return 0;
 }
 
 // one 3-D complex transform through the same stand-in FFTW plan type the

@@ -152,3 +152,15 @@ class RefLib:
         out = np.zeros_like(x)
         self.L.ref_fft3(ctypes.c_void_p(x.ctypes.data), ctypes.c_void_p(out.ctypes.data), Nx, Ny, Nz, sign)
         return out
+
+    def rec_sections(self, c1, c2):
+        """recPlan(CImg c1, CImg c2) + estimateNormFFT_RVE(): normC.  c1, c2:
+        uint8 images indexed [y, x] (height x width)."""
+        a1, a2 = (np.ascontiguousarray(np.asarray(c, np.uint8)) for c in (c1, c2))
+        (h1, w1), (h2, w2) = a1.shape, a2.shape
+        out = np.zeros(w1 * h1 * h2)
+        self.L.ref_rec_sections.restype = ctypes.c_int
+        rc = self.L.ref_rec_sections(ctypes.c_void_p(a1.ctypes.data), w1, h1, ctypes.c_void_p(a2.ctypes.data), w2, h2,
+                                     _p(out))
+        assert rc == 0, rc
+        return out

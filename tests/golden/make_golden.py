@@ -111,6 +111,19 @@ def main():
         r = ref.rec_run(shape, T, n, beta, seed)
         np.savez_compressed(os.path.join(HERE, f"rec_{Nx}x{Ny}x{Nz}.npz"), shape=shape, tpcf=T, seed=seed, n=n,
                             beta=beta, err=r["err"], rve=r["rve"], iterations=r["iterations"])
+    # the cut-section constructor + estimateNormFFT_RVE: seeded 8-bit sections
+    # (discs at 200, scattered pixels at 90, which the reference's integer
+    # division by the maximum maps to 0), square and non-square
+    rng = np.random.default_rng(7)
+    for (h, w) in ((12, 12), (9, 11)):
+        img = np.zeros((h, w), np.uint8)
+        yy, xx = np.mgrid[0:h, 0:w]
+        for _ in range(4):
+            cy, cx, rr = rng.uniform(0, h), rng.uniform(0, w), rng.uniform(1.5, 3)
+            img[(yy - cy) ** 2 + (xx - cx) ** 2 <= rr * rr] = 200
+        img[rng.random((h, w)) < 0.05] = 90
+        np.savez_compressed(os.path.join(HERE, f"rec_sections_{w}x{h}.npz"), c1=img, c2=img,
+                            normC=ref.rec_sections(img, img))
     print("fixtures written to", HERE)
 
 

@@ -227,3 +227,102 @@ def test_errors():
     with pytest.raises(m3d.M3DError):
         r.set_state(np.zeros(512, np.complex128), 0, 300, 0)
     r.close()
+
+
+# ---- cut-section constructor, one-shot transform, writers -------------------
+@pytest.mark.parametrize("name", ["rec_sections_12x12", "rec_sections_11x9"])
+def test_sections_norm_vs_reference_fixture(name):
+    """recPlan(CImg, CImg) + estimateNormFFT_RVE: normC against the
+    reference's (fixture) within 1e-7 of its maximum, as the numpy
+    restatement; then a short run against the restatement."""
+    g = load(name)
+    r = m3d.Reconstruction(None, sections=(g["c1"], g["c2"]))
+    with pytest.raises(m3d.M3DError):
+        r.run(3, 0.8)  # no target modulus before the estimate
+    r.estimate_norm()
+    nc = r.norm()
+    assert np.abs(nc - g["normC"]).max() / g["normC"].max() < 1e-7
+    h, w = g["c1"].shape
+    shape = (w, h, h)
+    assert (r.Nx, r.Ny, r.Nz) == shape
+    r.seed(4)
+    r.run(6, 0.8)
+    o = O.RecOracle(np.zeros(r.xyz), *shape)
+    o.normC = nc.copy()  # the same target, so the loop itself is compared
+    o.runRec(6, 0.8, 4)
+    assert np.abs(r.errors() - o.err).max() / o.err[0] < 1e-8
+    r.close()
+
+
+def test_sections_errors():
+    a = np.zeros((8, 8), np.uint8)
+    a[2:5, 2:5] = 255
+    with pytest.raises(m3d.M3DError):
+        m3d.Reconstruction(None, sections=(a, np.zeros((8, 8), np.uint8)))  # all-zero section
+    with pytest.raises(m3d.M3DError):
+        m3d.Reconstruction(None, sections=(a, a[:, :6]))  # sizes differ
+
+
+@pytest.mark.parametrize("shape", [(9, 10, 11), (171, 1, 1), (16, 16, 16)])
+def test_fft3_vs_numpy(shape):
+    rng = np.random.default_rng(1)
+    a = rng.standard_normal(int(np.prod(shape))) + 1j * rng.standard_normal(int(np.prod(shape)))
+    f = m3d.fft3(a, shape, -1)
+    want = np.fft.fftn(a.reshape(shape)).ravel()
+    assert np.abs(f - want).max() / np.abs(want).max() < 1e-13
+    b = m3d.fft3(f, shape, +1)
+    assert np.abs(b / a.size - a).max() < 1e-13
+
+
+def _png_pixels(path):
+    import struct
+    import zlib
+    data = open(path, "rb").read()
+    assert data[:8] == b"\x89PNG\r\n\x1a\n"
+    pos, idat = 8, b""
+    w = h = None
+    while pos < len(data):
+        n, = struct.unpack(">I", data[pos:pos + 4])
+        typ, body = data[pos + 4:pos + 8], data[pos + 8:pos + 8 + n]
+        crc, = struct.unpack(">I", data[pos + 8 + n:pos + 12 + n])
+        assert crc == zlib.crc32(typ + body) & 0xFFFFFFFF
+        if typ == b"IHDR":
+            w, h, depth, ctype = struct.unpack(">IIBB", body[:10])
+            assert depth == 8 and ctype == 0
+        elif typ == b"IDAT":
+            idat += body
+        pos += 12 + n
+    raw = zlib.decompress(idat)
+    rows = [raw[y * (w + 1):(y + 1) * (w + 1)] for y in range(h)]
+    assert all(r[0] == 0 for r in rows)
+    return np.array([list(r[1:]) for r in rows], np.uint8)  # [y, x]
+
+
+def test_writers(tmp_path):
+    """saveRecImages (PNG slices, rve_rec.txt, err.txt) and vtiWriter."""
+    shape = (9, 10, 11)
+    T = example_tpcf(shape)
+    a = m3d.recPlan(T, *shape, seed=3)
+    a.runRec(12, 0.8)
+    f = a.mTilda
+    folder = tmp_path / "ar1"
+    a.saveRecImages(str(folder))
+    Nx, Ny, Nz = shape
+    F = f.reshape(shape)
+    for i in range(Nx):
+        px = _png_pixels(folder / f"{i + 1}.png")  # [y = k, x = j]
+        assert px.shape == (Nz, Ny)
+        assert np.array_equal(px.T, (F[i] * 255).astype(np.uint8))
+    vals = np.loadtxt(folder / "rve_rec.txt")
+    assert np.array_equal(vals, f)
+    lines = open(folder / "err.txt").read().splitlines()
+    assert lines[0] == f"voloum fraction= {f.mean():.6g}"
+    e = np.array([float(x) for x in lines[1:]])
+    assert e.size == 11 and np.allclose(e, a.trackrealerrorA[:11], rtol=1e-5)
+    a.vtiWriter(str(folder / "rec.vti"), T)
+    txt = open(folder / "rec.vti").read()
+    assert 'WholeExtent="0 8 0 9 0 10"' in txt and 'NumberOfComponents="2"' in txt
+    body = txt.split('format="ascii">')[1].split("</DataArray>")[0]
+    arr = np.array(body.split(), float).reshape(-1, 2)
+    assert np.array_equal(arr[:, 0], f) and np.allclose(arr[:, 1], T, rtol=1e-9, atol=1e-12)
+    a.close()

@@ -114,3 +114,28 @@ def test_threshold_walk():
     field = (np.arange(xyz) + 0.5) / xyz  # uniform in (0, 1): 30 % ones needs a cut near 0.7
     b = o.threshold(field)
     assert abs(b.mean() - 0.3) < 1e-4 or abs(b.mean() - 0.3) <= 0.0015
+
+
+SECTIONS = ["rec_sections_12x12", "rec_sections_11x9"]
+
+
+@pytest.mark.parametrize("name", SECTIONS)
+def test_sections_golden_numpy(name):
+    """recPlan(CImg, CImg) + estimateNormFFT_RVE restated with numpy's FFT:
+    normC within 1e-7 of its maximum (sqrt(sqrt(|M|)) magnifies the rounding of
+    the near-zero coefficients)."""
+    g = load(name)
+    o = O.RecOracle.from_sections(g["c1"], g["c2"])
+    assert np.abs(o.normC - g["normC"]).max() / g["normC"].max() < 1e-7
+
+
+@have_ref
+@pytest.mark.parametrize("name", SECTIONS)
+def test_sections_bit_exact_on_reference_transform(name):
+    g = load(name)
+    R = ref_lib.RefLib()
+    h, w = g["c1"].shape
+    o = O.RecOracle.from_sections(g["c1"], g["c2"], fft=lambda a, sg: R.fft3(a, (w, h, h), sg),
+                                  fft2=lambda a, sh, sg: R.fft3(a, (sh[0], sh[1], 1), sg))
+    assert np.array_equal(o.normC, g["normC"])
+    assert np.array_equal(R.rec_sections(g["c1"], g["c2"]), g["normC"])
