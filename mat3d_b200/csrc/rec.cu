@@ -67,13 +67,25 @@ int failr(int code, const std::string& msg) {
     return code;
 }
 
-#define MR_CUDA(call)                                                                \
-    do {                                                                             \
-        cudaError_t e_ = (call);                                                     \
-        if (e_ != cudaSuccess) return failr(M3D_ERR_CUDA, cudaGetErrorString(e_)); \
+#define MR_CUDA(call)                                                                             \
+    do {                                                                                          \
+        cudaError_t e_ = (call);                                                                  \
+        if (e_ != cudaSuccess) return failr(M3D_ERR_CUDA, std::string(cudaGetErrorString(e_)) + " (" #call ")"); \
     } while (0)
 
 constexpr int kThreads = 128;
+
+// The dynamic shared-memory limit is an attribute of the kernel, shared by
+// every handle: raise it once to the device maximum (227 KB less the static
+// shared memory) rather than to one handle's need, which would lower it under
+// a larger handle made earlier.
+template <class K>
+void allow_smem(K kernel) {
+    cudaFuncAttributes a;
+    if (cudaFuncGetAttributes(&a, kernel) == cudaSuccess)
+        cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024 - (int)a.sharedSizeBytes);
+    (void)cudaGetLastError();
+}
 constexpr int kRestartPeriod = 150;  // remainder(i + 1, 150) == 0 (:320)
 
 struct RecCtl {
@@ -629,10 +641,17 @@ struct m3d_rec {
     template <int MaxR>
     int transform_t(int sign, bool out_norm) {
         const int nbz = (int)((zlines + G - 1) / G);
+        auto check = [&](const char* what) -> int {
+            const cudaError_t e = cudaGetLastError();
+            return e == cudaSuccess ? M3D_OK : failr(M3D_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+        };
+        if (int rc = check("before the transform")) return rc;
         if (sign < 0) krec_z<Z_FWD, MaxR><<<grid_z, kThreads, z_smem(), stream>>>(A, m, twz, pz, G, zlines, nbz, d_ctl);
         else krec_z<Z_BWD, MaxR><<<grid_z, kThreads, z_smem(), stream>>>(A, m, twz, pz, G, zlines, nbz, d_ctl);
+        if (int rc = check("z pass")) return rc;
         if (sign < 0) krec_y<Y_FWD, MaxR><<<grid_y, kThreads, y_smem(), stream>>>(A, twy, py, Nz, TZ, ntz, nb_y, d_ctl);
         else krec_y<Y_INV, MaxR><<<grid_y, kThreads, y_smem(), stream>>>(A, twy, py, Nz, TZ, ntz, nb_y, d_ctl);
+        if (int rc = check("y pass")) return rc;
         if (out_norm)
             krec_xout<XO_NORM, MaxR><<<grid_xr, kThreads, xr_smem(), stream>>>(A, R, twx, px, Ny, Nz, TZ, ntz, nb_x, sign, d_ctl);
         else
@@ -656,17 +675,17 @@ struct m3d_rec {
     template <int MaxR>
     void set_smem_t() {
         const int zs = (int)z_smem(), ys = (int)y_smem(), xs = (int)x_smem();
-        cudaFuncSetAttribute(krec_z<Z_FWD, MaxR>, cudaFuncAttributeMaxDynamicSharedMemorySize, zs);
-        cudaFuncSetAttribute(krec_z<Z_RAND, MaxR>, cudaFuncAttributeMaxDynamicSharedMemorySize, zs);
-        cudaFuncSetAttribute(krec_z<Z_INV, MaxR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)zi_smem());
-        cudaFuncSetAttribute(krec_y<Y_FWD, MaxR>, cudaFuncAttributeMaxDynamicSharedMemorySize, ys);
-        cudaFuncSetAttribute(krec_y<Y_RAND, MaxR>, cudaFuncAttributeMaxDynamicSharedMemorySize, ys);
-        cudaFuncSetAttribute(krec_y<Y_INV, MaxR>, cudaFuncAttributeMaxDynamicSharedMemorySize, ys);
-        cudaFuncSetAttribute(krec_xout<XO_ANGLE, MaxR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)xr_smem());
-        cudaFuncSetAttribute(krec_xout<XO_COPY, MaxR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)xr_smem());
-        cudaFuncSetAttribute(krec_xout<XO_NORM, MaxR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)xr_smem());
-        cudaFuncSetAttribute(krec_z<Z_BWD, MaxR>, cudaFuncAttributeMaxDynamicSharedMemorySize, zs);
-        cudaFuncSetAttribute(krec_xturn<MaxR>, cudaFuncAttributeMaxDynamicSharedMemorySize, xs);
+        allow_smem(krec_z<Z_FWD, MaxR>);
+        allow_smem(krec_z<Z_RAND, MaxR>);
+        allow_smem(krec_z<Z_INV, MaxR>);
+        allow_smem(krec_y<Y_FWD, MaxR>);
+        allow_smem(krec_y<Y_RAND, MaxR>);
+        allow_smem(krec_y<Y_INV, MaxR>);
+        allow_smem(krec_xout<XO_ANGLE, MaxR>);
+        allow_smem(krec_xout<XO_COPY, MaxR>);
+        allow_smem(krec_xout<XO_NORM, MaxR>);
+        allow_smem(krec_z<Z_BWD, MaxR>);
+        allow_smem(krec_xturn<MaxR>);
         int sms = 0;
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
         sms = std::max(1, sms);

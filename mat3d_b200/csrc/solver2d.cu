@@ -299,10 +299,13 @@ int m3d2d_create(int Nx, int Ny, m3d_solver2d** out) {
     cudaMemcpy(h->twy, ty.data(), Ny * sizeof(double2), cudaMemcpyHostToDevice);
     cudaMemset(h->eps, 0, f);
     cudaMemset(h->sig, 0, f);
-    if (h->rows_smem() > 48 * 1024)
-        cudaFuncSetAttribute(k2d_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->rows_smem());
-    if (h->cols_smem() > 48 * 1024)
-        cudaFuncSetAttribute(k2d_cols, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->cols_smem());
+// one limit per kernel for every handle (a per-handle value would lower it
+    // under a larger handle made earlier): the device maximum
+    for (const void* k : {(const void*)k2d_rows, (const void*)k2d_cols}) {
+        cudaFuncAttributes a;
+        if (cudaFuncGetAttributes(&a, k) == cudaSuccess)
+            cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024 - (int)a.sharedSizeBytes);
+    }
     (void)cudaGetLastError();
     *out = h;
     return M3D_OK;

@@ -91,3 +91,25 @@ def test_2d_errors():
     with pytest.raises(m3d.M3DError):
         s.run(25)  # no material / load yet
     s.close()
+
+
+def test_handles_of_different_sizes_coexist():
+    """A smaller handle made after a larger one must not lower the larger
+    one's shared-memory launch limit (both above the 48 KB default here)."""
+    big = m3d.Solver2D(1024, 1024)
+    rve = np.ones(1024 * 1024, np.int32)
+    rve[: 1024 * 300] = 0
+    big.material([68.9e9, 0.35, 400e9, 0.23], rve)
+    big.set_load(np.array([0, 0, 0.005], np.complex128))
+    big.run(2)
+    e1, _ = big.fields()
+    small = m3d.Solver2D(512, 512)
+    small.material([68.9e9, 0.35, 400e9, 0.23], np.ones(512 * 512, np.int32))
+    small.set_load(np.array([0, 0, 0.005], np.complex128))
+    small.run(2)
+    big.set_load(np.array([0, 0, 0.005], np.complex128))
+    big.run(2)
+    e2, _ = big.fields()
+    assert np.array_equal(e1, e2)
+    small.close()
+    big.close()

@@ -326,3 +326,21 @@ def test_writers(tmp_path):
     arr = np.array(body.split(), float).reshape(-1, 2)
     assert np.array_equal(arr[:, 0], f) and np.allclose(arr[:, 1], T, rtol=1e-9, atol=1e-12)
     a.close()
+
+
+def test_handles_of_different_sizes_coexist():
+    """A small handle made after a large one must not lower the large one's
+    shared-memory launch limit (the limit is a property of the kernel)."""
+    big_shape = (96, 96, 96)  # 99 KB of dynamic shared memory in the x turnaround
+    T = example_tpcf(big_shape)
+    big = m3d.Reconstruction(T, *big_shape)
+    big.seed(1)
+    big.run(2, 0.8)
+    e1 = big.errors()
+    small = m3d.Reconstruction(example_tpcf((4, 4, 4)), 4, 4, 4)
+    small.seed(1)
+    small.run(2, 0.8)
+    big.run(2, 0.8)
+    assert np.array_equal(big.errors(), e1)
+    small.close()
+    big.close()
