@@ -24,7 +24,7 @@ NVCC_FLAGS = [
 
 SOURCES = [os.path.join(CSRC, "solver.cu"), os.path.join(CSRC, "noalloc.cu"), os.path.join(CSRC, "compat.cpp"),
            os.path.join(CSRC, "batch.cpp"), os.path.join(CSRC, "serve.cpp"),
-           os.path.join(CSRC, "solver2d.cu"), os.path.join(CSRC, "rec.cu")]
+           os.path.join(CSRC, "solver2d.cu"), os.path.join(CSRC, "rec.cu"), os.path.join(CSRC, "rec_compat.cpp")]
 DEPS = SOURCES + [os.path.join(CSRC, f) for f in os.listdir(CSRC)] + [
     os.path.join(ROOT, "include", f) for f in os.listdir(os.path.join(ROOT, "include"))]
 

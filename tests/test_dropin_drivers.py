@@ -111,3 +111,35 @@ def test_thermal_example_driver_homogenization(tmp_path):
     KH, _ = o.homogenization(1e-9, 1e-9)
     assert np.abs(K - KH).max() / np.abs(KH).max() < 1e-5
     assert re.search(r"Mori-Tanaka", rep)
+
+
+def test_reconstruction_example_driver(tmp_path):
+    """example/reconst3d/main.cpp unchanged: the 171^3 isotropic TPCF, its
+    shift and transform through the header's FFTW subset (GPU), recPlan +
+    runRec(100, 0.8), saveRecImages("ar1") and vtiWriter("ar1/rec.vti", tpcf)."""
+    exe = need("reconst3d_example")
+    r = subprocess.run([exe], cwd=tmp_path, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    N = 171
+    d = os.path.join(tmp_path, "ar1")
+    assert all(os.path.exists(os.path.join(d, f"{i + 1}.png")) for i in range(N))
+    lines = open(os.path.join(d, "err.txt")).read().splitlines()
+    assert lines[0].startswith("voloum fraction= ")
+    vf = float(lines[0].split("=")[1])
+    assert abs(vf - 0.5) < 0.01  # the walk's target normC[0] / xyz = phi1 = 0.5 of the example's TPCF
+    errs = np.array([float(x) for x in lines[1:]])
+    assert errs.size == 99 and np.all(errs > 0) and errs[-1] < errs[0]
+    with open(os.path.join(d, "rve_rec.txt"), "rb") as f:
+        body = f.read()
+    vals = np.array(body.split(), float)
+    assert vals.size == N ** 3 and set(np.unique(vals)) <= {0.0, 1.0}
+    assert abs(vals.mean() - vf) < 1e-5
+    # the vti: 2 components (field, the centred TPCF), flat order
+    with open(os.path.join(d, "rec.vti")) as f:
+        head = [next(f) for _ in range(8)]
+        first = [next(f) for _ in range(3)]
+    assert 'NumberOfComponents="2"' in "".join(head) and 'WholeExtent="0 170 0 170 0 170"' in "".join(head)
+    t = O.tpcf_isotropic(N, 25.0, 0.4, 0.5)
+    for k, ln in enumerate(first):
+        a, b = (float(x) for x in ln.split())
+        assert a == vals[k] and abs(b - t[k]) < 1e-9
