@@ -136,7 +136,11 @@ def test_reconstruction_example_driver(tmp_path):
     assert abs(vals.mean() - vf) < 1e-5
     # the vti: 2 components (field, the centred TPCF), flat order
     with open(os.path.join(d, "rec.vti")) as f:
-        head = [next(f) for _ in range(8)]
+        head = []
+        for ln in f:
+            head.append(ln)
+            if "<DataArray" in ln:
+                break
         first = [next(f) for _ in range(3)]
     assert 'NumberOfComponents="2"' in "".join(head) and 'WholeExtent="0 170 0 170 0 170"' in "".join(head)
     t = O.tpcf_isotropic(N, 25.0, 0.4, 0.5)
