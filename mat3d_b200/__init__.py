@@ -302,11 +302,20 @@ class Solver:
             Ce, Se, ep, sg = Ce[0], Se[0], ep[0], sg[0]
         return Ce, Se, ep, sg, rc
 
-    def field(self, which=FIELD_STRAIN, b=0):
+    def field(self, which=FIELD_STRAIN, b=0, out=None):
+        """The field as a (C, V) view of voxel-major (AoS) data, or (V,) for
+        scalar fields.  ``out``: a caller-owned contiguous float64 buffer of
+        V*C (or V) elements to write into (e.g. pinned host memory, so the
+        device-to-host copy runs at full speed with no extra host copy)."""
         scalar = which in (FIELD_EPS_P, FIELD_DAMAGE)
-        out = np.zeros(self.V if scalar else self.V * self.C)
+        n = self.V if scalar else self.V * self.C
+        if out is None:
+            out = np.empty(n)
+        elif out.dtype != np.float64 or out.size != n or not out.flags.c_contiguous:
+            raise ValueError(f"out must be a contiguous float64 array of {n} elements")
         _check(self.L, self.L.m3d_get_field(self.h, which, b, _ptr(out)), "get_field")
-        return out if scalar else out.reshape(self.V, self.C).T  # (C, V) view of AoS data
+        flat = out.reshape(-1)
+        return flat if scalar else flat.reshape(self.V, self.C).T  # (C, V) view of AoS data
 
     def means(self, b=0):
         e = np.zeros(self.C)

@@ -80,3 +80,21 @@ def test_graph_reused_across_runs_and_iteration_cap():
     assert rc == m3d.NOT_CONVERGED
     assert s.stats()["iters"] == 7
     s.close()
+
+
+def test_field_into_caller_buffer():
+    """Solver.field(out=...) writes the voxel-major field into a caller-owned
+    buffer (pinned here) and equals the allocating form."""
+    import torch
+    shape = (16, 16, 16)
+    s = m3d.Solver(m3d.KIND_THERMAL, *shape, 0, "fp64", 1)
+    s.set_material_thermal(1.0, 20.0, sphere_rve(shape, 5.0))
+    s.set_load(np.array([0, 0, 1.0]))
+    s.run(1e-9, 0, 1, m3d.CRIT_RESIDUAL)
+    want = s.field(m3d.FIELD_STRAIN)
+    buf = torch.empty(3 * 16 ** 3, dtype=torch.float64).pin_memory().numpy()
+    got = s.field(m3d.FIELD_STRAIN, out=buf)
+    assert np.array_equal(got, want) and np.shares_memory(got, buf)
+    with pytest.raises(ValueError):
+        s.field(m3d.FIELD_STRAIN, out=np.empty(10))
+    s.close()
