@@ -577,6 +577,7 @@ struct m3d_rec {
     int G = 1, TZ = 1, ntz = 1;
     long long zlines = 0;
     int nb_y = 0, nb_x = 0;
+    int TZX = 1, ntzx = 1;  // column tile of the x passes (they also stage normC)
     int grid_y = 1, grid_z = 1, grid_zi = 1, grid_x = 1, grid_xr = 1;  // persistent CTAs per pass
     double normC0 = 0;
     unsigned long long seed = 1;
@@ -608,8 +609,8 @@ struct m3d_rec {
     size_t z_smem() const { return (size_t)Nz * 16 + 3 * (size_t)G * Nz * 16; }
     size_t zi_smem() const { return z_smem() + 2 * (size_t)G * Nz * 8; }
     size_t y_smem() const { return (size_t)Ny * 16 + 3 * (size_t)Ny * TZ * 16; }
-    size_t x_smem() const { return (size_t)Nx * 16 + 3 * (size_t)Nx * TZ * 16 + 2 * (size_t)Nx * TZ * 8; }
-    size_t xr_smem() const { return (size_t)Nx * 16 + 3 * (size_t)Nx * TZ * 16; }
+    size_t x_smem() const { return (size_t)Nx * 16 + 3 * (size_t)Nx * TZX * 16 + 2 * (size_t)Nx * TZX * 8; }
+    size_t xr_smem() const { return (size_t)Nx * 16 + 3 * (size_t)Nx * TZX * 16; }
     int grid1d() const { return (int)std::min<long long>(148 * 8, (xyz + kThreads - 1) / kThreads); }
 
     // the kernels of one pass, in order; `prof` brackets each with events
@@ -620,13 +621,13 @@ struct m3d_rec {
         mark(0);
         krec_z<Z_RAND, MaxR><<<grid_z, kThreads, z_smem(), stream>>>(A, m, twz, pz, G, zlines, nbz, d_ctl);
         krec_y<Y_RAND, MaxR><<<grid_y, kThreads, y_smem(), stream>>>(A, twy, py, Nz, TZ, ntz, nb_y, d_ctl);
-        krec_xout<XO_ANGLE, MaxR><<<grid_xr, kThreads, xr_smem(), stream>>>(A, R, twx, px, Ny, Nz, TZ, ntz, nb_x, -1, d_ctl);
+        krec_xout<XO_ANGLE, MaxR><<<grid_xr, kThreads, xr_smem(), stream>>>(A, R, twx, px, Ny, Nz, TZX, ntzx, nb_x, -1, d_ctl);
         mark(1);
         krec_z<Z_FWD, MaxR><<<grid_z, kThreads, z_smem(), stream>>>(A, m, twz, pz, G, zlines, nbz, d_ctl);
         mark(2);
         krec_y<Y_FWD, MaxR><<<grid_y, kThreads, y_smem(), stream>>>(A, twy, py, Nz, TZ, ntz, nb_y, d_ctl);
         mark(3);
-        krec_xturn<MaxR><<<grid_x, kThreads, x_smem(), stream>>>(A, normC, R, twx, px, Ny, Nz, TZ, ntz, nb_x, part, errs, d_ctl);
+        krec_xturn<MaxR><<<grid_x, kThreads, x_smem(), stream>>>(A, normC, R, twx, px, Ny, Nz, TZX, ntzx, nb_x, part, errs, d_ctl);
         mark(4);
         krec_y<Y_INV, MaxR><<<grid_y, kThreads, y_smem(), stream>>>(A, twy, py, Nz, TZ, ntz, nb_y, d_ctl);
         mark(5);
@@ -653,9 +654,9 @@ struct m3d_rec {
         else krec_y<Y_INV, MaxR><<<grid_y, kThreads, y_smem(), stream>>>(A, twy, py, Nz, TZ, ntz, nb_y, d_ctl);
         if (int rc = check("y pass")) return rc;
         if (out_norm)
-            krec_xout<XO_NORM, MaxR><<<grid_xr, kThreads, xr_smem(), stream>>>(A, R, twx, px, Ny, Nz, TZ, ntz, nb_x, sign, d_ctl);
+            krec_xout<XO_NORM, MaxR><<<grid_xr, kThreads, xr_smem(), stream>>>(A, R, twx, px, Ny, Nz, TZX, ntzx, nb_x, sign, d_ctl);
         else
-            krec_xout<XO_COPY, MaxR><<<grid_xr, kThreads, xr_smem(), stream>>>(A, R, twx, px, Ny, Nz, TZ, ntz, nb_x, sign, d_ctl);
+            krec_xout<XO_COPY, MaxR><<<grid_xr, kThreads, xr_smem(), stream>>>(A, R, twx, px, Ny, Nz, TZX, ntzx, nb_x, sign, d_ctl);
         launches += 3;
         MR_CUDA(cudaGetLastError());
         return M3D_OK;
@@ -915,7 +916,11 @@ static int rec_alloc(int Nx, int Ny, int Nz, int device, m3d_rec** out) {
     h->ntz = (Nz + h->TZ - 1) / h->TZ;
     h->zlines = (long long)Nx * Ny;
     h->nb_y = Nx * h->ntz;
-    h->nb_x = Ny * h->ntz;
+    // the x turnaround also double-buffers normC: a narrower tile, so that
+    // three CTAs still share an SM (227 KB)
+    h->TZX = std::max(1, std::min(h->TZ, (int)((75 * 1024 - 16 * (size_t)Nx) / (64 * (size_t)Nx))));
+    h->ntzx = (Nz + h->TZX - 1) / h->TZX;
+    h->nb_x = Ny * h->ntzx;
     if (h->zi_smem() > 220 * 1024 || h->y_smem() > 220 * 1024 || h->x_smem() > 220 * 1024) {
         delete h;
         return failr(M3D_ERR_UNSUPPORTED, "grid too large for the shared-memory line FFTs");
