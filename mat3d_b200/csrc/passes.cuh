@@ -81,18 +81,27 @@ struct FinNone {
     __device__ __forceinline__ void run(Ctl*, const double*, int, int, int, double*, double*) const {}
 };
 
+// completion-counter increment with acquire-release semantics at GPU scope:
+// the block's earlier writes (ordered before it by the preceding barrier) are
+// released with it, and the last arriver acquires every other block's
+__device__ __forceinline__ int atomic_add_acq_rel_gpu(int* p, int v) {
+    int old;
+    asm volatile("atom.acq_rel.gpu.global.add.s32 %0, [%1], %2;\n" : "=r"(old) : "l"(p), "r"(v) : "memory");
+    return old;
+}
+
 // The last block of a pass (per batch entry) to finish runs the finalize on
-// all blocks' partials: threadfence + completion counter, the counter reset
-// by that block for the next launch.  All threads of the block must call it.
+// all blocks' partials: barrier + one acquire-release completion counter
+// (rather than a fence in every thread), the counter reset by that block for
+// the next launch.  All threads of the block must call it.
 template <class Fin>
 __device__ __forceinline__ void fused_finalize(const Fin& fin, Ctl* ctl, const double* partials, int NS, int b) {
     if (fin.counter == nullptr) return;
     __shared__ int last;
     __shared__ double red[256];
     __shared__ double tot[16];
-    __threadfence();
     __syncthreads();
-    if (threadIdx.x == 0) last = (atomicAdd(&fin.counter[b], 1) == (int)gridDim.x - 1);
+    if (threadIdx.x == 0) last = (atomic_add_acq_rel_gpu(&fin.counter[b], 1) == (int)gridDim.x - 1);
     __syncthreads();
     if (!last) return;
     __threadfence();
