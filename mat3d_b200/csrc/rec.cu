@@ -135,6 +135,7 @@ __device__ __forceinline__ void cp_async8(void* sdst, const void* gsrc, bool val
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_group1() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
 
 enum ZMode { Z_FWD = 0, Z_RAND = 1, Z_INV = 2, Z_BWD = 3 };
 
@@ -159,16 +160,14 @@ __global__ void __launch_bounds__(kThreads) krec_z(double2* __restrict__ A, doub
     B[0] = tw + Nz;
     B[1] = B[0] + tsz;
     B[2] = B[1] + tsz;
-    double* MB[2];  // Z_INV: the old field's real part of the tile, double-buffered
-    MB[0] = (double*)(B[2] + tsz);
-    MB[1] = MB[0] + tsz;
+    double* MB = (double*)(B[2] + tsz);  // Z_INV: the old field's real part of the current tile
     const long long xyz = ctl->xyz;
     unsigned long long base = 0;
     if (MODE == Z_RAND) base = draw_base(ctl->seed, ctl->call);
     const double2* src = (MODE == Z_FWD || MODE == Z_BWD) ? m : A;
     // a tile's G lines are one contiguous run of voxels: v0 = tile G Nz ..
     auto valid_of = [&](int tile) { return (int)(min((long long)G, nlines - (long long)tile * G) * Nz); };
-    auto fetch = [&](double2* S, double* MS, int tile) {
+    auto fetch = [&](double2* S, int tile) {
         const long long v0 = (long long)tile * tsz;
         const int valid = valid_of(tile);
 #pragma unroll 4
@@ -176,28 +175,40 @@ __global__ void __launch_bounds__(kThreads) krec_z(double2* __restrict__ A, doub
             if (MODE == Z_RAND) S[t] = t < valid ? make_double2(draw_pm1(base, (unsigned long long)(v0 + t)), 0.0)
                                                  : make_double2(0, 0);
             else cp_async16(S + t, t < valid ? src + v0 + t : src, t < valid);
-            if (MODE == Z_INV) cp_async8(MS + t, t < valid ? &m[v0 + t].x : &m[0].x, t < valid);
         }
     };
     int tile = blockIdx.x;
-    if (tile < ntiles) fetch(B[0], MB[0], tile);
+    if (tile < ntiles) fetch(B[0], tile);
     cp_async_commit();
     for (int t = threadIdx.x; t < Nz; t += blockDim.x) tw[t] = twz[t];
     const LineLayout L{G, G, Nz, 0, 1, false};
     const double dxyz = (double)xyz;
     const double beta = MODE == Z_INV ? ctl->beta : 0.0;
     const bool hio = MODE == Z_INV && ctl->hio != 0;
-    int d = 0, mbi = 0;
+    int d = 0;
     for (; tile < ntiles; tile += gridDim.x) {
         cp_async_wait_all();
         __syncthreads();
         const int f = d == 0 ? 2 : d - 1;
+        if (MODE == Z_INV) {
+            // this tile's old field (the projection needs it only after the
+            // transform, so the copy completes behind it): its own group
+            const long long v0 = (long long)tile * tsz;
+            const int valid = valid_of(tile);
+#pragma unroll 4
+            for (int t = threadIdx.x; t < valid; t += blockDim.x) cp_async8(MB + t, &m[v0 + t].x, true);
+            cp_async_commit();
+        }
         const int nxt = tile + gridDim.x;
-        if (nxt < ntiles) fetch(B[f], MB[mbi ^ 1], nxt);
+        if (nxt < ntiles) fetch(B[f], nxt);
         cp_async_commit();
         double2* r = fft_lines<double2, MaxR>(B[d], B[d == 2 ? 0 : d + 1], tw, pz, L,
                                               (MODE == Z_INV || MODE == Z_BWD) ? +1 : -1);
-        const double* old = MB[mbi];
+        if (MODE == Z_INV) {
+            cp_async_wait_group1();  // the old field landed (the next tile may still be in flight)
+            __syncthreads();
+        }
+        const double* old = MB;
         const long long v0 = (long long)tile * tsz;
         const int valid = valid_of(tile);
         if (MODE != Z_INV) {
@@ -223,7 +234,6 @@ __global__ void __launch_bounds__(kThreads) krec_z(double2* __restrict__ A, doub
             }
         }
         d = f;
-        mbi ^= 1;
     }
     cp_async_wait_all();
 }
@@ -607,7 +617,7 @@ struct m3d_rec {
         if (stream) cudaStreamDestroy(stream);
     }
     size_t z_smem() const { return (size_t)Nz * 16 + 3 * (size_t)G * Nz * 16; }
-    size_t zi_smem() const { return z_smem() + 2 * (size_t)G * Nz * 8; }
+    size_t zi_smem() const { return z_smem() + (size_t)G * Nz * 8; }
     size_t y_smem() const { return (size_t)Ny * 16 + 3 * (size_t)Ny * TZ * 16; }
     size_t x_smem() const { return (size_t)Nx * 16 + 3 * (size_t)Nx * TZX * 16 + 2 * (size_t)Nx * TZX * 8; }
     size_t xr_smem() const { return (size_t)Nx * 16 + 3 * (size_t)Nx * TZX * 16; }
@@ -909,7 +919,9 @@ static int rec_alloc(int Nx, int Ny, int Nz, int device, m3d_rec** out) {
     }
     // ~48 KB of shared memory per CTA (two buffers of 16-byte elements) so
     // that several CTAs share an SM
-    h->G = std::max(1, std::min(16, (int)(48 * 1024 / (32 * (size_t)Nz))));
+    // z tiles: three 16-byte buffers plus the old field's 8-byte values in
+    // about 75 KB, so that three CTAs share an SM
+    h->G = std::max(1, std::min(16, (int)((75 * 1024 - 16 * (size_t)Nz) / (56 * (size_t)Nz))));
     const int nmax = std::max(Nx, Ny);
     h->TZ = std::max(1, std::min(16, (int)(48 * 1024 / (32 * (size_t)nmax))));
     h->TZ = std::min(h->TZ, Nz);
