@@ -1,6 +1,7 @@
 // fft_plan.hpp -- host-side set-up of the generic line FFTs: the radix
 // schedule of a length and its twiddle table (shared by the 3-D and 2-D solvers).
 #pragma once
+#include <algorithm>
 #include <cmath>
 #include <vector>
 
@@ -11,13 +12,18 @@ namespace m3d {
 // radix schedule: odd primes up to kMaxGenericRadix, largest first (the
 // first stage needs no twiddle multiplications, so the costliest butterfly
 // goes there), then 8, 4, 2; false if a factor is larger
-inline bool make_plan(int n, LinePlan& p) {
+// (fuse9: two factors 3 become one radix-9 stage -- one Stockham stage and
+// barrier fewer -- for callers whose kernels compile the 9-point butterfly)
+inline bool make_plan(int n, LinePlan& p, bool fuse9 = false) {
     std::vector<int> f, odd;
     int m = n;
     int p2 = 0;
     while (m % 2 == 0) { ++p2; m /= 2; }
+    if (fuse9)
+        while (m % 9 == 0) { odd.push_back(9); m /= 9; }
     for (int q = 3; q <= m; q += 2)
         while (m % q == 0) { odd.push_back(q); m /= q; }
+    std::sort(odd.begin(), odd.end());
     for (auto it = odd.rbegin(); it != odd.rend(); ++it) f.push_back(*it);
     for (; p2 >= 3; p2 -= 3) f.push_back(8);
     if (p2 == 2) f.push_back(4);

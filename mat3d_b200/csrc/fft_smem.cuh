@@ -213,9 +213,9 @@ __device__ __forceinline__ void butterfly_odd(const C2* __restrict__ src, C2* __
         T px = x0.x, py = x0.y, qx = 0, qy = 0;
 #pragma unroll
         for (int q = 1; q <= h; ++q) {
-            const int m = (q * k) % R;
-            const T cc = m <= h ? c[m - 1] : c[R - m - 1];
-            const T ss = m <= h ? sn[m - 1] : -sn[R - m - 1];
+            const int m = (q * k) % R;  // 0 only for a composite R (e.g. 3 * 3 for R = 9)
+            const T cc = m == 0 ? (T)1 : (m <= h ? c[m - 1] : c[R - m - 1]);
+            const T ss = m == 0 ? (T)0 : (m <= h ? sn[m - 1] : -sn[R - m - 1]);
             px += a[q - 1].x * cc;
             py += a[q - 1].y * cc;
             qx += b[q - 1].x * ss;
@@ -257,8 +257,8 @@ struct LineLayout {
 
 // Transforms every line; returns the buffer (a or b) that holds the result.
 // Must be called by all threads of the CTA; ends with __syncthreads().
-// Radices 2, 3, 4, 5, 8 are compile-time butterflies; odd primes 7..MaxR are
-// compile-time too when MaxR reaches them (each adds registers to the
+// Radices 2, 3, 4, 5, 8 are compile-time butterflies; odd radices 7..MaxR
+// (the primes and 9) are compile-time too when MaxR reaches them (each adds registers to the
 // kernel, so callers pick the smallest MaxR their lengths need); any other
 // radix runs the run-time generic butterfly.
 // one Stockham stage of radix R over every line of the tile (R fixed at
@@ -306,6 +306,7 @@ __device__ C2* fft_lines(C2* a, C2* b, const C2* tw, const LinePlan& p, const Li
             case 8: run_stage<C2, 8, 0>(a, b, tw, S, R, L, dl, dg, sign); break;
             default:
                 if constexpr (MaxR >= 7) if (R == 7) { run_stage<C2, 7, 1>(a, b, tw, S, R, L, dl, dg, sign); break; }
+                if constexpr (MaxR >= 9) if (R == 9) { run_stage<C2, 9, 1>(a, b, tw, S, R, L, dl, dg, sign); break; }
                 if constexpr (MaxR >= 11) if (R == 11) { run_stage<C2, 11, 1>(a, b, tw, S, R, L, dl, dg, sign); break; }
                 if constexpr (MaxR >= 13) if (R == 13) { run_stage<C2, 13, 1>(a, b, tw, S, R, L, dl, dg, sign); break; }
                 if constexpr (MaxR >= 17) if (R == 17) { run_stage<C2, 17, 1>(a, b, tw, S, R, L, dl, dg, sign); break; }

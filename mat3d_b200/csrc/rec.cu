@@ -913,7 +913,7 @@ static int rec_alloc(int Nx, int Ny, int Nz, int device, m3d_rec** out) {
     h->Nx = Nx; h->Ny = Ny; h->Nz = Nz;
     h->xyz = (long long)Nx * Ny * Nz;
     h->device = device;
-    if (!make_plan(Nx, h->px) || !make_plan(Ny, h->py) || !make_plan(Nz, h->pz)) {
+    if (!make_plan(Nx, h->px, true) || !make_plan(Ny, h->py, true) || !make_plan(Nz, h->pz, true)) {
         delete h;
         return failr(M3D_ERR_UNSUPPORTED, "grid sizes need prime factors <= 32");
     }
