@@ -517,8 +517,16 @@ __global__ void krec_thr_try(const double* __restrict__ re, RecCtl* ctl, long lo
     __shared__ bool last;
     const double cut = __dsub_rn(0.5, ctl->x);
     unsigned int cnt = 0;
-    for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < xyz; v += (long long)gridDim.x * blockDim.x)
-        cnt += re[v] < cut ? 1u : 0u;
+    // two values per 16-byte load (the copy is 256-byte aligned), the odd tail by one thread
+    const double2* re2 = reinterpret_cast<const double2*>(re);
+    const long long n2 = xyz / 2;
+    const long long tid = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+#pragma unroll 4
+    for (long long v = tid; v < n2; v += (long long)gridDim.x * blockDim.x) {
+        const double2 q = re2[v];
+        cnt += (q.x < cut ? 1u : 0u) + (q.y < cut ? 1u : 0u);
+    }
+    if ((xyz & 1) && tid == 0) cnt += re[xyz - 1] < cut ? 1u : 0u;
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) cnt += __shfl_down_sync(0xffffffffu, cnt, off);
     if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = cnt;

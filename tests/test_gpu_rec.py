@@ -47,7 +47,7 @@ def state_close(gpu, st, tol=1e-9):
     assert d < tol, d
 
 
-@pytest.mark.parametrize("shape", [(8, 8, 8), (6, 8, 10), (16, 12, 9)])
+@pytest.mark.parametrize("shape", [(8, 8, 8), (6, 8, 10), (16, 12, 9), (9, 9, 9), (7, 9, 11)])
 def test_initial_field_and_threshold_exact(shape):
     """n = 0: the initial draws (m = (U + 1) / 2) thresholded; both steps exact."""
     T = example_tpcf(shape)
@@ -143,8 +143,8 @@ def test_converged_pass_leaves_field():
     r.close()
 
 
-def test_threshold_exact_on_planted_field():
-    shape = (20, 20, 20)
+@pytest.mark.parametrize("shape", [(20, 20, 20), (21, 21, 21)])  # even and odd voxel counts
+def test_threshold_exact_on_planted_field(shape):
     T = example_tpcf(shape)
     rng = np.random.default_rng(4)
     f = rng.random(int(np.prod(shape))) * 1.2 - 0.1 + 1j * rng.random(int(np.prod(shape)))
