@@ -344,3 +344,21 @@ def test_handles_of_different_sizes_coexist():
     assert np.array_equal(big.errors(), e1)
     small.close()
     big.close()
+
+
+@pytest.mark.parametrize("shape", [(256, 200, 64), (96, 243, 35)])
+def test_larger_grids_vs_oracle(shape):
+    """Long lines and other tile sizes (256-point x lines, radices 5 and 9,
+    27-point stages): three passes against the restatement."""
+    T = example_tpcf(shape, A=6.0, Q=0.5, phi1=0.45)
+    r = m3d.Reconstruction(T, *shape)
+    r.seed(2)
+    r.run(0, 0.8)
+    o = O.RecOracle(T, *shape)
+    st = o.start(2)
+    r.set_state(st["mT"], 0, 0, 1)
+    r.iterate(3, 0.8)
+    e = [o.step(st, 0.8) for _ in range(3)]
+    assert np.abs(r.errors() - np.array(e)).max() / e[0] < 1e-10
+    state_close(r.get_state(), st, 1e-9)
+    r.close()
