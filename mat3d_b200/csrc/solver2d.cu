@@ -75,34 +75,73 @@ __global__ void k2d_pointwise(const double2* __restrict__ eps, double2* __restri
     }
 }
 
-// Row FFTs (along y, contiguous): G lines of length Ny per CTA.  Inverse rows
-// finish the iteration: eps = result / xy (FFTBCKWRD_epsilon :140-145).
+// 16-byte global -> shared copies that complete asynchronously (zero-filled when !ok)
+__device__ __forceinline__ void cp16(void* sdst, const void* gsrc, bool ok) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(sdst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(sa), "l"(gsrc), "r"(ok ? 16 : 0) : "memory");
+}
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
+// Row FFTs (along y, contiguous): tiles of G lines of length Ny, walked by
+// persistent CTAs with three shared buffers -- the next tile streams in by
+// cp.async while the current one is transformed.  Inverse rows finish the
+// iteration: eps = result / xy (FFTBCKWRD_epsilon :140-145).
+// (nbuf = 2 for the longest rows, whose third buffer does not fit: each tile
+// is then fetched after the previous one is stored)
 __global__ void k2d_rows(double2* __restrict__ buf, double2* __restrict__ eps, const double2* __restrict__ twy,
-                         LinePlan py, int G, int nlines, int sign, long long xy) {
+                         LinePlan py, int G, int nlines, int sign, long long xy, int nbuf) {
     extern __shared__ __align__(16) char smem_raw[];
     const int Ny = py.n;
+    const int tsz = G * Ny;
+    const int ntiles = (nlines + G - 1) / G;
     double2* tw = (double2*)smem_raw;
-    double2* A = tw + Ny;
-    double2* B = A + (size_t)G * Ny;
-    const long long l0 = (long long)blockIdx.x * G;
+    double2* S[3];
+    S[0] = tw + Ny;
+    S[1] = S[0] + tsz;
+    S[2] = S[1] + tsz;
+    // a tile's lines are one contiguous run: elements tile * G * Ny ..
+    auto valid_of = [&](int tile) { return min(G, nlines - tile * G) * Ny; };
+    auto fetch = [&](double2* D, int tile) {
+        const long long v0 = (long long)tile * tsz;
+        const int valid = valid_of(tile);
+        for (int i = threadIdx.x; i < tsz; i += blockDim.x) cp16(D + i, i < valid ? buf + v0 + i : buf, i < valid);
+    };
+    const bool pre = nbuf == 3;
+    int tile = blockIdx.x;
+    if (pre && tile < ntiles) fetch(S[0], tile);
+    cp_commit();
     for (int i = threadIdx.x; i < Ny; i += blockDim.x) tw[i] = twy[i];
-    for (int i = threadIdx.x; i < G * Ny; i += blockDim.x) {
-        const long long l = l0 + i / Ny;
-        A[i] = l < nlines ? buf[l * Ny + i % Ny] : make_double2(0, 0);
-    }
-    __syncthreads();
-    LineLayout L{G, G, Ny, 0, 1, false};
-    double2* r = fft_lines(A, B, tw, py, L, sign);
-    for (int i = threadIdx.x; i < G * Ny; i += blockDim.x) {
-        const long long l = l0 + i / Ny;
-        if (l >= nlines) continue;
-        if (eps) {
-            const double2 w = r[i];
-            eps[l * Ny + i % Ny] = make_double2(w.x / (double)xy, w.y / (double)xy);
-        } else {
-            buf[l * Ny + i % Ny] = r[i];
+    const LineLayout L{G, G, Ny, 0, 1, false};
+    int d = 0;
+    for (; tile < ntiles; tile += gridDim.x) {
+        if (!pre) {
+            __syncthreads();  // the previous tile's stores are done with the buffers
+            fetch(S[0], tile);
+            cp_commit();
         }
+        cp_wait_all();
+        __syncthreads();  // tile landed; the previous tile's stores are done with its buffers
+        const int f = d == 0 ? 2 : d - 1;
+        const int nxt = tile + gridDim.x;
+        if (pre) {
+            if (nxt < ntiles) fetch(S[f], nxt);
+            cp_commit();
+        }
+        double2* r = fft_lines(S[d], S[d == 2 ? 0 : d + 1], tw, py, L, sign);
+        const long long v0 = (long long)tile * tsz;
+        const int valid = valid_of(tile);
+        if (eps) {
+            for (int i = threadIdx.x; i < valid; i += blockDim.x) {
+                const double2 w = r[i];
+                eps[v0 + i] = make_double2(w.x / (double)xy, w.y / (double)xy);
+            }
+        } else {
+            for (int i = threadIdx.x; i < valid; i += blockDim.x) buf[v0 + i] = r[i];
+        }
+        if (pre) d = f;
     }
+    cp_wait_all();
 }
 
 // Column turnaround: TZ consecutive columns y of all Nx rows and 3 components;
@@ -245,15 +284,17 @@ struct m3d_solver2d {
         cudaFree(eps); cudaFree(sig); cudaFree(buf); cudaFree(twx); cudaFree(twy); cudaFree(phase); cudaFree(part);
         if (stream) cudaStreamDestroy(stream);
     }
-    size_t rows_smem() const { return (size_t)Ny * 16 + 2 * (size_t)G * Ny * 16; }
+    int rows_nbuf = 3;  // shared buffers of the row passes (3: the next tile prefetched)
+    int rows_grid = 1;  // persistent CTAs of the row passes
+    size_t rows_smem() const { return (size_t)Ny * 16 + (size_t)rows_nbuf * G * Ny * 16; }
     size_t cols_smem() const { return (size_t)Nx * 16 + 2 * (size_t)3 * Nx * TZ * 16; }
     int iterate() {
         const int nb = 592;
         k2d_pointwise<<<nb, 256, 0, stream>>>(eps, sig, buf, phase, k, xy);
         const int nlines = 3 * Nx;
-        k2d_rows<<<(nlines + G - 1) / G, 256, rows_smem(), stream>>>(buf, nullptr, twy, py, G, nlines, -1, xy);
+        k2d_rows<<<rows_grid, 256, rows_smem(), stream>>>(buf, nullptr, twy, py, G, nlines, -1, xy, rows_nbuf);
         k2d_cols<<<(Ny + TZ - 1) / TZ, 256, cols_smem(), stream>>>(buf, twx, px, Ny, TZ, k, xy);
-        k2d_rows<<<(nlines + G - 1) / G, 256, rows_smem(), stream>>>(buf, eps, twy, py, G, nlines, +1, xy);
+        k2d_rows<<<rows_grid, 256, rows_smem(), stream>>>(buf, eps, twy, py, G, nlines, +1, xy, rows_nbuf);
         launches += 4;
         M2_CUDA(cudaGetLastError());
         return M3D_OK;
@@ -278,6 +319,7 @@ int m3d2d_create(int Nx, int Ny, m3d_solver2d** out) {
     }
     // rows: G lines per CTA in ~48 KB; columns: TZ columns of 3 components in ~96 KB
     h->G = std::max(1, std::min(16, (int)(48 * 1024 / (32 * (size_t)Ny))));
+    if ((size_t)Ny * 16 + 3 * (size_t)h->G * Ny * 16 > 220 * 1024) h->rows_nbuf = 2;
     h->TZ = std::max(1, std::min(16, (int)(96 * 1024 / (96 * (size_t)Nx))));
     if (h->rows_smem() > 220 * 1024 || h->cols_smem() > 220 * 1024) {
         delete h;
@@ -305,6 +347,14 @@ int m3d2d_create(int Nx, int Ny, m3d_solver2d** out) {
         cudaFuncAttributes a;
         if (cudaFuncGetAttributes(&a, k) == cudaSuccess)
             cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024 - (int)a.sharedSizeBytes);
+    }
+    {
+        int per_sm = 0, sms = 0, dev = 0;
+        cudaGetDevice(&dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k2d_rows, 256, h->rows_smem());
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        const int tiles = (3 * Nx + h->G - 1) / h->G;
+        h->rows_grid = std::max(1, std::min(tiles, std::max(1, per_sm) * std::max(1, sms)));
     }
     (void)cudaGetLastError();
     *out = h;
