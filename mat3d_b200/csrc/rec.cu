@@ -1004,18 +1004,19 @@ static double int_product(long long a, long long b, long long c, long long d) {
 }
 
 // writers -----------------------------------------------------------------
-static unsigned crc32_of(const unsigned char* p, size_t n, unsigned crc = 0xFFFFFFFFu) {
-    static unsigned table[256];
-    static bool init = false;
-    if (!init) {
+struct Crc32Table {
+    unsigned t[256];
+    Crc32Table() {
         for (unsigned i = 0; i < 256; ++i) {
             unsigned c = i;
             for (int k = 0; k < 8; ++k) c = (c & 1) ? 0xEDB88320u ^ (c >> 1) : c >> 1;
-            table[i] = c;
+            t[i] = c;
         }
-        init = true;
     }
-    for (size_t i = 0; i < n; ++i) crc = table[(crc ^ p[i]) & 0xFF] ^ (crc >> 8);
+};
+static unsigned crc32_of(const unsigned char* p, size_t n, unsigned crc = 0xFFFFFFFFu) {
+    static const Crc32Table table;  // initialised once, thread-safely
+    for (size_t i = 0; i < n; ++i) crc = table.t[(crc ^ p[i]) & 0xFF] ^ (crc >> 8);
     return crc;
 }
 
