@@ -139,3 +139,20 @@ def test_sections_bit_exact_on_reference_transform(name):
                                   fft2=lambda a, sh, sg: R.fft3(a, (sh[0], sh[1], 1), sg))
     assert np.array_equal(o.normC, g["normC"])
     assert np.array_equal(R.rec_sections(g["c1"], g["c2"]), g["normC"])
+
+
+@have_ref
+@pytest.mark.parametrize("beta,n", [(0.5, 230), (0.95, 230), (0.0, 60)])
+def test_live_reference_other_betas(beta, n):
+    """The hybrid input-output step for other feedback constants (beta = 0
+    reduces it to an error-reduction step) stays bit-exact with the reference."""
+    shape = (7, 8, 9)
+    R = ref_lib.RefLib()
+    m = max(shape)
+    t = O.tpcf_isotropic(m, 2.5, 0.9, 0.35).reshape(m, m, m)[:7, :8, :9].ravel()
+    T = np.real(np.fft.fftn(O.ifftshift3(t, *shape).reshape(shape))).ravel()
+    r = R.rec_run(shape, T, n, beta, 11)
+    o = O.RecOracle(T, *shape, fft=lambda a, sg: R.fft3(a, shape, sg), libm_atan2=True)
+    o.runRec(n, beta, 11)
+    assert np.array_equal(o.err, r["err"])
+    assert np.array_equal(o.rve, r["rve"])
