@@ -178,8 +178,10 @@ int m3d_get_profile(const m3d_solver* h, m3d_profile* out);
    component-major: d_grad[c*V + v]).  All working memory is a fixed 32 MiB
    device array inside the library (held by every GPU that loads it until
    exit); grids that need more (beyond about 96^3) are rejected with
-   M3D_ERR_ARG.  The first call on a device looks up that array's address, so
-   make it before any stream capture.  Calls share the array: calls that
+   M3D_ERR_ARG.  Every call looks up that array's address with the calling
+   device current (so it stays valid after cudaDeviceReset); the first call on
+   a device also sets kernel attributes, so make it before any stream
+   capture.  Calls share the array: calls that
    overlap on the GPU race, serialise them.  stream: cudaStream_t (NULL = the
    legacy default stream).  Calls no cudaMalloc, cudaFree or allocating
    library routine. */

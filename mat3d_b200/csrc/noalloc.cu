@@ -13,9 +13,11 @@
 // every GPU that loads this library, from module load until process exit.
 //
 // Rules of use:
-//  * The first call on a device looks up the array's device address with
-//    cudaGetSymbolAddress (with that device current) and caches it; make that
-//    first call before any stream capture.
+//  * Every call looks up the array's device address with
+//    cudaGetSymbolAddress, with the calling device current (nothing is cached,
+//    so the address stays right after cudaDeviceReset reloads the module);
+//    the first call on a device also sets the kernels' shared-memory limits.
+//    Make that first call before any stream capture.
 //  * All calls share the one array and it keeps the last call's contents;
 //    every call clears what must start at zero itself.  Calls that overlap on
 //    the GPU (two streams, or two host threads) race on the array: serialise
@@ -46,7 +48,7 @@ constexpr int kMaxDevices = 64;
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
 
 std::mutex g_noalloc_mu;
-unsigned char* g_noalloc_ptr[kMaxDevices] = {};
+bool g_noalloc_attrs[kMaxDevices] = {};  // kernel attributes set on this device (guarded by g_noalloc_mu)
 
 int nfail(int st, const std::string& msg) {
     m3d_internal_set_error("m3d_thermal_solve_noalloc: " + msg);
@@ -72,17 +74,18 @@ bool plan_of(int n, LinePlan& p) {
     return true;
 }
 
-// phase ids -> 0 (inclusion) / 1 (matrix, any nonzero id), and the count of ones
+// phase ids -> 0 (inclusion) / 1 (matrix, any nonzero id), and the sum of the
+// raw ids (the reference's RVE.sum(), which picks the scheme)
 __global__ void k_noalloc_phase(const uint8_t* __restrict__ in, uint8_t* __restrict__ out, long long V,
-                                unsigned long long* ones) {
+                                unsigned long long* idsum) {
     unsigned long long c = 0;
     for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < V; v += (long long)gridDim.x * blockDim.x) {
-        const uint8_t p = in[v] != 0;
-        out[v] = p;
-        c += p;
+        const uint8_t id = in[v];
+        out[v] = id != 0;
+        c += id;
     }
     for (int o = 16; o > 0; o >>= 1) c += __shfl_down_sync(0xffffffffu, c, o);
-    if ((threadIdx.x & 31) == 0 && c) atomicAdd(ones, c);
+    if ((threadIdx.x & 31) == 0 && c) atomicAdd(idsum, c);
 }
 
 __global__ void k_noalloc_fill(double* x, long long V, double e0, double e1, double e2) {
@@ -159,25 +162,21 @@ extern "C" int m3d_thermal_solve_noalloc(int Nx, int Ny, int Nz, double km, doub
                                       " needs " + std::to_string(need >> 20) + " MiB of scratch; the limit is " +
                                       std::to_string(kScratchBytes >> 20) + " MiB (about 96^3)");
 
-    // per-device set-up: the array's device address, looked up once with the device current
+    // the array's device address, looked up with the calling device current
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return nfail(M3D_ERR_CUDA, "no current CUDA device");
     unsigned char* base = nullptr;
     {
-        std::lock_guard<std::mutex> lk(g_noalloc_mu);
-        if (!g_noalloc_ptr[dev]) {
-            void* p = nullptr;
-            const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-            if (e != cudaSuccess) return nfail(M3D_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
-            g_noalloc_ptr[dev] = (unsigned char*)p;
-        }
-        base = g_noalloc_ptr[dev];
+        void* p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess) return nfail(M3D_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+        base = (unsigned char*)p;
     }
     double2* spec = (double2*)(base + o_spec);
     double* part = (double*)(base + o_part);
     Ctl* ctl = (Ctl*)(base + o_ctl);
     int* counter = (int*)(base + o_cnt);
-    unsigned long long* ones = (unsigned long long*)(base + o_ones);
+    unsigned long long* idsum = (unsigned long long*)(base + o_ones);
     double2* tw = (double2*)(base + o_tw);
     double* mats = (double*)(base + o_mats);
     uint8_t* ph = base + o_ph;
@@ -188,17 +187,18 @@ extern "C" int m3d_thermal_solve_noalloc(int Nx, int Ny, int Nz, double km, doub
         if (e_ != cudaSuccess) return nfail(M3D_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
     } while (0)
 
-    // what must start at zero: the completion counter and the ones count
+    // what must start at zero: the completion counter and the id sum
     NA_CUDA(cudaMemsetAsync(counter, 0, sizeof(int), stream));
-    NA_CUDA(cudaMemsetAsync(ones, 0, sizeof(unsigned long long), stream));
-    k_noalloc_phase<<<296, 256, 0, stream>>>(d_phase, ph, g.V, ones);
+    NA_CUDA(cudaMemsetAsync(idsum, 0, sizeof(unsigned long long), stream));
+    k_noalloc_phase<<<296, 256, 0, stream>>>(d_phase, ph, g.V, idsum);
     NA_CUDA(cudaGetLastError());
-    unsigned long long n1 = 0;
-    NA_CUDA(cudaMemcpyAsync(&n1, ones, sizeof(n1), cudaMemcpyDeviceToHost, stream));
+    unsigned long long ids = 0;
+    NA_CUDA(cudaMemcpyAsync(&ids, idsum, sizeof(ids), cudaMemcpyDeviceToHost, stream));
     NA_CUDA(cudaStreamSynchronize(stream));
 
-    // scheme (the reference's integer-division rule, src/3dTherm/FFT_thermal3D.cpp:399-410)
-    const long long vol_1 = (long long)n1 / g.V;
+    // scheme (the reference's integer-division rule on the raw id sum,
+    // src/3dTherm/FFT_thermal3D.cpp:399-410, as m3d_set_material_thermal)
+    const long long vol_1 = (long long)ids / g.V;
     const int scheme = ((vol_1 >= 1 && km > ki) || (vol_1 < 1 && km < ki)) ? 1 : 2;
     const double k0 = std::sqrt(ki * km);
     const double kk[2] = {ki, km};
@@ -262,13 +262,15 @@ extern "C" int m3d_thermal_solve_noalloc(int Nx, int Ny, int Nz, double km, doub
     const size_t ysmem = (size_t)Ny * sizeof(double2) + 2 * (size_t)Ny * TZy * sizeof(double2);
     const size_t xsmem = (size_t)Nx * sizeof(double2) + 2 * (size_t)C * Nx * TZx * sizeof(double2) + 16 + 32 * 32 * 8;
     const int ntzy = (g.Hzp + TZy - 1) / TZy, ntzx = (g.Hzp + TZx - 1) / TZx;
-    static bool attrs[kMaxDevices] = {};  // kernel attributes are per device
-    if (!attrs[dev]) {
-        allow_dyn(k_zfwd<double, C, ProMat<double, C>>);
-        allow_dyn(k_ypass<double>);
-        allow_dyn(k_xturn<double, C, SpecGreen<double, C>>);
-        allow_dyn(k_zinv<double, C, EpiEM<double, C>, FinLinear>);
-        attrs[dev] = true;
+    {
+        std::lock_guard<std::mutex> lk(g_noalloc_mu);  // kernel attributes are per device
+        if (!g_noalloc_attrs[dev]) {
+            allow_dyn(k_zfwd<double, C, ProMat<double, C>>);
+            allow_dyn(k_ypass<double>);
+            allow_dyn(k_xturn<double, C, SpecGreen<double, C>>);
+            allow_dyn(k_zinv<double, C, EpiEM<double, C>, FinLinear>);
+            g_noalloc_attrs[dev] = true;
+        }
     }
     const double2* twx = tw;
     const double2* twy = tw + Nx;

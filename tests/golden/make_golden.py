@@ -9,7 +9,7 @@ The reference project ships no tests or expected outputs of its own, so these
 fixtures are the parity pin for the numpy oracle (tests/test_oracle_golden.py)
 and, through it, for the CUDA solver.
 
-    make -C oracle && python tests/golden/make_golden.py
+    make -C oracle REF=<reference sources> && python tests/golden/make_golden.py
 """
 from __future__ import annotations
 
