@@ -63,20 +63,30 @@ def bytes_per_vi(c, w):
 PASS_NAMES = ("z_forward", "y_forward", "x_turnaround", "y_inverse", "z_inverse")
 PASS_KERNELS = ("k_zfwd_fast (prologue + z R2C)", "k_ypass_fast<-1>", "k_xturn_fast (x FFT, Green, x IFFT)",
                 "k_ypass_fast<+1>", "k_zinv_fast (z C2R + EM update + finalize)")
+# two-pass sweeps (per-component operators): the profile's slot 2 is the x
+# turnaround, slot 4 the y-z slab pass, the other slots are empty
+PASS_NAMES_2 = (None, None, "x_turnaround", None, "yz_slab")
+PASS_KERNELS_2 = (None, None, "k_xturn_fast (x FFT, Green, x IFFT)", None,
+                  "k_slab<MIX> (y IFFT, z C2R, EM update, polarization, z R2C, y FFT + finalize)")
 
 
-def pass_bytes(c, w, N, forcing):
+def pass_bytes(c, w, N, forcing, two_pass=False):
     """Algorithmic bytes per launch of each sweep pass on an N^3 grid with c
     components of w-byte reals: the pass's own inputs and outputs (half
     spectrum N*N*Hzp complex per component, Hzp = N/2+1 rounded up to even;
     state c*V reals; 1-byte phase; the FP32 defect read by the refinement's
-    inner sweeps)."""
+    inner sweeps).  Two-pass sweeps: the x turnaround, and the slab pass that
+    reads and writes the spectrum and the state once, reads the defect and the
+    phase map once per component."""
     V = N ** 3
     hzp = ((N // 2 + 1) + 1) & ~1
     spec = c * N * N * hzp * 2 * w
     state = c * V * w
+    forcing_b = c * V * 4 if forcing else 0
+    if two_pass:
+        return (0, 0, 2 * spec, 0, 2 * spec + 2 * state + c * V + forcing_b)
     zfwd = state + V + spec
-    zinv = spec + 2 * state + V + (c * V * 4 if forcing else 0)
+    zinv = spec + 2 * state + V + forcing_b
     return (zfwd, 2 * spec, 2 * spec, 2 * spec, zinv)
 
 
@@ -974,16 +984,19 @@ def main():
         if n and sum(pms) > 0:
             p = int(np.argmax(pms))
             wb = 4 if fp32 else 8
+            two = pres["st"]["passes_per_sweep"] == 2
+            names, kernels = (PASS_NAMES_2, PASS_KERNELS_2) if two else (PASS_NAMES, PASS_KERNELS)
             forcing = w["precision"] == "fp32_refine" and fp32  # inner sweeps read the FP32 defect
-            pb = pass_bytes(c, wb, N, forcing)[p]
+            pb = pass_bytes(c, wb, N, forcing, two)[p]
             us = 1000 * pms[p] / n
-            tr = MEASURED_TRAFFIC.get((args.workload, PASS_NAMES[p], wb))
-            kern = {"bound": "hbm", "kernel": PASS_KERNELS[p], "pass": PASS_NAMES[p],
+            tr = MEASURED_TRAFFIC.get((args.workload, names[p], wb))
+            kern = {"bound": "hbm", "kernel": kernels[p], "pass": names[p],
                     "achieved": pb / (us * 1e-6) / 1e9, "peak": peak, "unit": "GB/s",
                     "frac": pb / (us * 1e-6) / 1e9 / peak, "traffic": tr[0] if tr else None,
                     "traffic_source": tr[1] if tr else None, "peak_source": peak_src,
                     "bytes_per_launch": pb, "launch_us": us, "share_of_sweep": pms[p] / sum(pms),
-                    "pass_us": {PASS_NAMES[q]: 1000 * pms[q] / n for q in range(5)}}
+                    "passes_per_sweep": 2 if two else 5,
+                    "pass_us": {names[q]: 1000 * pms[q] / n for q in range(5) if names[q]}}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -1014,7 +1027,7 @@ def main():
             "roofline_solve": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                                "frac": (achieved / peak) if achieved else None,
                                "peak_source": peak_src,
-                               "kernel": "the timed solves (one graph launch each: sweeps of 5 fused FFT passes)",
+                               "kernel": "the timed solves (one graph launch each: sweeps of fused FFT passes)",
                                "bytes_per_voxel_iter": {"fp32": b32, "fp64": b64},
                                "sweep_us": {"fp32": sweep_fp32_us, "fp64": sweep_fp64_us}},
             "fp64_solver": {"value": val64, "unit": UNIT, "ms_per_solve": ms64 / steps64,

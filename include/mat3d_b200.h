@@ -51,7 +51,7 @@
 extern "C" {
 #endif
 
-#define M3D_ABI_VERSION 1
+#define M3D_ABI_VERSION 2
 
 typedef enum {
     M3D_OK = 0,
@@ -98,6 +98,8 @@ typedef struct {
     double k0;               /* reference conductivity (thermal) */
     double vol_fraction[16]; /* per phase id */
     long long kernel_launches; /* kernels this handle launched since creation */
+    int passes_per_sweep;    /* launches per linear sweep of the last run: 5 (z, y, x, y, z passes) or
+                                2 (x turnaround + the y-z slab pass, per-component operators) */
 } m3d_stats;
 
 /* Create a solver for an Nx x Ny x Nz grid.  `batch` independent solves
@@ -159,7 +161,9 @@ typedef struct {
     double ms_fp32;      /* summed device time of FP32 sweeps */
     long long n_fp32;    /* FP32 sweeps timed */
     /* the same time split by pass (events around each pass of the linear
-       sweeps): z forward, y forward, x turnaround, y inverse, z inverse */
+       sweeps): z forward, y forward, x turnaround, y inverse, z inverse; on
+       two-pass sweeps (m3d_stats.passes_per_sweep == 2) slot 2 holds the x
+       turnaround and slot 4 the y-z slab pass, slots 0, 1 and 3 stay 0 */
     double pass_ms_fp64[5];
     double pass_ms_fp32[5];
 } m3d_profile;

@@ -52,7 +52,7 @@ class Stats(ctypes.Structure):
         ("residual", ctypes.c_double), ("eqvar", ctypes.c_double), ("diff_sum", ctypes.c_double),
         ("diff_eq", ctypes.c_double), ("solve_ms", ctypes.c_double), ("la0", ctypes.c_double),
         ("mu0", ctypes.c_double), ("k0", ctypes.c_double), ("vol_fraction", ctypes.c_double * 16),
-        ("kernel_launches", ctypes.c_longlong),
+        ("kernel_launches", ctypes.c_longlong), ("passes_per_sweep", ctypes.c_int),
     ]
 
     def as_dict(self):

@@ -25,6 +25,7 @@
 #include "physics.cuh"
 #include "inelastic.cuh"
 #include "passes_fast.cuh"
+#include "passes_slab.cuh"
 #include "fft_plan.hpp"
 
 #include <cudaTypedefs.h>
@@ -172,6 +173,7 @@ struct m3d_solver {
         std::vector<double> hOsum;
         int gkind = 0, gnyq = 0, gxw = 0;
         double gp1 = 0, gp2 = 0;
+        bool diag = false;  // P and A diagonal in the components for every phase (slab pass usable)
     };
     int nrve = 1;
     std::vector<RveHost> rv;
@@ -302,6 +304,16 @@ struct m3d_solver {
     int* d_err = nullptr;  // device-side error word (bounded waits that expired)
     bool ensure_ymaps(int CC);
     bool use_fast = true;
+    // two-pass sweeps (x turnaround + y-z slab pass) where the operators are
+    // per-component and the slab fits two CTAs per SM; M3D_NO_SLAB=1 keeps
+    // the five-pass sweep
+    bool use_slab = true;
+    template <typename T> bool slab_ok() const;
+    template <typename T, int CC, bool MIX, class Fin>
+    int pass_slab(Ctl* ctl, T* x, const float* r, typename Cx<T>::t* sp, Fin fin);
+    template <typename T, int CC>
+    int launch_em_slab(Ctl* ctl, T* x, const float* r, typename Cx<T>::t* sp, int zero_k0, int policy,
+                       const Ctl* outer);
     template <typename T, int CC> int tune_time(int sweeps, float* ms);
     int autotune(int sweeps, m3d_tune* out);
     template <typename T, int CC>
@@ -326,7 +338,8 @@ struct m3d_solver {
         }
     }
     long long graph_key(int type) const {
-        return ((((long long)type * 8192 + B) * 32 + nph_max()) * 2 + (use_fast ? 1 : 0)) * 4 + prec;
+        return (((((long long)type * 8192 + B) * 32 + nph_max()) * 2 + (use_fast ? 1 : 0)) * 4 + prec) * 2 +
+               (use_slab ? 1 : 0);
     }
     template <typename T, int CC>
     int run_linear_graph(double tol_field, double tol_eq, int criterion, int max_iter);
@@ -467,6 +480,12 @@ int m3d_solver::sync_ctl(Ctl* dctl) {
 void m3d_solver::snapshot_rve(int r) {
     RveHost& m = rv[r];
     m.set = true;
+    m.diag = hP.size() >= (size_t)nph * C * C && hA.size() >= (size_t)nph * C * C;
+    for (int p = 0; m.diag && p < nph; ++p)
+        for (int i = 0; i < C; ++i)
+            for (int j = 0; j < C; ++j)
+                if (i != j && (hP[((size_t)p * C + i) * C + j] != 0.0 || hA[((size_t)p * C + i) * C + j] != 0.0))
+                    m.diag = false;
     m.nph = nph;
     m.scheme = scheme;
     m.den_ref = den_ref;
@@ -724,6 +743,60 @@ int m3d_solver::launch_em(Ctl* ctl, T* x, const float* r, typename Cx<T>::t* sp,
     return launch_sweep<T, CC>(pro, green<T, CC>(zero_k0), epi, ctl, sp, policy, outer);
 }
 
+// ---- two-pass sweeps: x turnaround + y-z slab pass (passes_slab.cuh) --------
+// A slab instantiation is used where its shared memory leaves room for two
+// CTAs per SM.
+template <typename T, int NN>
+constexpr bool slab_fits() {
+    return SlabGeom<T, NN>::smem() <= (size_t)110 * 1024;
+}
+
+template <typename T>
+bool m3d_solver::slab_ok() const {
+    if (!use_fast || !use_slab || Ny != Nz) return false;
+    for (const RveHost& m : rv)
+        if (!m.diag) return false;
+    bool ok = false;
+    with_fast_n(Nz, [&](auto nc) { ok = slab_fits<T, decltype(nc)::value>(); });
+    return ok;
+}
+
+template <typename T, int CC, bool MIX, class Fin>
+int m3d_solver::pass_slab(Ctl* ctl, T* x, const float* r, typename Cx<T>::t* sp, Fin fin) {
+    SlabOps<T> ops{CC, d_phase, x, r, dm(off_P), dm(off_A), dm(off_Os), nph_max(), entries_per_rve(), mstride};
+    bool done = false;
+    with_fast_n(Nz, [&](auto nc) {
+        constexpr int NN = decltype(nc)::value;
+        if constexpr (slab_fits<T, NN>()) {
+            auto kern = k_slab<T, NN, MIX, Fin>;
+            allow_smem(kern);
+            kern<<<dim3(CC * Nx, B), kSlabThreads, SlabGeom<T, NN>::smem(), stream>>>(g, tw<T>(2), sp, ops, ctl,
+                                                                                      d_part, fin);
+            done = true;
+        }
+    });
+    if (!done) return fail(M3D_ERR_STATE, "slab pass requested for a grid without a slab kernel");
+    st.kernel_launches += 1;
+    M3D_CUDA(cudaGetLastError());
+    return M3D_OK;
+}
+
+// One two-pass sweep; the finalize runs in the last CTA of the slab pass.
+// Profiling slots: 2 = x turnaround, 4 = slab pass.
+template <typename T, int CC>
+int m3d_solver::launch_em_slab(Ctl* ctl, T* x, const float* r, typename Cx<T>::t* sp, int zero_k0, int policy,
+                               const Ctl* outer) {
+    prof_pass(0);
+    prof_pass(1);
+    prof_pass(2);
+    pass_x<T, CC>(green<T, CC>(zero_k0), ctl, sp);
+    prof_pass(3);
+    prof_pass(4);
+    const int rc = pass_slab<T, CC, true>(ctl, x, r, sp, FinLinear{policy, (double)g.V, outer, d_counter});
+    prof_pass(5);
+    return rc;
+}
+
 // Fill the state with the uniform load (setLoad, src/3d/FFT_analysis3D.cpp:551-564).
 template <typename T>
 __global__ void k_fill_load(T* x, const Ctl* ctl, int C, long long V) {
@@ -745,10 +818,18 @@ int m3d_solver::run_linear(double tol_field, double tol_eq, int criterion, int m
     C2* sp = (C2*)d_spec;
     const int chunk = kChunk;
     int before = 0;
+    const bool slab = criterion == M3D_CRIT_RESIDUAL && slab_ok<T>();
+    st.passes_per_sweep = slab ? 2 : 5;
+    if (slab) {
+        rc = pass_slab<T, CC, false>(d_ctl, x, nullptr, sp, FinNone{});
+        if (rc) return rc;
+    }
     for (;;) {
         for (int k = 0; k < chunk; ++k) {
             prof_mark(k);
-            if (criterion == M3D_CRIT_RESIDUAL) {
+            if (slab) {
+                rc = launch_em_slab<T, CC>(d_ctl, x, nullptr, sp, 0, POL_RESIDUAL, nullptr);
+            } else if (criterion == M3D_CRIT_RESIDUAL) {
                 rc = launch_em<T, CC>(d_ctl, x, nullptr, sp, 0, POL_RESIDUAL, nullptr);
             } else {
                 rc = launch_em<T, CC>(d_ctl, x, nullptr, sp, 0, POL_REF_SWEEP, nullptr);
@@ -798,6 +879,8 @@ int m3d_solver::run_refine(double tol_field, int max_iter) {
     long long n64 = 0, n32 = 0;
     bool first = true;
     const int chunk = 8;
+    const bool slab = slab_ok<float>();
+    st.passes_per_sweep = slab ? 2 : 5;
     for (;;) {
         ProRefine64<CC> pro = tab(ProRefine64<CC>{d_phase, x, first ? nullptr : d_delta, g.V, dm(off_P), nph_max(), nullptr});
         EpiDefect<CC> epi = tab(EpiDefect<CC>{d_phase, x, d_r32, g.V, dm(off_Os), nph_max(), nullptr});
@@ -825,11 +908,15 @@ int m3d_solver::run_refine(double tol_field, int max_iter) {
         }
         M3D_CUDA(cudaMemcpyAsync(d_ctl_in, h_ctl, B * sizeof(Ctl), cudaMemcpyHostToDevice, stream));
         M3D_CUDA(cudaMemsetAsync(d_delta, 0, (size_t)B * CC * g.V * sizeof(float), stream));
+        // two-pass sweeps carry the forward spectrum from sweep to sweep; the
+        // correction starts at 0, whose spectrum is 0
+        if (slab) M3D_CUDA(cudaMemsetAsync(sp32, 0, (size_t)B * CC * g.NL * g.Hzp * sizeof(float2), stream));
         int before = 0;
         for (;;) {
             for (int k = 0; k < chunk; ++k) {
                 prof_mark(k);
-                rc = launch_em<float, CC>(d_ctl_in, d_delta, d_r32, sp32, 1, POL_REFINE_INNER, d_ctl);
+                if (slab) rc = launch_em_slab<float, CC>(d_ctl_in, d_delta, d_r32, sp32, 1, POL_REFINE_INNER, d_ctl);
+                else rc = launch_em<float, CC>(d_ctl_in, d_delta, d_r32, sp32, 1, POL_REFINE_INNER, d_ctl);
                 if (rc) return rc;
             }
             prof_mark(chunk);
@@ -937,6 +1024,12 @@ int m3d_solver::run_linear_graph(double tol_field, double tol_eq, int criterion,
     k_fill_load<T><<<dim3(256, B * CC), 256, 0, stream>>>(x, d_ctl, CC, g.V);
     M3D_CUDA(cudaMemsetAsync(d_trips, 0, 8 * sizeof(int), stream));
     const bool resid = (criterion == M3D_CRIT_RESIDUAL);
+    const bool slab = resid && slab_ok<T>();
+    st.passes_per_sweep = slab ? 2 : 5;
+    if (slab) {
+        rc = pass_slab<T, CC, false>(d_ctl, x, nullptr, sp, FinNone{});
+        if (rc) return rc;
+    }
     GraphSlot& gs = gslot[resid ? 0 : 1];
     const long long key = graph_key(resid ? 0 : 1);
     if (gs.key != key) {
@@ -950,7 +1043,9 @@ int m3d_solver::run_linear_graph(double tol_field, double tol_eq, int criterion,
         M3D_CAP(add_while(top, nullptr, 0, h, &node, &body));
         const long long kl = st.kernel_launches;  // captured launches are counted per executed trip below
         M3D_CAP(cudaStreamBeginCaptureToGraph(stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
-        if (resid) {
+        if (slab) {
+            rc = launch_em_slab<T, CC>(d_ctl, x, nullptr, sp, 0, POL_RESIDUAL, nullptr);
+        } else if (resid) {
             rc = launch_em<T, CC>(d_ctl, x, nullptr, sp, 0, POL_RESIDUAL, nullptr);
         } else {
             rc = launch_em<T, CC>(d_ctl, x, nullptr, sp, 0, POL_REF_SWEEP, nullptr);
@@ -972,7 +1067,7 @@ int m3d_solver::run_linear_graph(double tol_field, double tol_eq, int criterion,
     if (rc) return rc;
     int trips[8];
     M3D_CUDA(cudaMemcpy(trips, d_trips, sizeof(trips), cudaMemcpyDeviceToHost));
-    st.kernel_launches += 1 + (long long)trips[0] * (resid ? 6 : 10);
+    st.kernel_launches += 1 + (long long)trips[0] * (slab ? 3 : (resid ? 6 : 10));
     long long sw = 0;
     int status = M3D_OK;
     for (int b = 0; b < B; ++b) {
@@ -1002,6 +1097,9 @@ int m3d_solver::run_refine_graph(double tol_field, int max_iter) {
     M3D_CUDA(cudaMemsetAsync(d_delta, 0, dbytes, stream));
     M3D_CUDA(cudaMemsetAsync(d_ctl_in, 0, (size_t)B * sizeof(Ctl), stream));
     M3D_CUDA(cudaMemsetAsync(d_trips, 0, 8 * sizeof(int), stream));
+    const bool slab = slab_ok<float>();
+    st.passes_per_sweep = slab ? 2 : 5;
+    const size_t sbytes32 = (size_t)B * CC * g.NL * g.Hzp * sizeof(float2);
     GraphSlot& gs = gslot[2];
     const long long key = graph_key(2);
     if (gs.key != key) {
@@ -1025,6 +1123,8 @@ int m3d_solver::run_refine_graph(double tol_field, int max_iter) {
         k_refine_mid<<<1, 256, 0, stream>>>(h_out, h_in, d_ctl, d_ctl_in, B, d_trips);
         M3D_CAP(cudaGetLastError());
         M3D_CAP(cudaMemsetAsync(d_delta, 0, dbytes, stream));
+        // two-pass sweeps: the correction starts at 0, whose spectrum is 0
+        if (slab) M3D_CAP(cudaMemsetAsync(sp32, 0, sbytes32, stream));
         {
             cudaStreamCaptureStatus cs;
             cudaGraph_t capg = nullptr;
@@ -1038,7 +1138,8 @@ int m3d_solver::run_refine_graph(double tol_field, int max_iter) {
         M3D_CAP(cudaStreamEndCapture(stream, &got));
         // inner body: FP32 correction sweep + loop control
         M3D_CAP(cudaStreamBeginCaptureToGraph(stream, b_in, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
-        rc = launch_em<float, CC>(d_ctl_in, d_delta, d_r32, sp32, 1, POL_REFINE_INNER, d_ctl);
+        if (slab) rc = launch_em_slab<float, CC>(d_ctl_in, d_delta, d_r32, sp32, 1, POL_REFINE_INNER, d_ctl);
+        else rc = launch_em<float, CC>(d_ctl_in, d_delta, d_r32, sp32, 1, POL_REFINE_INNER, d_ctl);
         if (rc) M3D_CAP(cudaErrorUnknown);
         k_loop_cond<<<1, 256, 0, stream>>>(h_in, d_ctl_in, B, d_trips, 2);
         M3D_CAP(cudaGetLastError());
@@ -1054,7 +1155,7 @@ int m3d_solver::run_refine_graph(double tol_field, int max_iter) {
     if (rc) return rc;
     int trips[8];
     M3D_CUDA(cudaMemcpy(trips, d_trips, sizeof(trips), cudaMemcpyDeviceToHost));
-    st.kernel_launches += 1 + (long long)trips[1] * 6 + (long long)trips[3] * 6;
+    st.kernel_launches += 1 + (long long)trips[1] * 6 + (long long)trips[3] * (slab ? 3 : 6);
     long long n64 = 0, n32 = 0;
     int status = M3D_OK;
     for (int b = 0; b < B; ++b) {
@@ -1086,6 +1187,7 @@ int m3d_solver::dispatch_run(double tol_field, double tol_eq, int nInc, int crit
 
 int m3d_solver::dispatch_core(double tol_field, double tol_eq, int nInc, int criterion, int max_iter) {
     if (max_iter <= 0) max_iter = (kind == M3D_KIND_MECH) ? 2000 : 500;
+    st.passes_per_sweep = 5;
     if (kind == M3D_KIND_MECH && behav != M3D_BEHAV_ELASTIC) {
         if (prec == M3D_PREC_FP32_REFINE)
             return fail(M3D_ERR_UNSUPPORTED, "FP32 refinement applies to the linear (elastic/thermal) solves; use FP32 or FP64 for ep/ed");
@@ -1243,6 +1345,8 @@ static int create_impl(int kind, int Nx, int Ny, int Nz, int behav, int precisio
         h->use_graph = !(e3 && e3[0] == '1');
         const char* e4 = std::getenv("M3D_TMA_Y");
         h->use_tma_y = (e4 && e4[0] == '1');
+        const char* e5 = std::getenv("M3D_NO_SLAB");
+        h->use_slab = !(e5 && e5[0] == '1');
     }
     int rc = h->alloc(batch);
     if (rc) { cudaStreamDestroy(h->stream); delete h; return rc; }

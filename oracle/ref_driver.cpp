@@ -15,6 +15,7 @@
 // Private members (iteration counter, scheme flags, setGF) are read through
 // the usual test-harness `#define private public`; class layout is unchanged.
 
+#include <chrono>
 #include <cmath>
 #include <complex>
 #include <cstdint>
@@ -63,6 +64,14 @@ protected:
     }
 };
 
+// Wall time of the last run's set-up (constructor: allocation and FFT plans;
+// material(): tables and the Green operator; setLoad()) and of its solve
+// (runAnalysis / homogenization), for the CPU baseline timing.
+double g_setup_s = 0, g_run_s = 0;
+double now_s() {
+    return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
 struct QuietScope {
     CountingNullBuf buf;
     std::streambuf* old;
@@ -98,6 +107,7 @@ int ref_mech_run(int Nx, int Ny, int Nz, const char* behav, const double* mat, i
     for (int i = 0; i < 6; ++i) { E(i) = E6[i]; X(i) = X06[i]; }
 
     fftw_plan_with_nthreads(fft_threads > 0 ? fft_threads : 3);
+    const double t0 = now_s();
     FFT_Analysis3D a(Nx, Ny, Nz, std::string(behav));
     a.material(m, R, nph);
     if (force_scheme == 1 || force_scheme == 2) {
@@ -113,7 +123,10 @@ int ref_mech_run(int Nx, int Ny, int Nz, const char* behav, const double* mat, i
         a.sigma_iter_old.resize(6, 1);
         a.epsilon_iter_old.resize(6, 1);
     }
+    const double t1 = now_s();
     a.runAnalysis(tol_field, tol_eq, nInc);
+    g_setup_s = t1 - t0;
+    g_run_s = now_s() - t1;
 
     if (eps_out) std::memcpy(eps_out, a.epsilon.data(), sizeof(double) * 6 * (size_t)V);
     if (sig_out) std::memcpy(sig_out, a.sigma.data(), sizeof(double) * 6 * (size_t)V);
@@ -178,10 +191,14 @@ int ref_therm_run(int Nx, int Ny, int Nz, double km, double ki, const int32_t* r
     MatrixDdd E(3, 1);
     for (int i = 0; i < 3; ++i) E(i) = E3[i];
     fftw_plan_with_nthreads(fft_threads > 0 ? fft_threads : 3);
+    const double t0 = now_s();
     FFT_analysis3d_thermal a(Nx, Ny, Nz);
     a.material(km, ki, R);
     a.setLoad(E);
+    const double t1 = now_s();
     a.runAnalysis(tol_field, tol_eq);
+    g_setup_s = t1 - t0;
+    g_run_s = now_s() - t1;
     if (grad_out) std::memcpy(grad_out, a.tempGradient.data(), sizeof(double) * 3 * (size_t)V);
     if (flux_out) std::memcpy(flux_out, a.heatFlux.data(), sizeof(double) * 3 * (size_t)V);
     if (sweeps_out) *sweeps_out = q.buf.iter_lines;
@@ -238,6 +255,12 @@ int ref_fft_c2r(int Nx, int Ny, int Nz, int c, const double* in_c128, double* ou
     fftw_execute(p);
     fftw_destroy_plan(p);
     return 0;
+}
+
+// set-up and solve wall times (seconds) of the last ref_mech_run / ref_therm_run
+void ref_last_timing(double* setup_s, double* run_s) {
+    if (setup_s) *setup_s = g_setup_s;
+    if (run_s) *run_s = g_run_s;
 }
 
 }  // extern "C"

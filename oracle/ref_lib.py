@@ -89,6 +89,13 @@ class RefLib:
                              _p(q), ctypes.byref(sw), ctypes.byref(sch))
         return dict(grad=g.reshape(V, 3).T.copy(), flux=q.reshape(V, 3).T.copy(), sweeps=sw.value, scheme=sch.value)
 
+    def last_timing(self):
+        """(set-up seconds, solve seconds) of the last mech_run / therm_run:
+        constructor + material() + setLoad() versus runAnalysis()."""
+        a, b = ctypes.c_double(), ctypes.c_double()
+        self.L.ref_last_timing(ctypes.byref(a), ctypes.byref(b))
+        return a.value, b.value
+
     def therm_homog(self, shape, km, ki, rve, tol_field, tol_eq):
         Nx, Ny, Nz = shape
         rve = np.ascontiguousarray(np.asarray(rve).ravel(), np.int32)

@@ -30,7 +30,7 @@ def test_exports():
 @pytest.mark.skipif(not os.path.exists(m3d.LIB_PATH), reason="library not built")
 def test_status_strings_and_version():
     L = m3d.load_library()
-    assert L.m3d_abi_version() == 1
+    assert L.m3d_abi_version() == 2
     assert L.m3d_status_string(0) == b"ok"
     assert b"iteration cap" in L.m3d_status_string(4)
 
