@@ -198,8 +198,11 @@ int m3d_thermal_solve_noalloc(int Nx, int Ny, int Nz, double km, double ki, cons
    RVEs of any grid sizes are added, then m3d_batch_homogenize gives each its
    effective tensor, as m3d_homogenize would for it alone (residual stop rule).
    RVEs of one grid size run together as one multi-RVE solve (all their load
-   cases in one graph launch), split only where the device-memory budget
-   requires. */
+   cases in one graph launch); the groups of different grid sizes run
+   concurrently (one host thread and CUDA stream each) when they fit the
+   device-memory budget together, else one after another, each split only
+   where the budget requires.  device_ms is the span from the first group's
+   start to the last group's end on the device. */
 typedef struct m3d_batch m3d_batch;
 typedef struct {
     long long sweeps, sweeps_fp64, sweeps_fp32;  /* summed over all entries (RVE x load case) */
@@ -211,6 +214,7 @@ typedef struct {
     int launches;            /* multi-RVE solves (groups x memory chunks) */
     long long kernel_launches;
     int autotuned;           /* groups whose launch schedule the autotuner picked */
+    int concurrent;          /* 1: the grid-size groups ran at once (one stream each), 0: one after another */
 } m3d_batch_stats;
 /* mem_budget_bytes <= 0: 85% of the free device memory at creation. */
 int m3d_batch_create(int kind, int precision, double mem_budget_bytes, m3d_batch** out);
@@ -302,6 +306,7 @@ typedef struct {
     int G, tzy, tzx;  /* generic kernels: z lines per CTA, y / x tile columns */
     double sweep_us;  /* measured time of one sweep with this schedule */
     int candidates;   /* schedules timed */
+    int slab;         /* 1: two-pass sweeps (x turnaround + y-z slab pass) */
 } m3d_tune;
 int m3d_autotune(m3d_solver* h, int sweeps, m3d_tune* out);
 

@@ -66,12 +66,13 @@ class BatchStats(ctypes.Structure):
                 ("sweeps_fp32", ctypes.c_longlong), ("voxel_iters", ctypes.c_longlong),
                 ("device_ms", ctypes.c_double), ("wall_ms", ctypes.c_double), ("rves", ctypes.c_int),
                 ("groups", ctypes.c_int), ("launches", ctypes.c_int), ("kernel_launches", ctypes.c_longlong),
-                ("autotuned", ctypes.c_int)]
+                ("autotuned", ctypes.c_int), ("concurrent", ctypes.c_int)]
 
 
 class Tune(ctypes.Structure):
     _fields_ = [("fast", ctypes.c_int), ("tma_y", ctypes.c_int), ("G", ctypes.c_int), ("tzy", ctypes.c_int),
-                ("tzx", ctypes.c_int), ("sweep_us", ctypes.c_double), ("candidates", ctypes.c_int)]
+                ("tzx", ctypes.c_int), ("sweep_us", ctypes.c_double), ("candidates", ctypes.c_int),
+                ("slab", ctypes.c_int)]
 
 
 class Request(ctypes.Structure):

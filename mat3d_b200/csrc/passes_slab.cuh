@@ -39,14 +39,17 @@
 
 namespace m3d {
 
-constexpr int kSlabThreads = 256;
-
 template <typename T, int N>
 struct SlabGeom {
     typedef typename Cx<T>::t C2;
+    // threads per CTA: 16 warps and one CTA per SM where one CTA can hold the
+    // FP32 128^2 slab with all its z lines in one chunk (the slabs then spread
+    // over the SMs in near-even rounds); 8 warps and two CTAs per SM otherwise
+    static constexpr int NT = (sizeof(T) == 4 && N == 128) ? 512 : 256;
+    static constexpr int MINB = NT == 512 ? 1 : 2;
     static constexpr int E = LineSplit<T, N>::E, TL = LineSplit<T, N>::Tl;
     static constexpr int CPW = 32 / TL;  // columns (y FFTs) or packed lines (z FFTs) per warp
-    static constexpr int NW = kSlabThreads / 32;
+    static constexpr int NW = NT / 32;
     static constexpr int Hz = N / 2 + 1, Hzp = HzOf<N>::Hzp;
     static constexpr int BMOD = sizeof(T) == 4 ? 16 : 8;  // complex elements per bank cycle
     static constexpr int SP = Hzp + ((4 - Hzp % BMOD) + BMOD) % BMOD;  // slab row stride, = 4 mod BMOD
@@ -54,7 +57,10 @@ struct SlabGeom {
     static constexpr int ROW = RowLen<T, N, false>::value, RSW = RowLen<T, N, false>::sw;  // z tile rows
     static constexpr int LPC = NW * CPW;  // packed z lines per chunk
     static constexpr int NPL = N / 2;     // packed lines per slab (rows 2m, 2m+1)
-    static constexpr int NG = (Hz + CPW - 1) / CPW;  // column groups (live columns kz < Hz)
+    // column groups: kz = 0 .. N/2-1, column 0 carrying the DC (kz = 0) and
+    // Nyquist (kz = N/2) columns packed into one complex FFT
+    static constexpr int NG = (N / 2) / CPW;
+    static_assert((N / 2) % CPW == 0, "whole column groups");
     static constexpr size_t s_bytes = (size_t)N * SP * sizeof(C2);
     static constexpr size_t xch_bytes = (size_t)NW * CPW * XS * sizeof(C2);
     static constexpr size_t tile_bytes = (size_t)LPC * ROW * sizeof(C2);
@@ -62,6 +68,9 @@ struct SlabGeom {
     static constexpr size_t smem() {
         return (size_t)N * sizeof(C2) + s_bytes + w_bytes + 64 * sizeof(double) + 3 * kMaxPhases * sizeof(T) + 16;
     }
+    // fits the CTAs per SM it is launched for (227 KB per SM, static shared
+    // memory of the finalize included)
+    static constexpr bool fits() { return smem() <= (MINB == 1 ? (size_t)220 * 1024 : (size_t)110 * 1024); }
     static_assert(SP % 2 == 0, "16-byte aligned slab rows");
     static_assert((Hzp * sizeof(C2)) % 16 == 0, "whole 16-byte copies per row");
 };
@@ -83,54 +92,147 @@ struct SlabOps {
     long long mstride;     // doubles per RVE table block
 };
 
-__device__ __forceinline__ void ld4x(const float* p, float (&o)[4]) {
-    const float4 v = *reinterpret_cast<const float4*>(p);
-    o[0] = v.x; o[1] = v.y; o[2] = v.z; o[3] = v.w;
+// One pointwise item of a chunk: voxels z0, z0+1 of rows 2m and 2m+1, i.e.
+// one 16-byte (FP32) pair of complex tile entries of packed line m.  A warp's
+// items are consecutive pairs of one line, so its tile accesses are
+// contiguous (conflict-free) and its global loads are 256-byte runs.
+template <typename T>
+struct SlabItem {
+    T x[4];       // row 2m: z0, z0+1; row 2m+1: z0, z0+1
+    float r[4];
+    uint32_t p;   // the four phase ids, one byte each
+};
+__device__ __forceinline__ void ld2(const float* p, float& a, float& b) {
+    const float2 v = *reinterpret_cast<const float2*>(p);
+    a = v.x; b = v.y;
 }
-__device__ __forceinline__ void ld4x(const double* p, double (&o)[4]) {
-    const double2 a = reinterpret_cast<const double2*>(p)[0], b = reinterpret_cast<const double2*>(p)[1];
-    o[0] = a.x; o[1] = a.y; o[2] = b.x; o[3] = b.y;
+__device__ __forceinline__ void ld2(const double* p, double& a, double& b) {
+    const double2 v = *reinterpret_cast<const double2*>(p);
+    a = v.x; b = v.y;
+}
+__device__ __forceinline__ void st2(float* p, float a, float b) { *reinterpret_cast<float2*>(p) = make_float2(a, b); }
+__device__ __forceinline__ void st2(double* p, double a, double b) {
+    *reinterpret_cast<double2*>(p) = make_double2(a, b);
+}
+// tile pair at z0 (even) of a tile row, its two logical entries (z0, z0+1)
+// in order whatever the row's swizzle (XOR 1)
+__device__ __forceinline__ void tile_get2(const float2* tr, int z0, int sw, float2& a, float2& b) {
+    const float4 v = *reinterpret_cast<const float4*>(tr + z0);
+    a = make_float2(sw ? v.z : v.x, sw ? v.w : v.y);
+    b = make_float2(sw ? v.x : v.z, sw ? v.y : v.w);
+}
+__device__ __forceinline__ void tile_put2(float2* tr, int z0, int sw, float2 a, float2 b) {
+    *reinterpret_cast<float4*>(tr + z0) = sw ? make_float4(b.x, b.y, a.x, a.y) : make_float4(a.x, a.y, b.x, b.y);
+}
+__device__ __forceinline__ void tile_get2(const double2* tr, int z0, int sw, double2& a, double2& b) {
+    a = tr[z0 ^ sw];
+    b = tr[(z0 + 1) ^ sw];
+}
+__device__ __forceinline__ void tile_put2(double2* tr, int z0, int sw, double2 a, double2 b) {
+    tr[z0 ^ sw] = a;
+    tr[(z0 + 1) ^ sw] = b;
 }
 
-// Column FFTs of the slab (all live kz columns, in place, natural order in
-// and out; SIGN < 0 forward, > 0 inverse).
+// Column FFTs of the slab (in place, natural order in and out; SIGN < 0
+// forward, > 0 inverse) over kz = 0 .. N/2, the DC and Nyquist columns
+// sharing one complex FFT (column 0):
+//   forward: both columns are real after the z R2C (their imaginary parts are
+//     exact zeros), so P = S0 + i S_N/2 is transformed and split by Hermitian
+//     symmetry, F0[k] = (F[k] + conj F[-k]) / 2, F_N/2[k] = (F[k] - conj F[-k]) / 2i;
+//   inverse: the z C2R keeps only the real parts of these two columns (FFTW's
+//     c2r semantics), and Re IFFT(S) = IFFT((S[k] + conj S[-k]) / 2), so the
+//     Hermitian parts H0 + i H_N/2 are transformed together and the real and
+//     imaginary parts of the result are the two columns' real parts.
+// The pre- and post-steps are done by the warp that owns column group 0.
 template <typename T, int N, int SIGN>
 __device__ __forceinline__ void slab_columns(typename Cx<T>::t* S, typename Cx<T>::t* W, const typename Cx<T>::t* tw) {
     typedef typename Cx<T>::t C2;
     typedef SlabGeom<T, N> G;
-    constexpr int E = G::E, TL = G::TL, CPW = G::CPW;
+    constexpr int E = G::E, TL = G::TL, CPW = G::CPW, SP = G::SP, H = N / 2;
+    constexpr int KPL = (N + 31) / 32;  // column entries per lane in the pack / split steps
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int col = lane % CPW, t = lane / CPW;
     C2* xl = W + (warp * CPW + col) * G::XS;
     const int sw = G::XSW ? (col & 1) : 0;
 #pragma unroll 1
     for (int gi = warp; gi < G::NG; gi += G::NW) {
-        const int kz = gi * CPW + col;
-        const bool ok = kz < G::Hz;
-        C2* base = S + (ok ? kz : 0);
+        if (gi == 0) {  // pack the DC and Nyquist columns into column 0
+            if constexpr (SIGN < 0) {
+#pragma unroll
+                for (int q = 0; q < KPL; ++q) {
+                    const int y = lane + 32 * q;
+                    if (y < N) S[y * SP] = mk<C2>(S[y * SP].x, S[y * SP + H].x);
+                }
+            } else {
+                C2 pk[KPL];
+#pragma unroll
+                for (int q = 0; q < KPL; ++q) {
+                    const int k = min(lane + 32 * q, N - 1), km = (N - k) % N;
+                    const C2 a = S[k * SP], a2 = S[km * SP], b = S[k * SP + H], b2 = S[km * SP + H];
+                    const C2 h0 = mk<C2>((T)0.5 * (a.x + a2.x), (T)0.5 * (a.y - a2.y));
+                    const C2 hn = mk<C2>((T)0.5 * (b.x + b2.x), (T)0.5 * (b.y - b2.y));
+                    pk[q] = mk<C2>(h0.x - hn.y, h0.y + hn.x);
+                }
+                __syncwarp();
+#pragma unroll
+                for (int q = 0; q < KPL; ++q)
+                    if (lane + 32 * q < N) S[(lane + 32 * q) * SP] = pk[q];
+            }
+            __syncwarp();
+        }
+        C2* base = S + gi * CPW + col;
         C2 v[E];
         if constexpr (SIGN < 0) {
 #pragma unroll
-            for (int j = 0; j < E; ++j) v[j] = ok ? base[(t + TL * j) * G::SP] : mk<C2>(0, 0);
+            for (int j = 0; j < E; ++j) v[j] = base[(t + TL * j) * SP];
             line_fwd<C2, E, TL>(v, t, xl, tw, sw);
-            if (ok) {
 #pragma unroll
-                for (int r = 0; r < E; ++r) base[spec_mode<E, TL>(t, r) * G::SP] = v[r];
-            }
+            for (int r = 0; r < E; ++r) base[spec_mode<E, TL>(t, r) * SP] = v[r];
         } else {
 #pragma unroll
-            for (int r = 0; r < E; ++r) v[r] = ok ? base[spec_mode<E, TL>(t, r) * G::SP] : mk<C2>(0, 0);
+            for (int r = 0; r < E; ++r) v[r] = base[spec_mode<E, TL>(t, r) * SP];
             line_inv<C2, E, TL>(v, t, xl, tw, sw);
-            if (ok) {
 #pragma unroll
-                for (int j = 0; j < E; ++j) base[(t + TL * j) * G::SP] = v[j];
+            for (int j = 0; j < E; ++j) base[(t + TL * j) * SP] = v[j];
+        }
+        if (gi == 0) {  // unpack column 0 into the DC and Nyquist columns
+            __syncwarp();
+            if constexpr (SIGN < 0) {
+                C2 f0[KPL], fn[KPL];
+#pragma unroll
+                for (int q = 0; q < KPL; ++q) {
+                    const int k = min(lane + 32 * q, N - 1), km = (N - k) % N;
+                    const C2 F = S[k * SP], Fm = S[km * SP];
+                    f0[q] = mk<C2>((T)0.5 * (F.x + Fm.x), (T)0.5 * (F.y - Fm.y));
+                    fn[q] = mk<C2>((T)0.5 * (F.y + Fm.y), (T)-0.5 * (F.x - Fm.x));
+                }
+                __syncwarp();
+#pragma unroll
+                for (int q = 0; q < KPL; ++q) {
+                    const int k = lane + 32 * q;
+                    if (k < N) {
+                        S[k * SP] = f0[q];
+                        S[k * SP + H] = fn[q];
+                    }
+                }
+            } else {
+#pragma unroll
+                for (int q = 0; q < KPL; ++q) {
+                    const int y = lane + 32 * q;
+                    if (y < N) {
+                        const C2 pv = S[y * SP];
+                        S[y * SP] = mk<C2>(pv.x, (T)0);
+                        S[y * SP + H] = mk<C2>(pv.y, (T)0);
+                    }
+                }
             }
+            __syncwarp();
         }
     }
 }
 
 template <typename T, int N, bool MIX, class Fin>
-__global__ void __launch_bounds__(kSlabThreads, 2)
+__global__ void __launch_bounds__(SlabGeom<T, N>::NT, SlabGeom<T, N>::MINB)
     k_slab(GridDims g, const typename Cx<T>::t* __restrict__ twz, typename Cx<T>::t* __restrict__ spec, SlabOps<T> ops,
            Ctl* ctl, double* partials, Fin fin) {
     typedef typename Cx<T>::t C2;
@@ -168,7 +270,7 @@ __global__ void __launch_bounds__(kSlabThreads, 2)
     for (int i = threadIdx.x; i < N; i += blockDim.x) tw[i] = twz[i];
     constexpr int CPR = (int)(G::Hzp * sizeof(C2) / 16);  // 16-byte copies per slab row
     if constexpr (MIX) {
-        for (int i = threadIdx.x; i < N * CPR; i += kSlabThreads) {
+        for (int i = threadIdx.x; i < N * CPR; i += G::NT) {
             const int row = i / CPR, q = i - row * CPR;
             cp_async((char*)(S + row * SP) + q * 16, (const char*)(gs + (long long)row * G::Hzp) + q * 16, 16, 16);
         }
@@ -185,6 +287,62 @@ __global__ void __launch_bounds__(kSlabThreads, 2)
     const T invV = (T)(1.0 / (double)g.V);
     const double wt = (C == 6 && c >= 3) ? 2.0 : 1.0;
     double acc[2] = {0.0, 0.0};
+    // pointwise items of a chunk per thread; the first PRE are loaded before
+    // the chunk's z inverse (their latency hidden by it), the rest after it
+    constexpr int HP = N / 2;  // z pairs per line
+    constexpr int IPT = (G::LPC * HP + G::NT - 1) / G::NT;
+    constexpr int PRE = MIX ? ((sizeof(T) == 4 && E < 16) ? IPT / 2 : IPT / 4) : 0;
+    auto load_item = [&](int it, int m0, SlabItem<T>& q) {
+        const int i = threadIdx.x + it * G::NT;
+        const int li = i / HP, z0 = 2 * (i - li * HP);
+        if (li >= G::LPC || m0 + li >= G::NPL) return;
+        const long long vo = (long long)(2 * (m0 + li)) * N + z0;
+        ld2(xs + vo, q.x[0], q.x[1]);
+        ld2(xs + vo + N, q.x[2], q.x[3]);
+        const uint32_t pa = *reinterpret_cast<const uint16_t*>(ph + vo);
+        const uint32_t pb = *reinterpret_cast<const uint16_t*>(ph + vo + N);
+        q.p = pa | (pb << 16);
+        if (MIX) {
+            if (rs) {
+                ld2(rs + vo, q.r[0], q.r[1]);
+                ld2(rs + vo + N, q.r[2], q.r[3]);
+            } else {
+                q.r[0] = q.r[1] = q.r[2] = q.r[3] = 0.f;
+            }
+        }
+    };
+    // (MIX) EM update x += A (x_c + r - x) with the residual partials; then
+    // the polarization P x of the (new) state, written into the tile
+    auto point_item = [&](int it, int m0, const SlabItem<T>& q) {
+        const int i = threadIdx.x + it * G::NT;
+        const int li = i / HP, z0 = 2 * (i - li * HP);
+        if (li >= G::LPC || m0 + li >= G::NPL) return;
+        C2* tr = W + li * ROW;
+        const int tsw = (li & 1) * G::RSW;
+        T v[4];
+#pragma unroll
+        for (int w = 0; w < 4; ++w) v[w] = q.x[w];
+        if constexpr (MIX) {
+            C2 a, bq;
+            tile_get2(tr, z0, tsw, a, bq);
+            const T xc[4] = {a.x, bq.x, a.y, bq.y};
+#pragma unroll
+            for (int w = 0; w < 4; ++w) {
+                const int pw = (q.p >> (8 * w)) & 0xff;
+                const T d = (xc[w] * invV + (T)q.r[w]) - q.x[w];
+                acc[0] += wt * (double)d * (double)d;
+                v[w] = q.x[w] + ca[pw] * d;
+                acc[1] += (double)co[pw] * (double)v[w];
+            }
+            const long long vo = (long long)(2 * (m0 + li)) * N + z0;
+            st2(xs + vo, v[0], v[1]);
+            st2(xs + vo + N, v[2], v[3]);
+        }
+        T pol[4];
+#pragma unroll
+        for (int w = 0; w < 4; ++w) pol[w] = cp[(q.p >> (8 * w)) & 0xff] * v[w];
+        tile_put2(tr, z0, tsw, mk<C2>(pol[0], pol[2]), mk<C2>(pol[1], pol[3]));
+    };
 #pragma unroll 1
     for (int m0 = 0; m0 < G::NPL; m0 += G::LPC) {
         const int li = warp * CPW + lw;  // this lane's packed line within the chunk
@@ -192,7 +350,10 @@ __global__ void __launch_bounds__(kSlabThreads, 2)
         const bool live = m < G::NPL;
         C2* row = W + li * ROW;
         const int sw = (li & 1) * G::RSW;
+        SlabItem<T> pre[PRE > 0 ? PRE : 1];
         if constexpr (MIX) {
+#pragma unroll
+            for (int it = 0; it < PRE; ++it) load_item(it, m0, pre[it]);
             // z inverse: the line's spectrum (rows 2m + i 2m+1) assembled from the
             // two stored half spectra as the lanes load it (Hermitian extension)
             const C2* ra = S + (live ? 2 * m : 0) * SP;
@@ -214,48 +375,14 @@ __global__ void __launch_bounds__(kSlabThreads, 2)
             for (int j = 0; j < E; ++j) row[(t + TL * j) ^ sw] = v[j];
         }
         __syncthreads();
-        // pointwise: (MIX) EM update x += A (x_c + r - x) with the residual
-        // partials, then the polarization P x of the (new) state into the tile
         {
-            const int rows = min(2 * G::LPC, N - 2 * m0);
-            const int nq = rows * N / 4;
-#pragma unroll 1
-            for (int i4 = threadIdx.x; i4 < nq; i4 += kSlabThreads) {
-                const int i = i4 * 4;
-                const int yl = i / N, z0 = i - yl * N;
-                const long long vo = (long long)(2 * m0 + yl) * N + z0;
-                const int lt = yl >> 1, odd = yl & 1;
-                C2* tr = W + lt * ROW;
-                const int tsw = (lt & 1) * G::RSW;
-                T xv[4];
-                ld4x(xs + vo, xv);
-                const uchar4 p4 = *reinterpret_cast<const uchar4*>(ph + vo);
-                const int pp[4] = {p4.x, p4.y, p4.z, p4.w};
-                if constexpr (MIX) {
-                    float rv[4] = {0.f, 0.f, 0.f, 0.f};
-                    if (rs) ld4x(rs + vo, rv);
-                    T xn[4];
+            SlabItem<T> rest[IPT - PRE > 0 ? IPT - PRE : 1];
 #pragma unroll
-                    for (int w = 0; w < 4; ++w) {
-                        const C2 u = tr[(z0 + w) ^ tsw];
-                        const T xc = (odd ? u.y : u.x) * invV;
-                        const T d = (xc + (T)rv[w]) - xv[w];
-                        acc[0] += wt * (double)d * (double)d;
-                        xn[w] = xv[w] + ca[pp[w]] * d;
-                        acc[1] += (double)co[pp[w]] * (double)xn[w];
-                    }
-                    if constexpr (sizeof(T) == 4) {
-                        *reinterpret_cast<float4*>(xs + vo) = make_float4(xn[0], xn[1], xn[2], xn[3]);
-                    } else {
-                        reinterpret_cast<double2*>(xs + vo)[0] = make_double2(xn[0], xn[1]);
-                        reinterpret_cast<double2*>(xs + vo)[1] = make_double2(xn[2], xn[3]);
-                    }
+            for (int it = PRE; it < IPT; ++it) load_item(it, m0, rest[it - PRE]);
 #pragma unroll
-                    for (int w = 0; w < 4; ++w) xv[w] = xn[w];
-                }
+            for (int it = 0; it < PRE; ++it) point_item(it, m0, pre[it]);
 #pragma unroll
-                for (int w = 0; w < 4; ++w) reinterpret_cast<T*>(&tr[(z0 + w) ^ tsw])[odd] = cp[pp[w]] * xv[w];
-            }
+            for (int it = PRE; it < IPT; ++it) point_item(it, m0, rest[it - PRE]);
         }
         __syncthreads();
         // z forward of the packed lines; each row is split into the two rows'
@@ -290,7 +417,7 @@ __global__ void __launch_bounds__(kSlabThreads, 2)
     }
     slab_columns<T, N, -1>(S, W, tw);
     __syncthreads();
-    for (int i = threadIdx.x; i < N * CPR; i += kSlabThreads) {
+    for (int i = threadIdx.x; i < N * CPR; i += G::NT) {
         const int row = i / CPR, q = i - row * CPR;
         *reinterpret_cast<float4*>((char*)(gs + (long long)row * G::Hzp) + q * 16) =
             *reinterpret_cast<const float4*>((const char*)(S + row * SP) + q * 16);

@@ -603,16 +603,20 @@ enum Policy {
 
 // tot[s] = sum over the nblk block partials of sum s, in a fixed order (every
 // thread strides the same blocks, then a fixed tree) -> bit-reproducible.
-// Called by all threads of a block of at most 256 threads (power of two).
+// Called by all threads of a block whose size is a power of two; the first
+// min(blockDim.x, 256) threads take part (red holds 256 doubles).
 __device__ __forceinline__ void sum_partials(const double* partials, int NS, int nblk, int b, double* red,
                                              double* tot) {
+    const int nt = blockDim.x < 256 ? (int)blockDim.x : 256;
     for (int s = 0; s < NS; ++s) {
-        double t = 0;
         const double* p = partials + ((long long)b * NS + s) * nblk;
-        for (int i = threadIdx.x; i < nblk; i += blockDim.x) t += __ldcg(p + i);
-        red[threadIdx.x] = t;
+        if (threadIdx.x < nt) {
+            double t = 0;
+            for (int i = threadIdx.x; i < nblk; i += nt) t += __ldcg(p + i);
+            red[threadIdx.x] = t;
+        }
         __syncthreads();
-        for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+        for (int o = nt / 2; o > 0; o >>= 1) {
             if (threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
             __syncthreads();
         }

@@ -748,7 +748,7 @@ int m3d_solver::launch_em(Ctl* ctl, T* x, const float* r, typename Cx<T>::t* sp,
 // CTAs per SM.
 template <typename T, int NN>
 constexpr bool slab_fits() {
-    return SlabGeom<T, NN>::smem() <= (size_t)110 * 1024;
+    return SlabGeom<T, NN>::fits();
 }
 
 template <typename T>
@@ -770,7 +770,7 @@ int m3d_solver::pass_slab(Ctl* ctl, T* x, const float* r, typename Cx<T>::t* sp,
         if constexpr (slab_fits<T, NN>()) {
             auto kern = k_slab<T, NN, MIX, Fin>;
             allow_smem(kern);
-            kern<<<dim3(CC * Nx, B), kSlabThreads, SlabGeom<T, NN>::smem(), stream>>>(g, tw<T>(2), sp, ops, ctl,
+            kern<<<dim3(CC * Nx, B), SlabGeom<T, NN>::NT, SlabGeom<T, NN>::smem(), stream>>>(g, tw<T>(2), sp, ops, ctl,
                                                                                       d_part, fin);
             done = true;
         }
@@ -1852,9 +1852,15 @@ int m3d_solver::tune_time(int sweeps, float* ms) {
     cudaEvent_t e0, e1;
     M3D_CUDA(cudaEventCreate(&e0));
     M3D_CUDA(cudaEventCreate(&e1));
-    rc = launch_em<T, CC>(d_ctl, x, r, sp, 0, POL_RESIDUAL, nullptr);  // warm-up (attributes, tensor maps)
+    const bool slab = slab_ok<T>();
+    auto sweep = [&]() {
+        return slab ? launch_em_slab<T, CC>(d_ctl, x, r, sp, 0, POL_RESIDUAL, nullptr)
+                    : launch_em<T, CC>(d_ctl, x, r, sp, 0, POL_RESIDUAL, nullptr);
+    };
+    if (slab) rc = pass_slab<T, CC, false>(d_ctl, x, nullptr, sp, FinNone{});
+    if (!rc) rc = sweep();  // warm-up (attributes, tensor maps)
     cudaEventRecord(e0, stream);
-    for (int k = 0; k < sweeps && !rc; ++k) rc = launch_em<T, CC>(d_ctl, x, r, sp, 0, POL_RESIDUAL, nullptr);
+    for (int k = 0; k < sweeps && !rc; ++k) rc = sweep();
     cudaEventRecord(e1, stream);
     cudaError_t e = cudaEventSynchronize(e1);
     if (!rc && e == cudaSuccess) cudaEventElapsedTime(ms, e0, e1);
@@ -1872,27 +1878,35 @@ int m3d_solver::autotune(int sweeps, m3d_tune* out) {
     const int G0 = fp64 ? G64 : G32, Y0 = fp64 ? TZy64 : TZy32, X0 = fp64 ? TZx64 : TZx32;  // heuristic tiles
     const size_t lim = 200 * 1024;
     if (fast_ok) {
-        // compile-time kernels with either y pass, and the generic kernels with their default tiles
-        cand.push_back(m3d_tune{1, 0, G0, Y0, X0, 0, 0});
-        cand.push_back(m3d_tune{1, 1, G0, Y0, X0, 0, 0});
-        cand.push_back(m3d_tune{0, 0, G0, Y0, X0, 0, 0});
+        // compile-time kernels with either y pass, the two-pass sweep where the
+        // operators allow it, and the generic kernels with their default tiles
+        cand.push_back(m3d_tune{1, 0, G0, Y0, X0, 0, 0, 0});
+        cand.push_back(m3d_tune{1, 1, G0, Y0, X0, 0, 0, 0});
+        const bool f1 = use_fast, s1 = use_slab;
+        use_fast = use_slab = true;
+        const bool slab_possible = fp64 ? slab_ok<double>() : slab_ok<float>();
+        use_fast = f1;
+        use_slab = s1;
+        if (slab_possible) cand.push_back(m3d_tune{1, 0, G0, Y0, X0, 0, 0, 1});
+        cand.push_back(m3d_tune{0, 0, G0, Y0, X0, 0, 0, 0});
     } else {
         // generic kernels: every tile size whose shared memory fits comfortably
         for (int Gv : {2, 4, 8, 16}) {
             if ((size_t)Nz * csz * (1 + (size_t)Gv * C) + 32 * 32 * 8 + op_smem<double, 6>() > lim) continue;
             for (int tz : {2, 4, 8, 16}) {
                 if (2 * (size_t)C * Nx * tz * csz + (size_t)Nx * csz > lim || 2 * (size_t)Ny * tz * csz > lim) continue;
-                cand.push_back(m3d_tune{0, 0, Gv, tz, tz, 0, 0});
+                cand.push_back(m3d_tune{0, 0, Gv, tz, tz, 0, 0, 0});
             }
         }
     }
-    const bool f0 = use_fast, t0 = use_tma_y;
+    const bool f0 = use_fast, t0 = use_tma_y, sl0 = use_slab;
     const int g32 = G32, g64 = G64, y32 = TZy32, y64 = TZy64, x32 = TZx32, x64 = TZx64;
     int best = -1;
     for (size_t i = 0; i < cand.size(); ++i) {
         m3d_tune& c = cand[i];
         use_fast = c.fast != 0;
         use_tma_y = c.tma_y != 0;
+        use_slab = c.slab != 0;
         (fp64 ? G64 : G32) = c.G;
         (fp64 ? TZy64 : TZy32) = c.tzy;
         (fp64 ? TZx64 : TZx32) = c.tzx;
@@ -1906,7 +1920,7 @@ int m3d_solver::autotune(int sweeps, m3d_tune* out) {
         c.sweep_us = 1000.0 * ms / sweeps;
         if (best < 0 || c.sweep_us < cand[best].sweep_us) best = (int)i;
     }
-    use_fast = f0; use_tma_y = t0;
+    use_fast = f0; use_tma_y = t0; use_slab = sl0;
     G32 = g32; G64 = g64; TZy32 = y32; TZy64 = y64; TZx32 = x32; TZx64 = x64;
     drop_graphs();
     if (best < 0) return fail(M3D_ERR_CUDA, "autotune: no candidate ran");
@@ -1942,6 +1956,7 @@ int m3d_autotune(m3d_solver* h, int sweeps, m3d_tune* out) {
     const bool fp64 = (h->prec == M3D_PREC_FP64);
     h->use_fast = t.fast != 0;
     h->use_tma_y = t.tma_y != 0;
+    h->use_slab = t.slab != 0;
     (fp64 ? h->G64 : h->G32) = t.G;
     (fp64 ? h->TZy64 : h->TZy32) = t.tzy;
     (fp64 ? h->TZx64 : h->TZx32) = t.tzx;

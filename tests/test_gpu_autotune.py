@@ -39,7 +39,8 @@ def test_tuned_schedule_matches_default(shape, prec):
     assert np.abs(C1 - C0).max() / np.abs(C0).max() < 1e-8
     # a later handle of the same shape reuses the remembered schedule without timing
     C2, t2 = homog(shape, prec, 0)
-    assert {k: t2[k] for k in ("fast", "tma_y", "G", "tzy", "tzx")} == {k: t[k] for k in ("fast", "tma_y", "G", "tzy", "tzx")}
+    keys = ("fast", "tma_y", "G", "tzy", "tzx", "slab")
+    assert {k: t2[k] for k in keys} == {k: t[k] for k in keys}
     assert np.array_equal(C2, C1)
 
 

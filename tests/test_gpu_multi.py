@@ -180,6 +180,9 @@ def test_batch_api_equals_single(kind, prec, budget_rves):
     st = bt.stats()
     assert st["rves"] == len(members) and st["groups"] == 3
     assert (st["launches"] >= 5) if budget_rves else (st["launches"] == 3)
+    # with the whole batch in budget the three grid sizes run at once (own
+    # threads and streams); a one-RVE budget runs them one after another
+    assert st["concurrent"] == (0 if budget_rves else 1)
     assert st["voxel_iters"] > 0 and st["device_ms"] > 0
     for i, (shape, mat, rve) in enumerate(members):
         s1 = m3d.Solver(kind, *shape, 0, prec, C)
