@@ -148,6 +148,11 @@ int m3d_get_field(m3d_solver* h, int which, int b, double* out);
 /* Volume averages of the strain-like and stress-like fields of entry b. */
 int m3d_get_means(m3d_solver* h, int b, double* strain_mean, double* stress_mean);
 int m3d_get_stats(const m3d_solver* h, m3d_stats* out);
+/* Entry b's own result of the last linear run (no counterpart in the reference,
+   which solves one load case per object): its sweep count (for FP32+FP64
+   refinement: FP64 defect sweeps, while *sweeps adds its FP32 sweeps), final
+   residual and status. */
+int m3d_get_entry_stats(const m3d_solver* h, int b, int* iters, long long* sweeps, double* residual, int* status);
 /* Per-increment averages of the ep/ed path (prop_homogenized, nInc x 9). */
 int m3d_get_increments(const m3d_solver* h, double* out, int max_rows);
 
@@ -273,6 +278,8 @@ typedef struct {
     int queued, running, peak_running;
     int resident_solvers;        /* solvers held (running + idle) */
     double resident_bytes, budget_bytes;
+    long long merged_solves;     /* solves that ran several requests as one multi-RVE batch */
+    long long merged_requests;   /* requests served by those solves */
 } m3d_serve_stats;
 /* mem_budget_bytes <= 0: 85% of the free device memory; workers: concurrent solves. */
 int m3d_serve_create(double mem_budget_bytes, int workers, m3d_server** out);

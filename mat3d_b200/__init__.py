@@ -100,7 +100,8 @@ class ServeStats(ctypes.Structure):
     _fields_ = [("submitted", ctypes.c_longlong), ("completed", ctypes.c_longlong), ("failed", ctypes.c_longlong),
                 ("queued", ctypes.c_int), ("running", ctypes.c_int), ("peak_running", ctypes.c_int),
                 ("resident_solvers", ctypes.c_int), ("resident_bytes", ctypes.c_double),
-                ("budget_bytes", ctypes.c_double)]
+                ("budget_bytes", ctypes.c_double), ("merged_solves", ctypes.c_longlong),
+                ("merged_requests", ctypes.c_longlong)]
 
 
 class Profile(ctypes.Structure):
@@ -116,7 +117,7 @@ EXPORTS = [
     "m3d_create", "m3d_destroy", "m3d_set_material_mech", "m3d_set_material_thermal", "m3d_set_load", "m3d_run",
     "m3d_homogenize", "m3d_get_field", "m3d_get_means", "m3d_get_stats", "m3d_get_increments",
     "m3d_status_string", "m3d_last_error", "m3d_abi_version", "m3d_get_stream", "m3d_set_stream",
-    "m3d_set_profiling", "m3d_get_profile", "m3d_thermal_solve_noalloc",
+    "m3d_set_profiling", "m3d_get_profile", "m3d_thermal_solve_noalloc", "m3d_get_entry_stats",
     "m3d_create_multi", "m3d_set_material_mech_rve", "m3d_set_material_thermal_rve", "m3d_footprint_bytes",
     "m3d_batch_create", "m3d_batch_add_mech", "m3d_batch_add_thermal", "m3d_batch_homogenize",
     "m3d_batch_get_stats", "m3d_batch_clear", "m3d_batch_destroy",
@@ -154,6 +155,8 @@ def load_library(path: str | None = None):
     L.m3d_get_means.argtypes = [vp, i, vp, vp]
     L.m3d_get_stats.argtypes = [vp, ctypes.POINTER(Stats)]
     L.m3d_get_increments.argtypes = [vp, vp, i]
+    L.m3d_get_entry_stats.argtypes = [vp, i, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_longlong),
+                                      ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int)]
     L.m3d_status_string.restype = ctypes.c_char_p
     L.m3d_status_string.argtypes = [i]
     L.m3d_last_error.restype = ctypes.c_char_p
@@ -328,6 +331,13 @@ class Solver:
         st = Stats()
         _check(self.L, self.L.m3d_get_stats(self.h, ctypes.byref(st)), "get_stats")
         return st.as_dict()
+
+    def entry_stats(self, b):
+        """Batch entry b's own iterations, sweeps, residual and status of the last run."""
+        it, sw, res, stt = ctypes.c_int(), ctypes.c_longlong(), ctypes.c_double(), ctypes.c_int()
+        _check(self.L, self.L.m3d_get_entry_stats(self.h, b, ctypes.byref(it), ctypes.byref(sw), ctypes.byref(res),
+                                                  ctypes.byref(stt)), "get_entry_stats")
+        return {"iters": it.value, "sweeps": sw.value, "residual": res.value, "status": stt.value}
 
     def autotune(self, sweeps=3):
         """Time the launch schedules and keep the fastest (sweeps = 0: apply

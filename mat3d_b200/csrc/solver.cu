@@ -881,6 +881,7 @@ int m3d_solver::run_refine(double tol_field, int max_iter) {
     const int chunk = 8;
     const bool slab = slab_ok<float>();
     st.passes_per_sweep = slab ? 2 : 5;
+    std::vector<long long> in32((size_t)B, 0);  // FP32 sweeps per entry
     for (;;) {
         ProRefine64<CC> pro = tab(ProRefine64<CC>{d_phase, x, first ? nullptr : d_delta, g.V, dm(off_P), nph_max(), nullptr});
         EpiDefect<CC> epi = tab(EpiDefect<CC>{d_phase, x, d_r32, g.V, dm(off_Os), nph_max(), nullptr});
@@ -928,9 +929,15 @@ int m3d_solver::run_refine(double tol_field, int max_iter) {
             for (int b = 0; b < B; ++b) alli = alli && h_ctl[b].done;
             if (alli) break;
         }
-        for (int b = 0; b < B; ++b) n32 += h_ctl[b].iters;
+        for (int b = 0; b < B; ++b) {
+            n32 += h_ctl[b].iters;
+            in32[b] += h_ctl[b].iters;
+        }
     }
-    for (int b = 0; b < B; ++b) n64 += h_ctl[b].iters;
+    for (int b = 0; b < B; ++b) {
+        n64 += h_ctl[b].iters;
+        h_ctl[b].aux[1] = (double)in32[b];  // as the graph-captured loop counts them (m3d_get_entry_stats)
+    }
     int status = M3D_OK;
     for (int b = 0; b < B; ++b) {
         if (h_ctl[b].status == 1 && status == M3D_OK) status = M3D_NOT_CONVERGED;
@@ -1998,6 +2005,18 @@ int m3d_set_stream(m3d_solver* h, void* s) {
 int m3d_get_stats(const m3d_solver* h, m3d_stats* out) {
     if (!h || !out) return fail(M3D_ERR_ARG, "NULL argument");
     *out = h->st;
+    return M3D_OK;
+}
+
+int m3d_get_entry_stats(const m3d_solver* h, int b, int* iters, long long* sweeps, double* residual, int* status) {
+    if (!h) return fail(M3D_ERR_ARG, "NULL handle");
+    if (b < 0 || b >= h->B || !h->h_ctl) return fail(M3D_ERR_ARG, "batch entry out of range");
+    const Ctl& c = h->h_ctl[b];
+    if (iters) *iters = c.iters;
+    // the refinement's control block counts its FP64 sweeps, its inner FP32 sweeps in aux[1]
+    if (sweeps) *sweeps = (long long)c.iters + (h->prec == M3D_PREC_FP32_REFINE ? (long long)c.aux[1] : 0);
+    if (residual) *residual = c.residual;
+    if (status) *status = c.status == 2 ? M3D_ERR_NAN : (c.status == 1 ? M3D_NOT_CONVERGED : M3D_OK);
     return M3D_OK;
 }
 

@@ -1,7 +1,9 @@
 """Serving loop (m3d_serve_*): requests of mixed kinds, behaviours and grid
 sizes submitted from several host threads run concurrently on the device,
-and every result equals the same request served alone (bitwise: each request
-runs on its own solver and stream)."""
+and every result equals the same request served alone, bitwise: a request
+runs on its own solver, or as one entry of a multi-RVE solve shared with
+queued requests of the same shape and stop rule, whose entries compute
+exactly what they would alone."""
 import threading
 
 import numpy as np
@@ -121,6 +123,30 @@ def test_budget_admission_serialises_and_matches():
     st = srv.stats()
     assert st["peak_running"] == 1  # one footprint at a time fits
     assert st["resident_bytes"] <= st["budget_bytes"]
+    srv.close()
+    check_same(mixed, serve_alone(reqs))
+
+
+def test_same_shape_requests_merge_and_match():
+    """Linear requests of one shape queued together run as multi-RVE solves
+    (continuous batching); each result is still bitwise the request alone."""
+    reqs = []
+    for i in range(10):
+        if i % 2 == 0:
+            reqs.append(dict(kind=m3d.KIND_THERMAL, shape=(32,) * 3, phase=sphere_rve(32, 6.0 + i / 2, i % 3),
+                             E=[0, 0.2 * (i % 3), 1.0], km=1.0, ki=5.0 + 10 * i, precision="fp32_refine", tol=1e-7,
+                             keep_field=(i % 4 == 0)))
+        else:
+            reqs.append(dict(kind=m3d.KIND_MECH, shape=(24,) * 3, phase=sphere_rve(24, 4.0 + i / 3), E=[1e-3, 0, 0, 0, 0, 0],
+                             mat=MAT_E, precision="fp64", tol=1e-8, keep_field=(i % 3 == 0)))
+    srv = m3d.Server(workers=1)
+    blocker = submit(srv, dict(kind=m3d.KIND_THERMAL, shape=(64,) * 3, phase=sphere_rve(64, 20.0), E=[0, 0, 1.0],
+                               km=1.0, ki=50.0, precision="fp64", tol=1e-10))
+    tickets = [submit(srv, q) for q in reqs]  # queued behind the blocker, then merged by shape
+    srv.wait(blocker, 120000.0)
+    mixed = collect(srv, tickets, reqs)
+    st = srv.stats()
+    assert st["failed"] == 0 and st["merged_solves"] >= 2 and st["merged_requests"] >= 4
     srv.close()
     check_same(mixed, serve_alone(reqs))
 
