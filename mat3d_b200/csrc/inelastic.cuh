@@ -114,15 +114,17 @@ struct InelasticPtrs {
     int* nr_fail;
 };
 
-// constitutive from the current eps; sums (NSUM=13): sig (6), eps (6), 0
+// constitutive from the current eps; sums (NSUM=13): sig (6), eps (6), 0.
+// The state is FP64 in both precisions; T is the transforms' type (the
+// strain increment xc arrives in it).
 template <typename T>
 struct EpiConstitutive {
     static constexpr int NSUM = 13;
-    InelasticPtrs<T> p;
+    InelasticPtrs<double> p;
     PhaseMech* sm;
     // entry-bound base pointers (bind)
-    T *eb = nullptr, *sb = nullptr, *db = nullptr;
-    const T *eob = nullptr, *sob = nullptr, *epb = nullptr;
+    double *eb = nullptr, *sb = nullptr, *db = nullptr;
+    const double *eob = nullptr, *sob = nullptr, *epb = nullptr;
     __device__ __forceinline__ void bind(int b) {
         const long long o6 = (long long)b * 6 * p.V, o1 = (long long)b * p.V;
         eb = p.eps + o6;
@@ -162,14 +164,14 @@ struct EpiConstitutive {
             double phi;
             j2_update(P, e, eo, so, (double)epb[v], sg, phi, p.nr_fail);
         } else {
-            double d = (double)db[v];
+            double d = db[v];
             damage_update(P, e, d, sg);
-            db[v] = (T)d;
+            db[v] = d;
         }
 #pragma unroll
         for (int c = 0; c < 6; ++c) {
-            eb[c * V + v] = (T)e[c];
-            sb[c * V + v] = (T)sg[c];
+            eb[c * V + v] = e[c];
+            sb[c * V + v] = sg[c];
             acc[c] += sg[c];
             acc[6 + c] += e[c];
         }
@@ -177,28 +179,39 @@ struct EpiConstitutive {
     }
 };
 
-// prologue: the stress field itself
+// prologue: the stress field (FP64 state) in the transforms' type, or, with
+// sig_old set, the stress increment of the load step sig - sig_old.  The
+// increment form (FP32 transforms under the residual stop rule): sig_old is
+// the previous step's equilibrated stress, so -Gamma0 (sig - sig_old)^ is the
+// same strain update up to that step's residual, while the FP32 rounding of
+// the transform scales with the increment instead of the total stress (which
+// grows with every load step).
 template <typename T>
 struct ProStress {
     static constexpr int NSUM = 0;
     static constexpr int kW = 1;  // scalar loads only
-    const T* sig;
+    const double* sig;
     long long V;
-    const T* sb = nullptr;
+    const double* sig_old = nullptr;
+    const double* sb = nullptr;
+    const double* sob = nullptr;
     struct Pre {
-        T s[6];
+        double s[6];
     };
-    __device__ __forceinline__ void bind(int b) { sb = sig + (long long)b * 6 * V; }
+    __device__ __forceinline__ void bind(int b) {
+        sb = sig + (long long)b * 6 * V;
+        sob = sig_old ? sig_old + (long long)b * 6 * V : nullptr;
+    }
     __device__ __forceinline__ void load_smem(char*, int = 0) {}
     __device__ __forceinline__ Pre load(int, long long v) const {
         Pre q;
 #pragma unroll
-        for (int c = 0; c < 6; ++c) q.s[c] = sb[c * V + v];
+        for (int c = 0; c < 6; ++c) q.s[c] = sob ? sb[c * V + v] - sob[c * V + v] : sb[c * V + v];
         return q;
     }
     __device__ __forceinline__ void eval_pre(const Pre& q, int, long long, T (&out)[6]) const {
 #pragma unroll
-        for (int c = 0; c < 6; ++c) out[c] = q.s[c];
+        for (int c = 0; c < 6; ++c) out[c] = (T)q.s[c];
     }
     __device__ __forceinline__ void eval(int b, long long v, T (&out)[6], double*) const { eval_pre(load(b, v), b, v, out); }
 };
@@ -257,8 +270,8 @@ __global__ void k_constitutive(EpiConstitutive<T> epi, const Ctl* ctl, double* p
 // Increment commit (export_homogen_var :722-746 then update_old_Variable
 // :693-719): sums of eps_t, sig (6), sig_eff (J2) or d (ed), eps_p; then
 // eps_p += dp where phi > 0, sig_old = sig, eps extrapolation.
-template <typename T>
-__global__ void k_commit(InelasticPtrs<T> p, T* eps_old_w, T* sig_old_w, T* ep_w, int t_comp, double* partials) {
+__global__ void k_commit(InelasticPtrs<double> p, double* eps_old_w, double* sig_old_w, double* ep_w, int t_comp,
+                         double* partials) {
     extern __shared__ __align__(16) char smem_raw[];
     double* red = (double*)smem_raw;
     PhaseMech* sm = (PhaseMech*)(smem_raw + 32 * 32 * sizeof(double));
@@ -297,9 +310,9 @@ __global__ void k_commit(InelasticPtrs<T> p, T* eps_old_w, T* sig_old_w, T* ep_w
                 so[c] = (double)p.sig_old[idx];
             }
             const double dp = j2_update(P, e, eo, so, ep, st, phi, p.nr_fail);
-            if (phi > 0) ep_w[(long long)b * p.V + v] = (T)(ep + dp);
+            if (phi > 0) ep_w[(long long)b * p.V + v] = ep + dp;
 #pragma unroll
-            for (int c = 0; c < 6; ++c) sig_old_w[((long long)b * 6 + c) * p.V + v] = (T)s[c];
+            for (int c = 0; c < 6; ++c) sig_old_w[((long long)b * 6 + c) * p.V + v] = s[c];
         } else {
             acc[7] += (double)p.dmg[(long long)b * p.V + v];
         }
@@ -307,8 +320,8 @@ __global__ void k_commit(InelasticPtrs<T> p, T* eps_old_w, T* sig_old_w, T* ep_w
         for (int c = 0; c < 6; ++c) {
             const long long idx = ((long long)b * 6 + c) * p.V + v;
             const double eo = (double)p.eps_old[idx];
-            eps_old_w[idx] = (T)e[c];
-            p.eps[idx] = (T)(e[c] + (e[c] - eo));
+            eps_old_w[idx] = e[c];
+            p.eps[idx] = e[c] + (e[c] - eo);
         }
     }
     block_reduce_store<9>(acc, red, partials, b, gridDim.x, blockIdx.x);

@@ -150,18 +150,8 @@ constexpr size_t xturn_fast_smem() {
            (size_t)32 * NSUM * sizeof(double);
 }
 
-// CTAs per SM that the x turnaround's shared memory allows (227 KB per SM,
-// 1 KB reserved per CTA); the launch bound lets the registers match it
-template <typename T, int N, int C, int NSUM>
-struct XMinBlocks {
-    static constexpr size_t per = xturn_fast_smem<T, N, C, NSUM>() + 1024;
-    static constexpr int v = (int)((227 * 1024) / per);
-    static constexpr int value = v < 1 ? 1 : (v > 16 ? 16 : v);
-};
-
 template <typename T, int N, int C, class Spec>
-__global__ void __launch_bounds__(32 * XWarps<T, N, C>::value, (XMinBlocks<T, N, C, Spec::NSUM>::value))
-    k_xturn_fast(GridDims g, const typename Cx<T>::t* __restrict__ twx,
+__global__ void __launch_bounds__(kFastThreads) k_xturn_fast(GridDims g, const typename Cx<T>::t* __restrict__ twx,
                                                             typename Cx<T>::t* __restrict__ spec, Spec op,
                                                             const Ctl* __restrict__ ctl, double* partials) {
     typedef typename Cx<T>::t C2;

@@ -286,7 +286,9 @@ __global__ void __launch_bounds__(SlabGeom<T, N>::NT, SlabGeom<T, N>::MINB)
     const int t = lane % TL, lw = lane / TL;
     const T invV = (T)(1.0 / (double)g.V);
     const double wt = (C == 6 && c >= 3) ? 2.0 : 1.0;
-    double acc[2] = {0.0, 0.0};
+    // per-thread partial sums in the field's type (a thread sums a few dozen
+    // voxels), widened to FP64 once for the block reduction
+    T racc = 0, oacc = 0;
     // pointwise items of a chunk per thread; the first PRE are loaded before
     // the chunk's z inverse (their latency hidden by it), the rest after it
     constexpr int HP = N / 2;  // z pairs per line
@@ -330,9 +332,9 @@ __global__ void __launch_bounds__(SlabGeom<T, N>::NT, SlabGeom<T, N>::MINB)
             for (int w = 0; w < 4; ++w) {
                 const int pw = (q.p >> (8 * w)) & 0xff;
                 const T d = (xc[w] * invV + (T)q.r[w]) - q.x[w];
-                acc[0] += wt * (double)d * (double)d;
+                racc += d * d;
                 v[w] = q.x[w] + ca[pw] * d;
-                acc[1] += (double)co[pw] * (double)v[w];
+                oacc += co[pw] * v[w];
             }
             const long long vo = (long long)(2 * (m0 + li)) * N + z0;
             st2(xs + vo, v[0], v[1]);
@@ -423,6 +425,7 @@ __global__ void __launch_bounds__(SlabGeom<T, N>::NT, SlabGeom<T, N>::MINB)
             *reinterpret_cast<const float4*>((const char*)(S + row * SP) + q * 16);
     }
     if constexpr (MIX) {
+        double acc[2] = {wt * (double)racc, (double)oacc};
         block_reduce_store<2>(acc, red, partials, b, gridDim.x, blockIdx.x);
         fused_finalize(fin, ctl, partials, 2, b);
     }

@@ -1405,8 +1405,8 @@ long long m3d_footprint_bytes(int kind, int Nx, int Ny, int Nz, int behav, int p
                   + std::max(std::max(NL / 2 + 1, (long long)Ny * Hzp), 1024LL) * B * 16 * 8  // partials
                   + B * (2 * (long long)sizeof(Ctl) + 4) + 64;
     if (precision == M3D_PREC_FP32_REFINE) b += 2 * B * C * V * 4;  // correction + defect
-    if (kind == M3D_KIND_MECH && behav != M3D_BEHAV_ELASTIC)
-        b += B * V * xw * (18 + (behav == M3D_BEHAV_J2 ? 7 : 1));   // eps, sig, eps_old (+ sig_old, ep | d)
+    if (kind == M3D_KIND_MECH && behav != M3D_BEHAV_ELASTIC)  // FP64 eps, sig, eps_old (+ sig_old, ep | d)
+        b += B * V * 8 * (18 + (behav == M3D_BEHAV_J2 ? 7 : 1));
     return b;
 }
 

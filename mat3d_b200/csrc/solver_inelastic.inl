@@ -15,7 +15,7 @@ void InelasticState::free_all() {
 
 int InelasticState::setup(m3d_solver* h) {
     free_all();
-    const size_t w = (h->prec == M3D_PREC_FP32) ? 4 : 8;
+    const size_t w = 8;  // FP64 state in both precisions (the transforms carry the precision)
     const size_t V = (size_t)h->g.V, B = (size_t)h->B;
     M3D_CUDA(cudaMalloc(&eps, B * 6 * V * w));
     M3D_CUDA(cudaMalloc(&sig, B * 6 * V * w));
@@ -73,7 +73,7 @@ static int colsum_mean(m3d_solver* h, const void* x, int C, int b, double* out) 
 }
 
 int InelasticState::means(m3d_solver* h, int b, double* strain_mean, double* stress_mean) {
-    const bool f32 = h->prec == M3D_PREC_FP32;
+    const bool f32 = false;  // FP64 state
     int rc = M3D_OK;
     if (strain_mean) rc = f32 ? colsum_mean<float>(h, eps, 6, b, strain_mean) : colsum_mean<double>(h, eps, 6, b, strain_mean);
     if (rc) return rc;
@@ -88,7 +88,7 @@ __global__ void k_copy_scalar(const TX* __restrict__ x, int b, long long V, doub
 }
 
 int InelasticState::get_field(m3d_solver* h, int which, int b, double* out) {
-    const bool f32 = h->prec == M3D_PREC_FP32;
+    const bool f32 = false;  // FP64 state
     if (which == M3D_FIELD_STRAIN)
         return f32 ? export_field<float, 6>(h, eps, nullptr, b, out) : export_field<double, 6>(h, eps, nullptr, b, out);
     if (which == M3D_FIELD_STRESS)
@@ -119,12 +119,13 @@ int m3d_solver::run_inelastic(double tol_field, double tol_eq, int nInc, int cri
     static_assert(CC == 6, "inelastic path is mechanical");
     const long long V = g.V;
     const int bj = (behav == M3D_BEHAV_J2) ? BEHAV_J2 : BEHAV_DAMAGE;
-    T* eps = (T*)in.eps;
-    T* sig = (T*)in.sig;
-    T* eps_old = (T*)in.eps_old;
-    T* sig_old = (T*)in.sig_old;
-    T* ep = (T*)in.ep;
-    T* dmg = (T*)in.dmg;
+    typedef double S;  // state type (FP64 in both precisions)
+    S* eps = (S*)in.eps;
+    S* sig = (S*)in.sig;
+    S* eps_old = (S*)in.eps_old;
+    S* sig_old = (S*)in.sig_old;
+    S* ep = (S*)in.ep;
+    S* dmg = (S*)in.dmg;
     C2* sp = (C2*)d_spec;
     // initial state: eps = dE, sig = eps_old = sig_old = 0, eps_p = 1.236547e-9 (:56-98, :799)
     std::vector<double> dE((size_t)B * 6);
@@ -132,13 +133,13 @@ int m3d_solver::run_inelastic(double tol_field, double tol_eq, int nInc, int cri
         for (int c = 0; c < 6; ++c) dE[b * 6 + c] = E[b * 6 + c] / (nInc * 1.);
     for (int b = 0; b < B; ++b)
         for (int c = 0; c < 6; ++c)
-            k_fill<T><<<256, 256, 0, stream>>>(eps + ((long long)b * 6 + c) * V, V, (T)dE[b * 6 + c]);
-    M3D_CUDA(cudaMemsetAsync(sig, 0, (size_t)B * 6 * V * sizeof(T), stream));
-    M3D_CUDA(cudaMemsetAsync(eps_old, 0, (size_t)B * 6 * V * sizeof(T), stream));
-    if (sig_old) M3D_CUDA(cudaMemsetAsync(sig_old, 0, (size_t)B * 6 * V * sizeof(T), stream));
-    if (ep) k_fill<T><<<256, 256, 0, stream>>>(ep, (long long)B * V, (T)1.236547e-9);
+            k_fill<S><<<256, 256, 0, stream>>>(eps + ((long long)b * 6 + c) * V, V, dE[b * 6 + c]);
+    M3D_CUDA(cudaMemsetAsync(sig, 0, (size_t)B * 6 * V * sizeof(S), stream));
+    M3D_CUDA(cudaMemsetAsync(eps_old, 0, (size_t)B * 6 * V * sizeof(S), stream));
+    if (sig_old) M3D_CUDA(cudaMemsetAsync(sig_old, 0, (size_t)B * 6 * V * sizeof(S), stream));
+    if (ep) k_fill<S><<<256, 256, 0, stream>>>(ep, (long long)B * V, 1.236547e-9);
     st.kernel_launches += (long long)B * 6 + (ep ? 1 : 0);
-    if (dmg) M3D_CUDA(cudaMemsetAsync(dmg, 0, (size_t)B * V * sizeof(T), stream));
+    if (dmg) M3D_CUDA(cudaMemsetAsync(dmg, 0, (size_t)B * V * sizeof(S), stream));
     M3D_CUDA(cudaMemsetAsync(in.d_nrfail, 0, sizeof(int), stream));
 
     for (int b = 0; b < B; ++b) {
@@ -171,16 +172,19 @@ int m3d_solver::run_inelastic(double tol_field, double tol_eq, int nInc, int cri
     for (int j = 0; j < 6; ++j)
         if (X0[j] != 0) { t_comp = j; break; }
 
-    InelasticPtrs<T> P{d_phase, eps, sig, eps_old, sig_old, ep, dmg, V, in.d_ph, nph, bj, in.d_nrfail};
+    InelasticPtrs<S> P{d_phase, eps, sig, eps_old, sig_old, ep, dmg, V, in.d_ph, nph, bj, in.d_nrfail};
     EpiConstitutive<T> cons{P, nullptr};
     EpiBasic<T> epi{cons};
     ProStress<T> pro{sig, V};
+    // FP32 transforms under the residual rule: transform the load step's
+    // stress increment (J2 keeps the previous step's stress)
+    if (sizeof(T) == 4 && criterion == M3D_CRIT_RESIDUAL && sig_old) pro.sig_old = sig_old;
     SpecBasic<T> spec{green<T, 6>(0), SpecEqVar<T, 6>{g}};
     const size_t phb = (size_t)nph * sizeof(PhaseMech) + 64;
     const int cblk = 592;
     const size_t csmem = 32 * 32 * 8 + phb;
     allow_smem(k_constitutive<T>);
-    allow_smem(k_commit<T>);
+    allow_smem(k_commit);
     prop.assign((size_t)nInc * 9, 0.0);
     long long total = 0;
     int nx = 0, done_inc = nInc, status = M3D_OK;
@@ -240,7 +244,7 @@ int m3d_solver::run_inelastic(double tol_field, double tol_eq, int nInc, int cri
         }
         if (nx == 3) { done_inc = inc; break; }
         // export_homogen_var + update_old_Variable (entry 0 is reported)
-        k_commit<T><<<dim3(cblk, B), 256, csmem, stream>>>(P, eps_old, sig_old, ep, t_comp, d_part);
+        k_commit<<<dim3(cblk, B), 256, csmem, stream>>>(P, eps_old, sig_old, ep, t_comp, d_part);
         st.kernel_launches += 1;
         M3D_CUDA(cudaGetLastError());
         std::vector<double> hp((size_t)cblk * 9);
