@@ -865,6 +865,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true",
                     help="default workload only: skip the other configs' summaries")
+    ap.add_argument("--profile-passes", action="store_true",
+                    help="single-RVE workloads: K solves on the host-driven sweep loop with CUDA events around "
+                         "every pass (the launch sequence an ncu capture sees), print the per-pass times")
     args = ap.parse_args()
     w = WORKLOADS[args.workload]
 
@@ -890,6 +893,9 @@ def main():
         if world > 1:
             dist.destroy_process_group()
         return
+    if args.profile_passes:
+        print(json.dumps(profile_passes(args, w)))
+        return
     extras = args.workload == "thermal128" and world == 1 and not args.no_extras
     line = run_single(args, w, args.workload, rank, world, local, emit=not extras)
     if extras:
@@ -897,6 +903,40 @@ def main():
         print(json.dumps(line))
     if world > 1:
         dist.destroy_process_group()
+
+
+def profile_passes(args, w):
+    """K solves of a single-RVE workload with per-pass CUDA events (host-driven
+    loop); per sweep and per pass device times of the FP32 and FP64 sweeps."""
+    import mat3d_b200 as m3d
+    N = w["N"]
+    rve, _ = make_rve(w)
+    j2 = w.get("behav") == "ep"
+    if w["kind"] == "thermal":
+        s = m3d.Solver(m3d.KIND_THERMAL, N, N, N, m3d.ELASTIC, w["precision"], 1)
+        s.set_material_thermal(w["km"], w["ki"], rve)
+    else:
+        s = m3d.Solver(m3d.KIND_MECH, N, N, N, m3d.J2 if j2 else m3d.ELASTIC, w["precision"], 1)
+        s.set_material_mech(MAT_J2 if j2 else MAT_ELASTIC, rve)
+    E = np.array(w["E"], float)
+    X0 = np.array(w["X0"], float) if "X0" in w else None
+    s.set_profiling(True)
+    for _ in range(max(args.steps, 1)):
+        s.set_load(E, X0)
+        s.run(w["tol"], w["tol"], w.get("nInc", 1), m3d.CRIT_RESIDUAL)
+    p, st = s.profile(), s.stats()
+    names = PASS_NAMES_2 if st["passes_per_sweep"] == 2 else PASS_NAMES
+    out = {"workload": args.workload, "solves": max(args.steps, 1), "passes_per_sweep": st["passes_per_sweep"],
+           "sweeps_fp32": p["n_fp32"], "sweeps_fp64": p["n_fp64"]}
+    for tag, n, ms, pms in (("fp32", p["n_fp32"], p["ms_fp32"], p["pass_ms_fp32"]),
+                            ("fp64", p["n_fp64"], p["ms_fp64"], p["pass_ms_fp64"])):
+        if n:
+            out[f"sweep_us_{tag}"] = 1000 * ms / n
+            # the refinement's FP64 defect sweeps run the five passes
+            nm = names if (tag == "fp32" or w["precision"] == "fp64") else PASS_NAMES
+            out[f"pass_us_{tag}"] = {nm[q]: 1000 * pms[q] / n for q in range(5) if nm[q]}
+    s.close()
+    return out
 
 
 def run_extras(args, rank, world, local):

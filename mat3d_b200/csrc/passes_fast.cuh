@@ -236,6 +236,88 @@ __global__ void __launch_bounds__(kFastThreads) k_xturn_fast(GridDims g, const t
 }
 
 // ---------------------------------------------------------------------------
+// x turnaround with the three components of a column in registers (thermal
+// fields in FP32): each lane loads its E points of all three components
+// straight from global memory (every load of a warp covers CPW consecutive
+// columns of TL rows), transforms them with only the column's exchange row in
+// shared memory, applies the spectral operator to the three components of
+// each of its modes from registers, and transforms back.  Compared with the
+// staged kernel above, no component is staged or round-tripped through shared
+// memory for the operator: about 200 fewer shared-memory instructions per
+// lane, the same per-line arithmetic (results are bitwise equal).  Used up to
+// N = 64, where the 3 x E points per lane fit the registers without spilling.
+// ---------------------------------------------------------------------------
+constexpr int kXRegWarps = 4;
+
+template <typename T, int N, int NSUM>
+constexpr size_t xturn_reg_smem() {
+    typedef typename Cx<T>::t C2;
+    constexpr int CPW = 32 / LineSplit<T, N>::Tl;
+    return (size_t)N * sizeof(C2) + (size_t)kXRegWarps * CPW * RowLen<T, N, true>::value * sizeof(C2) + 16 +
+           (size_t)32 * (NSUM > 0 ? NSUM : 1) * sizeof(double);
+}
+
+template <typename T, int N, class Spec>
+__global__ void __launch_bounds__(32 * kXRegWarps) k_xturn_reg(GridDims g, const typename Cx<T>::t* __restrict__ twx,
+                                                              typename Cx<T>::t* __restrict__ spec, Spec op,
+                                                              const Ctl* __restrict__ ctl, double* partials) {
+    typedef typename Cx<T>::t C2;
+    constexpr int C = 3;
+    constexpr int E = LineSplit<T, N>::E, TL = LineSplit<T, N>::Tl, CPW = 32 / TL;
+    constexpr int RL = RowLen<T, N, true>::value;
+    const int b = blockIdx.y;
+    if (ctl[b].done) return;
+    op.prepare(ctl, b);
+    extern __shared__ __align__(16) char smem_raw[];
+    C2* tw = (C2*)smem_raw;
+    C2* xch = tw + N;  // [warp][col][RL]
+    double* red = (double*)align_up((char*)(xch + kXRegWarps * CPW * RL), 16);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int col = lane % CPW, t = lane / CPW;
+    constexpr int ncol_cta = kXRegWarps * CPW;
+    const int ntz = (g.Hzp + ncol_cta - 1) / ncol_cta;
+    const int y = blockIdx.x / ntz;
+    const int kz = (blockIdx.x - y * ntz) * ncol_cta + warp * CPW + col;
+    const bool ok = kz < g.Hzp;
+    const long long cstride = g.NL * g.Hzp;            // component stride
+    const long long xstride = (long long)g.Ny * g.Hzp;  // x stride
+    C2* base = spec + ((long long)b * C * g.NL + y) * g.Hzp + (ok ? kz : 0);
+    C2* xl = xch + (warp * CPW + col) * RL;
+    const int sw = RowLen<T, N, true>::sw ? (col & 1) : 0;
+    C2 v[C][E];
+#pragma unroll
+    for (int c = 0; c < C; ++c)
+#pragma unroll
+        for (int j = 0; j < E; ++j) v[c][j] = ok ? base[c * cstride + (long long)(t + TL * j) * xstride] : mk<C2>(0, 0);
+    for (int i = threadIdx.x; i < N; i += blockDim.x) tw[i] = twx[i];
+    __syncthreads();
+#pragma unroll
+    for (int c = 0; c < C; ++c) line_fwd<C2, E, TL>(v[c], t, xl, tw, sw);
+    double acc[Spec::NSUM > 0 ? Spec::NSUM : 1] = {};
+    const bool live = ok && kz < g.Hz;
+#pragma unroll
+    for (int r = 0; r < E; ++r) {
+        C2 m[C] = {v[0][r], v[1][r], v[2][r]};
+        if (live) op.apply(b, spec_mode<E, TL>(t, r), y, kz, m, acc, ctl);
+#pragma unroll
+        for (int c = 0; c < C; ++c) v[c][r] = m[c];
+    }
+    if constexpr (Spec::NSUM > 0) {
+        block_reduce_store<Spec::NSUM>(acc, red, partials, b, gridDim.x, blockIdx.x);
+    }
+    if constexpr (Spec::kInverse) {
+#pragma unroll
+        for (int c = 0; c < C; ++c) {
+            line_inv<C2, E, TL>(v[c], t, xl, tw, sw);
+            if (ok) {
+#pragma unroll
+                for (int j = 0; j < E; ++j) base[c * cstride + (long long)(t + TL * j) * xstride] = v[c][j];
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
 // z passes.  Tile of G voxel lines x NCL complex lines (NCL = ceil(C/2)).
 // ---------------------------------------------------------------------------
 template <int C> struct NclOf { static constexpr int value = (C + 1) / 2; };

@@ -39,13 +39,12 @@
 
 namespace m3d {
 
-template <typename T, int N>
+// NT threads per CTA: 256 (8 warps, two CTAs per SM) or 512 (16 warps, one
+// CTA per SM: the FP32 128^2 slab with all its z lines in one chunk)
+template <typename T, int N, int NT_ = 256>
 struct SlabGeom {
     typedef typename Cx<T>::t C2;
-    // threads per CTA: 16 warps and one CTA per SM where one CTA can hold the
-    // FP32 128^2 slab with all its z lines in one chunk (the slabs then spread
-    // over the SMs in near-even rounds); 8 warps and two CTAs per SM otherwise
-    static constexpr int NT = (sizeof(T) == 4 && N == 128) ? 512 : 256;
+    static constexpr int NT = NT_;
     static constexpr int MINB = NT == 512 ? 1 : 2;
     static constexpr int E = LineSplit<T, N>::E, TL = LineSplit<T, N>::Tl;
     static constexpr int CPW = 32 / TL;  // columns (y FFTs) or packed lines (z FFTs) per warp
@@ -144,10 +143,10 @@ __device__ __forceinline__ void tile_put2(double2* tr, int z0, int sw, double2 a
 //     Hermitian parts H0 + i H_N/2 are transformed together and the real and
 //     imaginary parts of the result are the two columns' real parts.
 // The pre- and post-steps are done by the warp that owns column group 0.
-template <typename T, int N, int SIGN>
+template <typename T, int N, int NT, int SIGN>
 __device__ __forceinline__ void slab_columns(typename Cx<T>::t* S, typename Cx<T>::t* W, const typename Cx<T>::t* tw) {
     typedef typename Cx<T>::t C2;
-    typedef SlabGeom<T, N> G;
+    typedef SlabGeom<T, N, NT> G;
     constexpr int E = G::E, TL = G::TL, CPW = G::CPW, SP = G::SP, H = N / 2;
     constexpr int KPL = (N + 31) / 32;  // column entries per lane in the pack / split steps
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -231,12 +230,12 @@ __device__ __forceinline__ void slab_columns(typename Cx<T>::t* S, typename Cx<T
     }
 }
 
-template <typename T, int N, bool MIX, class Fin>
-__global__ void __launch_bounds__(SlabGeom<T, N>::NT, SlabGeom<T, N>::MINB)
+template <typename T, int N, int NT, bool MIX, class Fin>
+__global__ void __launch_bounds__(NT, SlabGeom<T, N, NT>::MINB)
     k_slab(GridDims g, const typename Cx<T>::t* __restrict__ twz, typename Cx<T>::t* __restrict__ spec, SlabOps<T> ops,
            Ctl* ctl, double* partials, Fin fin) {
     typedef typename Cx<T>::t C2;
-    typedef SlabGeom<T, N> G;
+    typedef SlabGeom<T, N, NT> G;
     constexpr int E = G::E, TL = G::TL, CPW = G::CPW, SP = G::SP, ROW = G::ROW;
     const int b = blockIdx.y;
     if (ctl[b].done) return;
@@ -278,7 +277,7 @@ __global__ void __launch_bounds__(SlabGeom<T, N>::NT, SlabGeom<T, N>::MINB)
     }
     __syncthreads();
     if constexpr (MIX) {
-        slab_columns<T, N, +1>(S, W, tw);
+        slab_columns<T, N, NT, +1>(S, W, tw);
         __syncthreads();
     }
 
@@ -417,7 +416,7 @@ __global__ void __launch_bounds__(SlabGeom<T, N>::NT, SlabGeom<T, N>::MINB)
         }
         __syncthreads();
     }
-    slab_columns<T, N, -1>(S, W, tw);
+    slab_columns<T, N, NT, -1>(S, W, tw);
     __syncthreads();
     for (int i = threadIdx.x; i < N * CPR; i += G::NT) {
         const int row = i / CPR, q = i - row * CPR;

@@ -308,6 +308,10 @@ struct m3d_solver {
     // per-component and the slab fits two CTAs per SM; M3D_NO_SLAB=1 keeps
     // the five-pass sweep
     bool use_slab = true;
+    int slab_nt = 512;  // M3D_SLAB_NT=256: two 256-thread slab CTAs per SM at FP32 128^2
+    // thermal FP32 x turnaround with the three components in registers
+    // (M3D_XTURN_STAGED=1 keeps the shared-memory-staged kernel)
+    bool use_xreg = true;
     template <typename T> bool slab_ok() const;
     template <typename T, int CC, bool MIX, class Fin>
     int pass_slab(Ctl* ctl, T* x, const float* r, typename Cx<T>::t* sp, Fin fin);
@@ -656,8 +660,18 @@ int m3d_solver::pass_x(Spec op, Ctl* ctl, typename Cx<T>::t* sp) {
     int nblk = 0;
     const bool done = use_fast && with_fast_n(Nx, [&](auto nc) {
         constexpr int NN = decltype(nc)::value;
-        constexpr int WPC = XWarps<T, NN, CC>::value;
         constexpr int CPW = 32 / LineSplit<T, NN>::Tl;
+        if constexpr (CC == 3 && sizeof(T) == 4 && NN <= 64) {
+            if (use_xreg) {  // the three components in registers (fits them without spilling up to N = 64)
+                const int ntz = (g.Hzp + kXRegWarps * CPW - 1) / (kXRegWarps * CPW);
+                nblk = Ny * ntz;
+                allow_smem(k_xturn_reg<T, NN, Spec>);
+                k_xturn_reg<T, NN, Spec><<<dim3(nblk, B), kXRegWarps * 32, xturn_reg_smem<T, NN, Spec::NSUM>(), stream>>>(
+                    g, tw<T>(0), sp, op, ctl, d_part);
+                return;
+            }
+        }
+        constexpr int WPC = XWarps<T, NN, CC>::value;
         const int ntz = (g.Hzp + WPC * CPW - 1) / (WPC * CPW);
         nblk = Ny * ntz;
         allow_smem(k_xturn_fast<T, NN, CC, Spec>);
@@ -746,9 +760,13 @@ int m3d_solver::launch_em(Ctl* ctl, T* x, const float* r, typename Cx<T>::t* sp,
 // ---- two-pass sweeps: x turnaround + y-z slab pass (passes_slab.cuh) --------
 // A slab instantiation is used where its shared memory leaves room for two
 // CTAs per SM.
+// CTA width of the slab pass: 512 threads (one CTA per SM) for the FP32 128^2
+// slab unless M3D_SLAB_NT=256 asks for two 256-thread CTAs per SM; 256
+// threads for every other size
+template <typename T, int NN> constexpr int slab_nt_wide() { return (sizeof(T) == 4 && NN == 128) ? 512 : 256; }
 template <typename T, int NN>
 constexpr bool slab_fits() {
-    return SlabGeom<T, NN>::fits();
+    return SlabGeom<T, NN, slab_nt_wide<T, NN>()>::fits();
 }
 
 template <typename T>
@@ -768,10 +786,18 @@ int m3d_solver::pass_slab(Ctl* ctl, T* x, const float* r, typename Cx<T>::t* sp,
     with_fast_n(Nz, [&](auto nc) {
         constexpr int NN = decltype(nc)::value;
         if constexpr (slab_fits<T, NN>()) {
-            auto kern = k_slab<T, NN, MIX, Fin>;
-            allow_smem(kern);
-            kern<<<dim3(CC * Nx, B), SlabGeom<T, NN>::NT, SlabGeom<T, NN>::smem(), stream>>>(g, tw<T>(2), sp, ops, ctl,
-                                                                                      d_part, fin);
+            constexpr int NTW = slab_nt_wide<T, NN>();
+            if (NTW == 512 && slab_nt == 256 && SlabGeom<T, NN, 256>::fits()) {
+                auto kern = k_slab<T, NN, 256, MIX, Fin>;
+                allow_smem(kern);
+                kern<<<dim3(CC * Nx, B), 256, SlabGeom<T, NN, 256>::smem(), stream>>>(g, tw<T>(2), sp, ops, ctl, d_part,
+                                                                                    fin);
+            } else {
+                auto kern = k_slab<T, NN, NTW, MIX, Fin>;
+                allow_smem(kern);
+                kern<<<dim3(CC * Nx, B), NTW, SlabGeom<T, NN, NTW>::smem(), stream>>>(g, tw<T>(2), sp, ops, ctl, d_part,
+                                                                                    fin);
+            }
             done = true;
         }
     });
@@ -1354,6 +1380,10 @@ static int create_impl(int kind, int Nx, int Ny, int Nz, int behav, int precisio
         h->use_tma_y = (e4 && e4[0] == '1');
         const char* e5 = std::getenv("M3D_NO_SLAB");
         h->use_slab = !(e5 && e5[0] == '1');
+        const char* e7 = std::getenv("M3D_SLAB_NT");
+        h->slab_nt = (e7 && std::atoi(e7) == 256) ? 256 : 512;
+        const char* e6 = std::getenv("M3D_XTURN_STAGED");
+        h->use_xreg = !(e6 && e6[0] == '1');
     }
     int rc = h->alloc(batch);
     if (rc) { cudaStreamDestroy(h->stream); delete h; return rc; }
