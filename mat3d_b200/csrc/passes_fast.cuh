@@ -20,6 +20,7 @@
 #pragma once
 #include "fft_reg.cuh"
 #include "passes.cuh"
+#include "physics.cuh"
 #include "tma.cuh"
 
 namespace m3d {
@@ -315,6 +316,127 @@ __global__ void __launch_bounds__(32 * kXRegWarps) k_xturn_reg(GridDims g, const
             }
         }
     }
+}
+
+// ---------------------------------------------------------------------------
+// x turnaround of the thermal Green operators in rank-one form.  Both act on
+// a mode through d = xi . v only (physics.cuh, SpecGreen):
+//   gradient-based  v_c' = xi_c D,                 D = -p1 d / |xi|^2
+//   flux-based      v_c' = -p1 (v_c - xi_c D),    D = d / |xi|^2
+// and along an x column xi_z and xi_y are constant, so the inverse transforms
+// of the three outputs need only IFFT(D) and IFFT(xi_x D):
+//   gradient  out_z = xi_z IFFT(D), out_y = xi_y IFFT(D), out_x = IFFT(xi_x D)
+//   flux      out_c = -p1 N v_c + p1 (same terms),  N v_c = IFFT(FFT(v_c))
+// (unnormalised transforms; v_c is re-read from global memory, where it still
+// lies).  d is accumulated while each component is transformed, so a column
+// costs three forward and two inverse line transforms instead of six, and no
+// component is staged in shared memory.  The k = 0 mode, whose value is set
+// rather than computed (the load or 0), is handled in the one column holding
+// it: D(0) = 0 and the missing constant is added to every x.  Arithmetic is
+// the same to rounding (FP32); the wave vectors follow SpecGreen's sign and
+// wrap rules exactly.
+// ---------------------------------------------------------------------------
+// CTAs per SM the rank-one x turnaround is compiled for (bounds its registers)
+template <int N> struct XR1MinB { static constexpr int value = N == 128 ? 3 : (N == 96 ? 2 : 4); };
+
+template <typename T, int N>
+__global__ void __launch_bounds__(32 * kXRegWarps, XR1MinB<N>::value) k_xturn_r1(GridDims g, const typename Cx<T>::t* __restrict__ twx,
+                                                             typename Cx<T>::t* __restrict__ spec, SpecGreenT<T> op,
+                                                             const Ctl* __restrict__ ctl) {
+    typedef typename Cx<T>::t C2;
+    constexpr int C = 3;
+    constexpr int E = LineSplit<T, N>::E, TL = LineSplit<T, N>::Tl, CPW = 32 / TL;
+    constexpr int RL = RowLen<T, N, true>::value;
+    const int b = blockIdx.y;
+    if (ctl[b].done) return;
+    op.prepare(ctl, b);
+    extern __shared__ __align__(16) char smem_raw[];
+    C2* tw = (C2*)smem_raw;
+    C2* xch = tw + N;  // [warp][col][RL]
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int col = lane % CPW, t = lane / CPW;
+    constexpr int ncol_cta = kXRegWarps * CPW;
+    const int ntz = (g.Hzp + ncol_cta - 1) / ncol_cta;
+    const int y = blockIdx.x / ntz;
+    const int kz = (blockIdx.x - y * ntz) * ncol_cta + warp * CPW + col;
+    const bool ok = kz < g.Hzp;
+    const long long cstride = g.NL * g.Hzp;            // component stride
+    const long long xstride = (long long)g.Ny * g.Hzp;  // x stride
+    C2* base = spec + ((long long)b * C * g.NL + y) * g.Hzp + (ok ? kz : 0);
+    C2* xl = xch + (warp * CPW + col) * RL;
+    const int sw = RowLen<T, N, true>::sw ? (col & 1) : 0;
+    const bool grad = op.kind == GREEN_TGRAD;
+    const T fz = (T)sfreq(kz, op.pos_nyq ? g.Nz / 2 : (g.Nz - 1) / 2, g.Nz);
+    const T fy = (T)sfreq(y, op.pos_nyq ? g.Ny / 2 : (g.Ny - 1) / 2, g.Ny);
+    const bool origin = (y == 0 && kz == 0);  // the column holding the k = 0 mode
+    for (int i = threadIdx.x; i < N; i += blockDim.x) tw[i] = twx[i];
+    __syncthreads();
+    C2 v[E], d[E];
+    T fx[E];   // x frequency of each of this lane's modes
+    C2 k0[C];  // mode 0 of each component (origin column)
+#pragma unroll
+    for (int r = 0; r < E; ++r) {
+        fx[r] = (T)sfreq(spec_mode<E, TL>(t, r), op.pos_nyq ? g.Nx / 2 : (g.Nx - 1) / 2, op.xwrap);
+        d[r] = mk<C2>(0, 0);
+    }
+    // one component per trip (its loads are not hoisted over the others'
+    // transforms: the registers hold one component and d)
+#pragma unroll 1
+    for (int c = 0; c < C; ++c) {
+#pragma unroll
+        for (int j = 0; j < E; ++j) v[j] = ok ? base[c * cstride + (long long)(t + TL * j) * xstride] : mk<C2>(0, 0);
+        line_fwd<C2, E, TL>(v, t, xl, tw, sw);
+        const C2 m0 = mk<C2>(__shfl_sync(0xffffffffu, v[0].x, col), __shfl_sync(0xffffffffu, v[0].y, col));  // t = 0: mode 0
+        if (c == 0) k0[0] = m0;
+        else if (c == 1) k0[1] = m0;
+        else k0[2] = m0;
+        const T fcol = c == 0 ? fz : fy;
+#pragma unroll
+        for (int r = 0; r < E; ++r) {
+            const T fc = c == 2 ? fx[r] : fcol;
+            d[r] = mk<C2>(d[r].x + fc * v[r].x, d[r].y + fc * v[r].y);
+        }
+    }
+    // D = coef d per mode; the x-frequency weighted copy for the x component
+#pragma unroll
+    for (int r = 0; r < E; ++r) {
+        const int mode = spec_mode<E, TL>(t, r);
+        const T n2 = fz * fz + fy * fy + fx[r] * fx[r];
+        const T coef = (origin && mode == 0) ? (T)0 : (grad ? -op.p1 : (T)1) / n2;
+        d[r] = mk<C2>(coef * d[r].x, coef * d[r].y);
+        v[r] = mk<C2>(fx[r] * d[r].x, fx[r] * d[r].y);
+    }
+    // the k = 0 mode's value (the load, or 0 in a correction solve) minus what
+    // the rank-one terms give there (0, and -p1 N mean for the flux form)
+    C2 add[C] = {mk<C2>(0, 0), mk<C2>(0, 0), mk<C2>(0, 0)};
+    if (origin) {
+#pragma unroll
+        for (int c = 0; c < C; ++c) {
+            const T kc = op.zero_k0 ? (T)0 : (T)ctl[b].kzero[c];
+            add[c] = grad ? mk<C2>(kc, 0) : mk<C2>(kc + op.p1 * k0[c].x, op.p1 * k0[c].y);
+        }
+    }
+    const T sc = grad ? (T)1 : op.p1;  // scale of the rank-one terms
+    // out_c = sc * (column term) [- p1 N v_c] + add_c, written over v_c
+    auto emit = [&](int c, const C2 (&u)[E], T f) {
+#pragma unroll
+        for (int j = 0; j < E; ++j) {
+            C2* p = base + c * cstride + (long long)(t + TL * j) * xstride;
+            C2 o = mk<C2>(sc * f * u[j].x, sc * f * u[j].y);
+            if (!grad) {
+                const C2 in = *p;
+                o = mk<C2>(o.x - op.p1 * (T)N * in.x, o.y - op.p1 * (T)N * in.y);
+            }
+            *p = mk<C2>(o.x + add[c].x, o.y + add[c].y);
+        }
+    };
+    line_inv<C2, E, TL>(d, t, xl, tw, sw);  // IFFT(D), natural order
+    if (ok) {
+        emit(0, d, fz);
+        emit(1, d, fy);
+    }
+    line_inv<C2, E, TL>(v, t, xl, tw, sw);  // IFFT(xi_x D)
+    if (ok) emit(2, v, (T)1);
 }
 
 // ---------------------------------------------------------------------------

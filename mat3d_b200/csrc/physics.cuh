@@ -130,6 +130,8 @@ struct SpecGreen {
     }
 };
 
+template <typename T> using SpecGreenT = SpecGreen<T, 3>;
+
 // ----------------------------------------------------------------------------
 // Reference stop rule (convergenceCheck): forward spectrum of the stress (heat
 // flux) reduced to cc = sum sqrt|...| and dd^2 = |stress^(0)|^2

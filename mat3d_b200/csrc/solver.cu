@@ -17,6 +17,7 @@
 #include <map>
 #include <mutex>
 #include <tuple>
+#include <type_traits>
 #include <set>
 #include <string>
 #include <vector>
@@ -308,10 +309,12 @@ struct m3d_solver {
     // per-component and the slab fits two CTAs per SM; M3D_NO_SLAB=1 keeps
     // the five-pass sweep
     bool use_slab = true;
-    int slab_nt = 512;  // M3D_SLAB_NT=256: two 256-thread slab CTAs per SM at FP32 128^2
+    int slab_nt = 256;  // M3D_SLAB_NT=512: one 512-thread slab CTA per SM at FP32 128^2 (measured slower)
     // thermal FP32 x turnaround with the three components in registers
     // (M3D_XTURN_STAGED=1 keeps the shared-memory-staged kernel)
     bool use_xreg = true;
+    // thermal FP32 x turnaround in rank-one form (M3D_XTURN_R1=0 turns it off)
+    bool use_xr1 = true;
     template <typename T> bool slab_ok() const;
     template <typename T, int CC, bool MIX, class Fin>
     int pass_slab(Ctl* ctl, T* x, const float* r, typename Cx<T>::t* sp, Fin fin);
@@ -661,6 +664,17 @@ int m3d_solver::pass_x(Spec op, Ctl* ctl, typename Cx<T>::t* sp) {
     const bool done = use_fast && with_fast_n(Nx, [&](auto nc) {
         constexpr int NN = decltype(nc)::value;
         constexpr int CPW = 32 / LineSplit<T, NN>::Tl;
+        if constexpr (CC == 3 && sizeof(T) == 4 && NN <= 128 && std::is_same<Spec, SpecGreen<T, 3>>::value) {
+            if (use_xr1) {  // thermal Green operators in rank-one form
+                const int ntz = (g.Hzp + kXRegWarps * CPW - 1) / (kXRegWarps * CPW);
+                nblk = Ny * ntz;
+                const size_t sm = (size_t)NN * sizeof(typename Cx<T>::t) +
+                                  (size_t)kXRegWarps * CPW * RowLen<T, NN, true>::value * sizeof(typename Cx<T>::t);
+                allow_smem(k_xturn_r1<T, NN>);
+                k_xturn_r1<T, NN><<<dim3(nblk, B), kXRegWarps * 32, sm, stream>>>(g, tw<T>(0), sp, op, ctl);
+                return;
+            }
+        }
         if constexpr (CC == 3 && sizeof(T) == 4 && NN <= 64) {
             if (use_xreg) {  // the three components in registers (fits them without spilling up to N = 64)
                 const int ntz = (g.Hzp + kXRegWarps * CPW - 1) / (kXRegWarps * CPW);
@@ -760,9 +774,9 @@ int m3d_solver::launch_em(Ctl* ctl, T* x, const float* r, typename Cx<T>::t* sp,
 // ---- two-pass sweeps: x turnaround + y-z slab pass (passes_slab.cuh) --------
 // A slab instantiation is used where its shared memory leaves room for two
 // CTAs per SM.
-// CTA width of the slab pass: 512 threads (one CTA per SM) for the FP32 128^2
-// slab unless M3D_SLAB_NT=256 asks for two 256-thread CTAs per SM; 256
-// threads for every other size
+// CTA width of the slab pass: two 256-thread CTAs per SM (measured 56 us vs
+// 60 us per launch at FP32 128^2 against one 512-thread CTA, which
+// M3D_SLAB_NT=512 selects there)
 template <typename T, int NN> constexpr int slab_nt_wide() { return (sizeof(T) == 4 && NN == 128) ? 512 : 256; }
 template <typename T, int NN>
 constexpr bool slab_fits() {
@@ -1381,7 +1395,9 @@ static int create_impl(int kind, int Nx, int Ny, int Nz, int behav, int precisio
         const char* e5 = std::getenv("M3D_NO_SLAB");
         h->use_slab = !(e5 && e5[0] == '1');
         const char* e7 = std::getenv("M3D_SLAB_NT");
-        h->slab_nt = (e7 && std::atoi(e7) == 256) ? 256 : 512;
+        h->slab_nt = (e7 && std::atoi(e7) == 512) ? 512 : 256;
+        const char* e8 = std::getenv("M3D_XTURN_R1");
+        h->use_xr1 = !(e8 && e8[0] == '0');
         const char* e6 = std::getenv("M3D_XTURN_STAGED");
         h->use_xreg = !(e6 && e6[0] == '1');
     }

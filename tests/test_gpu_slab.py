@@ -134,3 +134,21 @@ def test_slab_multi_rve(monkeypatch):
         s.set_material_thermal(*ks[r], rves[r])
         K1, *_ = s.homogenize(1e-9, 0, m3d.CRIT_RESIDUAL)
         assert np.array_equal(K[r], K1)
+
+
+@pytest.mark.parametrize("N", [32, 64, 128])
+@pytest.mark.parametrize("km,ki", [(1.0, 100.0), (30.0, 25.0)])  # gradient-based, flux-based
+@pytest.mark.parametrize("prec,tol", [("fp32", 1e-6), ("fp32_refine", 1e-9)])
+def test_rank_one_x_turnaround_matches_staged(N, km, ki, prec, tol, monkeypatch):
+    """The thermal x turnaround in rank-one form (three forward, two inverse
+    line FFTs) against the staged kernel that applies the Green operator mode
+    by mode: FP32 fields within 1e-5, refined fields within 1e-8."""
+    shape = (N, N, N)
+    rve = sphere_rve(shape, N / 4, center=(N / 2 + 1, N / 2, N / 2 - 1))
+    E = np.array([0.2, 0.3, 1.0])
+    out = []
+    for r1 in ("1", "0"):
+        monkeypatch.setenv("M3D_XTURN_R1", r1)
+        (a,), st = thermal_solve(shape, km, ki, rve, E, prec, tol, monkeypatch, slab=True)
+        out.append(a)
+    assert rel(out[0], out[1]) < (1e-5 if prec == "fp32" else 1e-8), rel(out[0], out[1])
