@@ -314,6 +314,8 @@ typedef struct {
     double sweep_us;  /* measured time of one sweep with this schedule */
     int candidates;   /* schedules timed */
     int slab;         /* 1: two-pass sweeps (x turnaround + y-z slab pass) */
+    int schedule;     /* generic line FFTs: order of the radix stages (0 largest odd factor first,
+                         1 smallest odd first, 2 powers of two first, 3 radix-4 for the powers of two) */
 } m3d_tune;
 int m3d_autotune(m3d_solver* h, int sweeps, m3d_tune* out);
 

@@ -72,7 +72,7 @@ class BatchStats(ctypes.Structure):
 class Tune(ctypes.Structure):
     _fields_ = [("fast", ctypes.c_int), ("tma_y", ctypes.c_int), ("G", ctypes.c_int), ("tzy", ctypes.c_int),
                 ("tzx", ctypes.c_int), ("sweep_us", ctypes.c_double), ("candidates", ctypes.c_int),
-                ("slab", ctypes.c_int)]
+                ("slab", ctypes.c_int), ("schedule", ctypes.c_int)]
 
 
 class Request(ctypes.Structure):

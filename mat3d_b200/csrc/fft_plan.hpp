@@ -13,8 +13,12 @@ namespace m3d {
 // first stage needs no twiddle multiplications, so the costliest butterfly
 // goes there), then 8, 4, 2; false if a factor is larger
 // (fuse9: two factors 3 become one radix-9 stage -- one Stockham stage and
-// barrier fewer -- for callers whose kernels compile the 9-point butterfly)
-inline bool make_plan(int n, LinePlan& p, bool fuse9 = false) {
+// barrier fewer -- for callers whose kernels compile the 9-point butterfly).
+// Any order of the factors is a valid Stockham schedule; `order` picks one
+// for the autotuner: 0 the above, 1 odd factors smallest first, 2 the
+// power-of-two stages first, 3 the power of two as radix-4 stages (and one 2).
+constexpr int kPlanOrders = 4;
+inline bool make_plan(int n, LinePlan& p, bool fuse9 = false, int order = 0) {
     std::vector<int> f, odd;
     int m = n;
     int p2 = 0;
@@ -24,10 +28,18 @@ inline bool make_plan(int n, LinePlan& p, bool fuse9 = false) {
     for (int q = 3; q <= m; q += 2)
         while (m % q == 0) { odd.push_back(q); m /= q; }
     std::sort(odd.begin(), odd.end());
-    for (auto it = odd.rbegin(); it != odd.rend(); ++it) f.push_back(*it);
-    for (; p2 >= 3; p2 -= 3) f.push_back(8);
-    if (p2 == 2) f.push_back(4);
-    if (p2 == 1) f.push_back(2);
+    std::vector<int> pow2;
+    if (order == 3) {
+        for (; p2 >= 2; p2 -= 2) pow2.push_back(4);
+    } else {
+        for (; p2 >= 3; p2 -= 3) pow2.push_back(8);
+        if (p2 == 2) pow2.push_back(4);
+    }
+    if (p2 == 1) pow2.push_back(2);
+    if (order == 2) f = pow2;
+    if (order == 1) f.insert(f.end(), odd.begin(), odd.end());
+    else f.insert(f.end(), odd.rbegin(), odd.rend());
+    if (order != 2) f.insert(f.end(), pow2.begin(), pow2.end());
     if (f.empty()) f.push_back(1);
     if ((int)f.size() > kMaxStages) return false;
     for (int r : f)

@@ -1360,7 +1360,10 @@ static int create_impl(int kind, int Nx, int Ny, int Nz, int behav, int precisio
     h->g.Hzp = even_up(Nz / 2 + 1);
     h->g.V = (long long)Nx * Ny * Nz;
     h->g.NL = (long long)Nx * Ny;
-    if (!make_plan(Nx, h->px) || !make_plan(Ny, h->py) || !make_plan(Nz, h->pz)) {
+    // M3D_FFT_SCHEDULE=<0..3>: the generic line FFTs' radix-stage order (make_plan)
+    const char* esch = std::getenv("M3D_FFT_SCHEDULE");
+    const int sched = esch ? std::max(0, std::min(kPlanOrders - 1, std::atoi(esch))) : 0;
+    if (!make_plan(Nx, h->px, false, sched) || !make_plan(Ny, h->py, false, sched) || !make_plan(Nz, h->pz, false, sched)) {
         delete h;
         return fail(M3D_ERR_UNSUPPORTED, "grid sizes need prime factors <= 32");
     }
@@ -1933,33 +1936,53 @@ int m3d_solver::autotune(int sweeps, m3d_tune* out) {
     if (fast_ok) {
         // compile-time kernels with either y pass, the two-pass sweep where the
         // operators allow it, and the generic kernels with their default tiles
-        cand.push_back(m3d_tune{1, 0, G0, Y0, X0, 0, 0, 0});
-        cand.push_back(m3d_tune{1, 1, G0, Y0, X0, 0, 0, 0});
+        cand.push_back(m3d_tune{1, 0, G0, Y0, X0, 0, 0, 0, 0});
+        cand.push_back(m3d_tune{1, 1, G0, Y0, X0, 0, 0, 0, 0});
         const bool f1 = use_fast, s1 = use_slab;
         use_fast = use_slab = true;
         const bool slab_possible = fp64 ? slab_ok<double>() : slab_ok<float>();
         use_fast = f1;
         use_slab = s1;
-        if (slab_possible) cand.push_back(m3d_tune{1, 0, G0, Y0, X0, 0, 0, 1});
-        cand.push_back(m3d_tune{0, 0, G0, Y0, X0, 0, 0, 0});
+        if (slab_possible) cand.push_back(m3d_tune{1, 0, G0, Y0, X0, 0, 0, 1, 0});
+        cand.push_back(m3d_tune{0, 0, G0, Y0, X0, 0, 0, 0, 0});
     } else {
-        // generic kernels: every tile size whose shared memory fits comfortably
+        // generic kernels: every tile size whose shared memory fits comfortably,
+        // and (with the heuristic tiles) every distinct order of the radix stages
         for (int Gv : {2, 4, 8, 16}) {
             if ((size_t)Nz * csz * (1 + (size_t)Gv * C) + 32 * 32 * 8 + op_smem<double, 6>() > lim) continue;
             for (int tz : {2, 4, 8, 16}) {
                 if (2 * (size_t)C * Nx * tz * csz + (size_t)Nx * csz > lim || 2 * (size_t)Ny * tz * csz > lim) continue;
-                cand.push_back(m3d_tune{0, 0, Gv, tz, tz, 0, 0, 0});
+                cand.push_back(m3d_tune{0, 0, Gv, tz, tz, 0, 0, 0, 0});
             }
+        }
+        auto same = [](const LinePlan& a, const LinePlan& b) {
+            if (a.nstages != b.nstages) return false;
+            for (int i = 0; i < a.nstages; ++i)
+                if (a.radix[i] != b.radix[i]) return false;
+            return true;
+        };
+        for (int o = 1; o < kPlanOrders; ++o) {
+            LinePlan qx{}, qy{}, qz{}, rx{}, ry{}, rz{};
+            if (!make_plan(Nx, qx, false, o) || !make_plan(Ny, qy, false, o) || !make_plan(Nz, qz, false, o)) continue;
+            bool dup = false;
+            for (int o2 = 0; o2 < o && !dup; ++o2)
+                if (make_plan(Nx, rx, false, o2) && make_plan(Ny, ry, false, o2) && make_plan(Nz, rz, false, o2))
+                    dup = same(qx, rx) && same(qy, ry) && same(qz, rz);
+            if (!dup) cand.push_back(m3d_tune{0, 0, G0, Y0, X0, 0, 0, 0, o});
         }
     }
     const bool f0 = use_fast, t0 = use_tma_y, sl0 = use_slab;
     const int g32 = G32, g64 = G64, y32 = TZy32, y64 = TZy64, x32 = TZx32, x64 = TZx64;
+    const LinePlan px0 = px, py0 = py, pz0 = pz;
     int best = -1;
     for (size_t i = 0; i < cand.size(); ++i) {
         m3d_tune& c = cand[i];
         use_fast = c.fast != 0;
         use_tma_y = c.tma_y != 0;
         use_slab = c.slab != 0;
+        make_plan(Nx, px, false, c.schedule);
+        make_plan(Ny, py, false, c.schedule);
+        make_plan(Nz, pz, false, c.schedule);
         (fp64 ? G64 : G32) = c.G;
         (fp64 ? TZy64 : TZy32) = c.tzy;
         (fp64 ? TZx64 : TZx32) = c.tzx;
@@ -1974,6 +1997,7 @@ int m3d_solver::autotune(int sweeps, m3d_tune* out) {
         if (best < 0 || c.sweep_us < cand[best].sweep_us) best = (int)i;
     }
     use_fast = f0; use_tma_y = t0; use_slab = sl0;
+    px = px0; py = py0; pz = pz0;
     G32 = g32; G64 = g64; TZy32 = y32; TZy64 = y64; TZx32 = x32; TZx64 = x64;
     drop_graphs();
     if (best < 0) return fail(M3D_ERR_CUDA, "autotune: no candidate ran");
@@ -2010,6 +2034,9 @@ int m3d_autotune(m3d_solver* h, int sweeps, m3d_tune* out) {
     h->use_fast = t.fast != 0;
     h->use_tma_y = t.tma_y != 0;
     h->use_slab = t.slab != 0;
+    make_plan(h->Nx, h->px, false, t.schedule);
+    make_plan(h->Ny, h->py, false, t.schedule);
+    make_plan(h->Nz, h->pz, false, t.schedule);
     (fp64 ? h->G64 : h->G32) = t.G;
     (fp64 ? h->TZy64 : h->TZy32) = t.tzy;
     (fp64 ? h->TZx64 : h->TZx32) = t.tzx;
