@@ -355,11 +355,15 @@ __global__ void __launch_bounds__(32 * kXRegWarps, XR1MinB<N>::value) k_xturn_r1
     C2* xch = tw + N;  // [warp][col][RL]
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int col = lane % CPW, t = lane / CPW;
-    constexpr int ncol_cta = kXRegWarps * CPW;
-    const int ntz = (g.Hzp + ncol_cta - 1) / ncol_cta;
-    const int y = blockIdx.x / ntz;
-    const int kz = (blockIdx.x - y * ntz) * ncol_cta + warp * CPW + col;
-    const bool ok = kz < g.Hzp;
+    // warp-granular work items: item = (y, group of CPW kz columns), kXRegWarps
+    // consecutive items per CTA, so the short last group of a y row (Hzp is
+    // not a multiple of CPW) costs one warp, not a whole CTA
+    const int ngrp = (g.Hzp + CPW - 1) / CPW;
+    const int item = blockIdx.x * kXRegWarps + warp;
+    const bool have = item < g.Ny * ngrp;
+    const int y = have ? item / ngrp : 0;
+    const int kz = (item - y * ngrp) * CPW + col;
+    const bool ok = have && kz < g.Hzp;
     const long long cstride = g.NL * g.Hzp;            // component stride
     const long long xstride = (long long)g.Ny * g.Hzp;  // x stride
     C2* base = spec + ((long long)b * C * g.NL + y) * g.Hzp + (ok ? kz : 0);
@@ -368,9 +372,10 @@ __global__ void __launch_bounds__(32 * kXRegWarps, XR1MinB<N>::value) k_xturn_r1
     const bool grad = op.kind == GREEN_TGRAD;
     const T fz = (T)sfreq(kz, op.pos_nyq ? g.Nz / 2 : (g.Nz - 1) / 2, g.Nz);
     const T fy = (T)sfreq(y, op.pos_nyq ? g.Ny / 2 : (g.Ny - 1) / 2, g.Ny);
-    const bool origin = (y == 0 && kz == 0);  // the column holding the k = 0 mode
+    const bool origin = ok && y == 0 && kz == 0;  // the column holding the k = 0 mode
     for (int i = threadIdx.x; i < N; i += blockDim.x) tw[i] = twx[i];
     __syncthreads();
+    if (!have) return;  // no block barrier follows
     C2 v[E], d[E];
     T fx[E];   // x frequency of each of this lane's modes
     C2 k0[C];  // mode 0 of each component (origin column)

@@ -665,9 +665,9 @@ int m3d_solver::pass_x(Spec op, Ctl* ctl, typename Cx<T>::t* sp) {
         constexpr int NN = decltype(nc)::value;
         constexpr int CPW = 32 / LineSplit<T, NN>::Tl;
         if constexpr (CC == 3 && sizeof(T) == 4 && NN <= 128 && std::is_same<Spec, SpecGreen<T, 3>>::value) {
-            if (use_xr1) {  // thermal Green operators in rank-one form
-                const int ntz = (g.Hzp + kXRegWarps * CPW - 1) / (kXRegWarps * CPW);
-                nblk = Ny * ntz;
+            if (use_xr1) {  // thermal Green operators in rank-one form; warp-granular (y, column group) items
+                const int ngrp = (g.Hzp + CPW - 1) / CPW;
+                nblk = (Ny * ngrp + kXRegWarps - 1) / kXRegWarps;
                 const size_t sm = (size_t)NN * sizeof(typename Cx<T>::t) +
                                   (size_t)kXRegWarps * CPW * RowLen<T, NN, true>::value * sizeof(typename Cx<T>::t);
                 allow_smem(k_xturn_r1<T, NN>);
