@@ -27,6 +27,19 @@ namespace m3d {
 
 constexpr int kFastThreads = 128;
 
+// CTAs per SM the FP64 z kernels of long lines (N >= 96) with up to three
+// components are compiled for: their register cap is 65536 / (128 x value)
+// per thread.  Uncapped, the 128-point thermal z inverse takes 244 registers
+// (two 4-warp CTAs per SM); at three CTAs it fits 168 with a small spill.
+// Six- and nine-component kernels keep no cap (a 168 cap spills ~1 KB).
+#ifndef M3D_FP64_MINB
+#define M3D_FP64_MINB 3
+#endif
+template <typename T, int N, int C>
+struct FastMinB {
+    static constexpr int value = (sizeof(T) == 8 && N >= 96 && C <= 3) ? M3D_FP64_MINB : 1;
+};
+
 // Shared-memory bank layout of a line's row (which is also its exchange
 // buffer).  Rows hold at least max(N, E*(T+1)) complex elements, padded so
 // that row length == `tgt` modulo the number of complex elements per
@@ -333,14 +346,17 @@ __global__ void __launch_bounds__(32 * kXRegWarps) k_xturn_reg(GridDims g, const
 // component is staged in shared memory.  The k = 0 mode, whose value is set
 // rather than computed (the load or 0), is handled in the one column holding
 // it: D(0) = 0 and the missing constant is added to every x.  Arithmetic is
-// the same to rounding (FP32); the wave vectors follow SpecGreen's sign and
+// the same to rounding (FP32 and FP64); the wave vectors follow SpecGreen's sign and
 // wrap rules exactly.
 // ---------------------------------------------------------------------------
-// CTAs per SM the rank-one x turnaround is compiled for (bounds its registers)
-template <int N> struct XR1MinB { static constexpr int value = N == 128 ? 3 : (N == 96 ? 2 : 4); };
+// CTAs per SM the rank-one x turnaround is compiled for (bounds its registers;
+// an FP64 lane holds twice the registers per point)
+template <typename T, int N> struct XR1MinB {
+    static constexpr int value = sizeof(T) == 4 ? (N == 128 ? 3 : (N == 96 ? 2 : 4)) : (N == 128 ? 2 : 3);
+};
 
 template <typename T, int N>
-__global__ void __launch_bounds__(32 * kXRegWarps, XR1MinB<N>::value) k_xturn_r1(GridDims g, const typename Cx<T>::t* __restrict__ twx,
+__global__ void __launch_bounds__(32 * kXRegWarps, XR1MinB<T, N>::value) k_xturn_r1(GridDims g, const typename Cx<T>::t* __restrict__ twx,
                                                              typename Cx<T>::t* __restrict__ spec, SpecGreenT<T> op,
                                                              const Ctl* __restrict__ ctl) {
     typedef typename Cx<T>::t C2;
@@ -534,7 +550,7 @@ __device__ __forceinline__ void z_tile_fft(C2* tile, const C2* tw) {
 }
 
 template <typename T, int N, int C, class Pro>
-__global__ void __launch_bounds__(kFastThreads) k_zfwd_fast(GridDims g, const typename Cx<T>::t* __restrict__ twz,
+__global__ void __launch_bounds__(kFastThreads, FastMinB<T, N, C>::value) k_zfwd_fast(GridDims g, const typename Cx<T>::t* __restrict__ twz,
                                                            typename Cx<T>::t* __restrict__ spec, Pro pro,
                                                            const Ctl* __restrict__ ctl) {
     typedef typename Cx<T>::t C2;
@@ -640,7 +656,7 @@ __global__ void __launch_bounds__(kFastThreads) k_zfwd_fast(GridDims g, const ty
 }
 
 template <typename T, int N, int C, class Epi, class Fin>
-__global__ void __launch_bounds__(kFastThreads) k_zinv_fast(GridDims g, const typename Cx<T>::t* __restrict__ twz,
+__global__ void __launch_bounds__(kFastThreads, FastMinB<T, N, C>::value) k_zinv_fast(GridDims g, const typename Cx<T>::t* __restrict__ twz,
                                                            const typename Cx<T>::t* __restrict__ spec, Epi epi,
                                                            Ctl* ctl, double* partials, Fin fin) {
     typedef typename Cx<T>::t C2;

@@ -313,7 +313,7 @@ struct m3d_solver {
     // thermal FP32 x turnaround with the three components in registers
     // (M3D_XTURN_STAGED=1 keeps the shared-memory-staged kernel)
     bool use_xreg = true;
-    // thermal FP32 x turnaround in rank-one form (M3D_XTURN_R1=0 turns it off)
+    // thermal x turnaround in rank-one form (M3D_XTURN_R1=0 turns it off)
     bool use_xr1 = true;
     template <typename T> bool slab_ok() const;
     template <typename T, int CC, bool MIX, class Fin>
@@ -664,7 +664,9 @@ int m3d_solver::pass_x(Spec op, Ctl* ctl, typename Cx<T>::t* sp) {
     const bool done = use_fast && with_fast_n(Nx, [&](auto nc) {
         constexpr int NN = decltype(nc)::value;
         constexpr int CPW = 32 / LineSplit<T, NN>::Tl;
-        if constexpr (CC == 3 && sizeof(T) == 4 && NN <= 128 && std::is_same<Spec, SpecGreen<T, 3>>::value) {
+        // (not FP64 at N = 96: its 24 points per lane spill at any register cap)
+        if constexpr (CC == 3 && NN <= 128 && (sizeof(T) == 4 || NN != 96) &&
+                      std::is_same<Spec, SpecGreen<T, 3>>::value) {
             if (use_xr1) {  // thermal Green operators in rank-one form; warp-granular (y, column group) items
                 const int ngrp = (g.Hzp + CPW - 1) / CPW;
                 nblk = (Ny * ngrp + kXRegWarps - 1) / kXRegWarps;

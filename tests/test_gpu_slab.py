@@ -138,11 +138,11 @@ def test_slab_multi_rve(monkeypatch):
 
 @pytest.mark.parametrize("N", [32, 64, 128])
 @pytest.mark.parametrize("km,ki", [(1.0, 100.0), (30.0, 25.0)])  # gradient-based, flux-based
-@pytest.mark.parametrize("prec,tol", [("fp32", 1e-6), ("fp32_refine", 1e-9)])
+@pytest.mark.parametrize("prec,tol", [("fp32", 1e-6), ("fp32_refine", 1e-9), ("fp64", 1e-10)])
 def test_rank_one_x_turnaround_matches_staged(N, km, ki, prec, tol, monkeypatch):
     """The thermal x turnaround in rank-one form (three forward, two inverse
     line FFTs) against the staged kernel that applies the Green operator mode
-    by mode: FP32 fields within 1e-5, refined fields within 1e-8."""
+    by mode: FP32 fields within 1e-5, refined and FP64 fields within 1e-8."""
     shape = (N, N, N)
     rve = sphere_rve(shape, N / 4, center=(N / 2 + 1, N / 2, N / 2 - 1))
     E = np.array([0.2, 0.3, 1.0])
