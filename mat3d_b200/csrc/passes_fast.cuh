@@ -461,6 +461,193 @@ __global__ void __launch_bounds__(32 * kXRegWarps, XR1MinB<T, N>::value) k_xturn
 }
 
 // ---------------------------------------------------------------------------
+// The rank-one x turnaround with its column loads staged by TMA.  A warp walks
+// work items (entry, y, group of CPW kz columns) persistently; each component
+// of an item is one 3-D box (CPW columns x 1 row x N points along x) copied
+// into one of the warp's two slots.  The copies of a warp form one sequence
+// (item k, component c) = copy 3k + c, slot (3k + c) mod 2, and copy m + 2 is
+// requested as soon as copy m has been read and transformed: a copy is in
+// flight while the previous one is transformed, across item boundaries, so
+// the loads' latency is hidden by the transforms.  Columns past Hzp (the short last group) are
+// zero-filled by the copy, as the plain kernel zero-fills them.  The
+// arithmetic is k_xturn_r1's, operation for operation, so the two give equal
+// bits.  Every barrier wait is bounded: on expiry the error word is set, the
+// warp waits (bounded) for the copies it still has in flight and stops.
+// ---------------------------------------------------------------------------
+template <typename T, int N>
+struct XR1Tma {
+    typedef typename Cx<T>::t C2;
+    static constexpr int E = LineSplit<T, N>::E, TL = LineSplit<T, N>::Tl, CPW = 32 / TL;
+    static constexpr int RL = RowLen<T, N, true>::value;
+    static constexpr int SLOT = N * CPW;  // complex elements per slot: [x][column]
+    static constexpr uint32_t slot_bytes = (uint32_t)(SLOT * sizeof(C2));
+    static_assert(slot_bytes % 128 == 0, "slots stay 128-byte aligned");
+    static constexpr size_t smem() {
+        return 128 + (size_t)kXRegWarps * 2 * slot_bytes + (size_t)N * sizeof(C2) +
+               (size_t)kXRegWarps * CPW * RL * sizeof(C2) + 16 + (size_t)kXRegWarps * 2 * sizeof(uint64_t);
+    }
+};
+
+// CTAs per SM: those of the plain kernel (at FP32 N = 128 three, 168
+// registers; a 128-register cap for four CTAs -- every 128^3 work item in one
+// round -- spills and measured the same, 25.2 us per launch)
+#ifndef M3D_XR1TMA_MINB
+#define M3D_XR1TMA_MINB 0
+#endif
+template <typename T, int N> struct XR1TmaMinB {
+    static constexpr int value = M3D_XR1TMA_MINB > 0 ? M3D_XR1TMA_MINB : XR1MinB<T, N>::value;
+};
+
+template <typename T, int N>
+__global__ void __launch_bounds__(32 * kXRegWarps, XR1TmaMinB<T, N>::value)
+    k_xturn_r1_tma(const __grid_constant__ CUtensorMap map, GridDims g, const typename Cx<T>::t* __restrict__ twx,
+                   typename Cx<T>::t* __restrict__ spec, SpecGreenT<T> op, const Ctl* __restrict__ ctl, int nitems,
+                   int* err) {
+    typedef typename Cx<T>::t C2;
+    typedef XR1Tma<T, N> X;
+    constexpr int C = 3;
+    constexpr int E = X::E, TL = X::TL, CPW = X::CPW, RL = X::RL;
+    extern __shared__ __align__(16) char smem_raw[];
+    C2* stage = (C2*)align_up(smem_raw, 128);
+    C2* tw = stage + kXRegWarps * 2 * X::SLOT;
+    C2* xch = tw + N;
+    uint64_t* bars = (uint64_t*)align_up((char*)(xch + kXRegWarps * CPW * RL), 16);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int col = lane % CPW, t = lane / CPW;
+    for (int i = threadIdx.x; i < N; i += blockDim.x) tw[i] = twx[i];
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < kXRegWarps * 2; ++s) mbar_init(&bars[s], 1);
+        mbar_fence_init();
+    }
+    __syncthreads();  // the only block barrier
+    C2* st = stage + warp * 2 * X::SLOT;
+    uint64_t* bar = bars + warp * 2;
+    C2* xl = xch + (warp * CPW + col) * RL;
+    const int sw = RowLen<T, N, true>::sw ? (col & 1) : 0;
+    const int ngrp = (g.Hzp + CPW - 1) / CPW;
+    const int per_entry = g.Ny * ngrp;
+    const int wstride = gridDim.x * kXRegWarps;
+    const long long cstride = g.NL * g.Hzp;            // component stride
+    const long long xstride = (long long)g.Ny * g.Hzp;  // x stride
+    // this warp's next item (from `it` on) whose entry is still iterating
+    auto next = [&](int it) {
+        for (; it < nitems; it += wstride)
+            if (!ctl[it / per_entry].done) return it;
+        return -1;
+    };
+    auto issue = [&](int m, int it) {  // lane 0: copy m (component m % 3 of item `it`) into slot m % 2
+        const int b = it / per_entry, rem = it - b * per_entry;
+        const int y = rem / ngrp, grp = rem - y * ngrp;
+        mbar_expect_tx(&bar[m & 1], X::slot_bytes);
+        tma_load_3d(st + (m & 1) * X::SLOT, &map, 2 * grp * CPW, y, (b * C + m % 3) * g.Nx, &bar[m & 1]);
+    };
+    int it = next(blockIdx.x * kXRegWarps + warp);
+    int issued = 0;  // copies requested so far (warp-uniform)
+    if (it >= 0) {
+        if (lane == 0) {
+            issue(0, it);
+            issue(1, it);
+        }
+        issued = 2;
+    }
+    int m = 0;  // the next copy to consume
+    while (it >= 0) {
+        const int nx = next(it + wstride);
+        const int b = it / per_entry, rem = it - b * per_entry;
+        const int y = rem / ngrp;
+        const int kz = (rem - y * ngrp) * CPW + col;
+        const bool ok = kz < g.Hzp;
+        op.prepare(ctl, b);
+        C2* base = spec + ((long long)b * C * g.NL + y) * g.Hzp + (ok ? kz : 0);
+        const bool grad = op.kind == GREEN_TGRAD;
+        const T fz = (T)sfreq(kz, op.pos_nyq ? g.Nz / 2 : (g.Nz - 1) / 2, g.Nz);
+        const T fy = (T)sfreq(y, op.pos_nyq ? g.Ny / 2 : (g.Ny - 1) / 2, g.Ny);
+        const bool origin = ok && y == 0 && kz == 0;
+        C2 v[E], d[E];
+        T fx[E];  // x frequency of each of this lane's modes
+        C2 k0[C];
+#pragma unroll
+        for (int r = 0; r < E; ++r) {
+            fx[r] = (T)sfreq(spec_mode<E, TL>(t, r), op.pos_nyq ? g.Nx / 2 : (g.Nx - 1) / 2, op.xwrap);
+            d[r] = mk<C2>(0, 0);
+        }
+        bool failed = false;
+#pragma unroll 1
+        for (int c = 0; c < C; ++c, ++m) {
+            const bool arrived = mbar_wait(&bar[m & 1], (uint32_t)((m >> 1) & 1), err);
+            if (__any_sync(0xffffffffu, !arrived)) { failed = true; break; }
+            const C2* sl = st + (m & 1) * X::SLOT;
+#pragma unroll
+            for (int j = 0; j < E; ++j) v[j] = sl[(t + TL * j) * CPW + col];
+            line_fwd<C2, E, TL>(v, t, xl, tw, sw);
+            // the slot is refilled only after every lane's reads of it have
+            // returned (the transform consumed them; line_fwd ends with a warp
+            // barrier) and a proxy fence orders them before the copy's writes
+            const int it2 = c == 0 ? it : nx;  // copy m + 2: this item's component 2, or the next item's 0 and 1
+            if (it2 >= 0) {
+                if (lane == 0) {
+                    fence_proxy_async();
+                    issue(m + 2, it2);
+                }
+                issued = m + 3;
+            }
+            const C2 m0 = mk<C2>(__shfl_sync(0xffffffffu, v[0].x, col), __shfl_sync(0xffffffffu, v[0].y, col));
+            if (c == 0) k0[0] = m0;
+            else if (c == 1) k0[1] = m0;
+            else k0[2] = m0;
+            const T fcol = c == 0 ? fz : fy;
+#pragma unroll
+            for (int r = 0; r < E; ++r) {
+                const T fc = c == 2 ? fx[r] : fcol;
+                d[r] = mk<C2>(d[r].x + fc * v[r].x, d[r].y + fc * v[r].y);
+            }
+        }
+        if (failed) {
+            // wait (bounded, no further error) for the copies still in flight: m .. issued - 1
+            for (int q = m; q < issued; ++q) mbar_wait(&bar[q & 1], (uint32_t)((q >> 1) & 1), nullptr, 1 << 16);
+            return;
+        }
+#pragma unroll
+        for (int r = 0; r < E; ++r) {
+            const int mode = spec_mode<E, TL>(t, r);
+            const T n2 = fz * fz + fy * fy + fx[r] * fx[r];
+            const T coef = (origin && mode == 0) ? (T)0 : (grad ? -op.p1 : (T)1) / n2;
+            d[r] = mk<C2>(coef * d[r].x, coef * d[r].y);
+            v[r] = mk<C2>(fx[r] * d[r].x, fx[r] * d[r].y);
+        }
+        C2 add[C] = {mk<C2>(0, 0), mk<C2>(0, 0), mk<C2>(0, 0)};
+        if (origin) {
+#pragma unroll
+            for (int c = 0; c < C; ++c) {
+                const T kc = op.zero_k0 ? (T)0 : (T)ctl[b].kzero[c];
+                add[c] = grad ? mk<C2>(kc, 0) : mk<C2>(kc + op.p1 * k0[c].x, op.p1 * k0[c].y);
+            }
+        }
+        const T sc = grad ? (T)1 : op.p1;
+        auto emit = [&](int c, const C2 (&u)[E], T f) {
+#pragma unroll
+            for (int j = 0; j < E; ++j) {
+                C2* p = base + c * cstride + (long long)(t + TL * j) * xstride;
+                C2 o = mk<C2>(sc * f * u[j].x, sc * f * u[j].y);
+                if (!grad) {
+                    const C2 in = *p;
+                    o = mk<C2>(o.x - op.p1 * (T)N * in.x, o.y - op.p1 * (T)N * in.y);
+                }
+                *p = mk<C2>(o.x + add[c].x, o.y + add[c].y);
+            }
+        };
+        line_inv<C2, E, TL>(d, t, xl, tw, sw);
+        if (ok) {
+            emit(0, d, fz);
+            emit(1, d, fy);
+        }
+        line_inv<C2, E, TL>(v, t, xl, tw, sw);
+        if (ok) emit(2, v, (T)1);
+        it = nx;
+    }
+}
+
+// ---------------------------------------------------------------------------
 // z passes.  Tile of G voxel lines x NCL complex lines (NCL = ceil(C/2)).
 // ---------------------------------------------------------------------------
 template <int C> struct NclOf { static constexpr int value = (C + 1) / 2; };

@@ -304,6 +304,14 @@ struct m3d_solver {
     int ymap_B = -1;
     int* d_err = nullptr;  // device-side error word (bounded waits that expired)
     bool ensure_ymaps(int CC);
+    // TMA-staged rank-one x turnaround (thermal, FP32): a 3-D map of the half
+    // spectrum, boxes of cpw columns x 1 row x Nx points (M3D_XTURN_TMA=0
+    // keeps the plain rank-one kernel)
+    bool use_xr1_tma = true;
+    CUtensorMap xmap32{};
+    const void* xmap_base = nullptr;
+    int xmap_B = -1, xmap_cpw = -1;
+    bool ensure_xmap(int cpw);
     bool use_fast = true;
     // two-pass sweeps (x turnaround + y-z slab pass) where the operators are
     // per-component and the slab fits two CTAs per SM; M3D_NO_SLAB=1 keeps
@@ -399,6 +407,7 @@ int m3d_solver::alloc(int batch) {
         M3D_CUDA(cudaMemset(d_err, 0, sizeof(int)));
     }
     ymap_base = nullptr;  // tensor maps name the old spectrum
+    xmap_base = nullptr;
     cudaFree(d_x); cudaFree(d_delta); cudaFree(d_r32); cudaFree(d_spec); cudaFree(d_part);
     cudaFree(d_ctl); cudaFree(d_ctl_in);
     if (h_ctl) cudaFreeHost(h_ctl);
@@ -619,6 +628,28 @@ bool m3d_solver::ensure_ymaps(int CC) {
     return true;
 }
 
+// Tensor map of the FP32 half spectrum for the TMA-staged rank-one x
+// turnaround: 3-D, (2*Hzp scalars, Ny rows, B*3*Nx lines), boxes of cpw
+// complex columns x 1 row x Nx lines (one component of one work item).
+bool m3d_solver::ensure_xmap(int cpw) {
+    if (xmap_base == d_spec && xmap_B == B && xmap_cpw == cpw) return true;
+    auto enc = tensor_map_encoder();
+    const long long L = (long long)B * 3 * Nx;
+    if (!enc || L >= (1LL << 31) || Nx > 256 || !d_err) return false;
+    const cuuint64_t dims[3] = {(cuuint64_t)2 * g.Hzp, (cuuint64_t)Ny, (cuuint64_t)L};
+    const cuuint64_t strides[2] = {(cuuint64_t)g.Hzp * 8, (cuuint64_t)Ny * g.Hzp * 8};
+    const cuuint32_t box[3] = {(cuuint32_t)(2 * cpw), 1, (cuuint32_t)Nx};
+    const cuuint32_t estr[3] = {1, 1, 1};
+    const CUresult r = enc(&xmap32, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, d_spec, dims, strides, box, estr,
+                           CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                           CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return false;
+    xmap_base = d_spec;
+    xmap_B = B;
+    xmap_cpw = cpw;
+    return true;
+}
+
 template <typename T>
 void m3d_solver::pass_y(int sign, int CC, Ctl* ctl, typename Cx<T>::t* sp) {
     typedef typename Cx<T>::t C2;
@@ -669,6 +700,25 @@ int m3d_solver::pass_x(Spec op, Ctl* ctl, typename Cx<T>::t* sp) {
                       std::is_same<Spec, SpecGreen<T, 3>>::value) {
             if (use_xr1) {  // thermal Green operators in rank-one form; warp-granular (y, column group) items
                 const int ngrp = (g.Hzp + CPW - 1) / CPW;
+                if constexpr (sizeof(T) == 4) {
+                    if (use_xr1_tma && (void*)sp == d_spec && ensure_xmap(CPW)) {  // column loads staged by TMA
+                        typedef XR1Tma<T, NN> X;
+                        auto kern = k_xturn_r1_tma<T, NN>;
+                        allow_smem(kern);
+                        static const int slots = [kern] {  // resident CTAs per SM x SMs
+                            int per_sm = 1, dev = 0, nsm = 148;
+                            cudaGetDevice(&dev);
+                            cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+                            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kXRegWarps * 32, X::smem());
+                            (void)cudaGetLastError();
+                            return std::max(1, per_sm) * nsm;
+                        }();
+                        const int nitems = B * Ny * ngrp;
+                        nblk = std::max(1, std::min((nitems + kXRegWarps - 1) / kXRegWarps, slots));
+                        kern<<<nblk, kXRegWarps * 32, X::smem(), stream>>>(xmap32, g, tw<T>(0), sp, op, ctl, nitems, d_err);
+                        return;
+                    }
+                }
                 nblk = (Ny * ngrp + kXRegWarps - 1) / kXRegWarps;
                 const size_t sm = (size_t)NN * sizeof(typename Cx<T>::t) +
                                   (size_t)kXRegWarps * CPW * RowLen<T, NN, true>::value * sizeof(typename Cx<T>::t);
@@ -1224,7 +1274,7 @@ int m3d_solver::run_refine_graph(double tol_field, int max_iter) {
 
 int m3d_solver::dispatch_run(double tol_field, double tol_eq, int nInc, int criterion, int max_iter) {
     int rc = dispatch_core(tol_field, tol_eq, nInc, criterion, max_iter);
-    if (use_tma_y && d_err) {
+    if (d_err) {  // the TMA-staged passes' bounded waits
         int e = 0;
         if (cudaMemcpy(&e, d_err, sizeof(int), cudaMemcpyDeviceToHost) == cudaSuccess && e) {
             cudaMemset(d_err, 0, sizeof(int));
@@ -1403,6 +1453,8 @@ static int create_impl(int kind, int Nx, int Ny, int Nz, int behav, int precisio
         h->slab_nt = (e7 && std::atoi(e7) == 512) ? 512 : 256;
         const char* e8 = std::getenv("M3D_XTURN_R1");
         h->use_xr1 = !(e8 && e8[0] == '0');
+        const char* e9 = std::getenv("M3D_XTURN_TMA");
+        h->use_xr1_tma = !(e9 && e9[0] == '0');
         const char* e6 = std::getenv("M3D_XTURN_STAGED");
         h->use_xreg = !(e6 && e6[0] == '1');
     }

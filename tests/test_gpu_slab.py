@@ -152,3 +152,25 @@ def test_rank_one_x_turnaround_matches_staged(N, km, ki, prec, tol, monkeypatch)
         (a,), st = thermal_solve(shape, km, ki, rve, E, prec, tol, monkeypatch, slab=True)
         out.append(a)
     assert rel(out[0], out[1]) < (1e-5 if prec == "fp32" else 1e-8), rel(out[0], out[1])
+
+
+@pytest.mark.parametrize("N", [32, 48, 64, 96, 128])
+@pytest.mark.parametrize("km,ki", [(1.0, 100.0), (30.0, 25.0)])  # gradient-based, flux-based
+@pytest.mark.parametrize("prec,tol,batch", [("fp32", 1e-6, 1), ("fp32_refine", 1e-9, 1), ("fp32", 1e-6, 3)])
+def test_tma_staged_rank_one_is_bitwise_equal(N, km, ki, prec, tol, batch, monkeypatch):
+    """The rank-one x turnaround with its column loads staged by TMA does the
+    plain rank-one kernel's arithmetic: equal fields and sweep counts, also
+    with several entries converging at different sweeps (batch 3: the load
+    rolled per entry) and on a grid whose last column group is short."""
+    shape = (N, N, N)
+    rve = sphere_rve(shape, N / 4, center=(N / 2 + 1, N / 2, N / 2 - 1))
+    E = np.array([0.2, 0.3, 1.0])
+    out, sts = [], []
+    for tma in ("1", "0"):
+        monkeypatch.setenv("M3D_XTURN_TMA", tma)
+        f, st = thermal_solve(shape, km, ki, rve, E, prec, tol, monkeypatch, slab=True, batch=batch)
+        out.append(f)
+        sts.append(st)
+    assert sts[0]["sweeps"] == sts[1]["sweeps"]
+    for a, b in zip(*out):
+        assert np.array_equal(a, b)
