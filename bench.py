@@ -90,11 +90,13 @@ def pass_bytes(c, w, N, forcing, two_pass=False):
     return (zfwd, 2 * spec, 2 * spec, 2 * spec, zinv)
 
 
-# DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum, warm
-# cache) from the ncu capture summarised in
-# profiles/thermal128_fp32_sweep_kernels.md, keyed (workload, pass, word bytes)
+# DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) from
+# the ncu captures summarised in profiles/, keyed (workload, pass, word bytes):
+# the five-pass z inverse with a warm cache, the y-z slab pass of the two-pass
+# sweep from a --set full capture (cold cache: ncu flushes the caches first)
 MEASURED_TRAFFIC = {
     ("thermal128", "z_inverse", 4): (12.0e6, "profiles/thermal128_fp32_sweep_kernels.md"),
+    ("thermal128", "yz_slab", 4): (81.8e6, "profiles/thermal128_fp32_two_pass_sweep.md"),
 }
 
 
