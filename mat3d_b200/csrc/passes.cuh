@@ -23,7 +23,17 @@ struct GridDims {
     int Nx, Ny, Nz, Hz, Hzp;
     long long V;   // Nx*Ny*Nz
     long long NL;  // Nx*Ny (z lines)
+    // compacted launches: live[0] = number of entries still iterating,
+    // live[1..] their ids in order; the launch's entry slots (blockIdx.y)
+    // index this list.  Null: slot = entry.
+    const int* live = nullptr;
 };
+
+// Batch entry of launch slot s; -1 for a slot past the live list.
+__device__ __forceinline__ int entry_of(const GridDims& g, int s) {
+    if (!g.live) return s;
+    return s < g.live[0] ? g.live[1 + s] : -1;
+}
 
 // Per batch entry control block (device memory).
 struct Ctl {
@@ -123,8 +133,8 @@ __global__ void __launch_bounds__(256) k_zfwd(GridDims g, LinePlan pz, const typ
                                               typename Cx<T>::t* __restrict__ spec, Pro pro, const Ctl* __restrict__ ctl,
                                               int G, double* partials) {
     typedef typename Cx<T>::t C2;
-    const int b = blockIdx.y;
-    if (ctl[b].done) return;
+    const int b = entry_of(g, blockIdx.y);
+    if (b < 0 || ctl[b].done) return;
     extern __shared__ __align__(16) char smem_raw[];
     const int Nz = g.Nz;
     const int npairs = G / 2;
@@ -191,9 +201,9 @@ __global__ void __launch_bounds__(256) k_ypass(GridDims g, LinePlan py, const ty
                                                typename Cx<T>::t* __restrict__ spec, int TZ, int C, int sign,
                                                const Ctl* __restrict__ ctl) {
     typedef typename Cx<T>::t C2;
-    const int cb = blockIdx.y;
-    const int b = cb / C;
-    if (ctl[b].done) return;
+    const int b = entry_of(g, blockIdx.y / C);
+    if (b < 0 || ctl[b].done) return;
+    const int cb = b * C + blockIdx.y % C;
     extern __shared__ __align__(16) char smem_raw[];
     const int Ny = g.Ny, Hzp = g.Hzp;
     C2* tw = (C2*)smem_raw;
@@ -226,8 +236,8 @@ __global__ void __launch_bounds__(256) k_xturn(GridDims g, LinePlan px, const ty
                                                typename Cx<T>::t* __restrict__ spec, int TZ, Spec op,
                                                const Ctl* __restrict__ ctl, double* partials) {
     typedef typename Cx<T>::t C2;
-    const int b = blockIdx.y;
-    if (ctl[b].done) return;
+    const int b = entry_of(g, blockIdx.y);
+    if (b < 0 || ctl[b].done) return;
     op.prepare(ctl, b);
     extern __shared__ __align__(16) char smem_raw[];
     const int Nx = g.Nx, Ny = g.Ny, Hzp = g.Hzp;
@@ -289,8 +299,8 @@ __global__ void __launch_bounds__(256) k_zinv(GridDims g, LinePlan pz, const typ
                                               const typename Cx<T>::t* __restrict__ spec, Epi epi, Ctl* ctl, int G,
                                               double* partials, Fin fin) {
     typedef typename Cx<T>::t C2;
-    const int b = blockIdx.y;
-    if (ctl[b].done) return;
+    const int b = entry_of(g, blockIdx.y);
+    if (b < 0 || ctl[b].done) return;
     extern __shared__ __align__(16) char smem_raw[];
     const int Nz = g.Nz, Hz = g.Hz, Hzp = g.Hzp;
     const int npairs = G / 2;

@@ -95,8 +95,9 @@ __global__ void __launch_bounds__(kFastThreads) k_ypass_fast(GridDims g, const t
     typedef typename Cx<T>::t C2;
     constexpr int E = LineSplit<T, N>::E, TL = LineSplit<T, N>::Tl, CPW = 32 / TL;
     constexpr int XS = RowLen<T, N, true>::value;
-    const int cb = blockIdx.y;
-    if (ctl[cb / C].done) return;
+    const int b = entry_of(g, blockIdx.y / C);
+    if (b < 0 || ctl[b].done) return;
+    const int cb = b * C + blockIdx.y % C;
     extern __shared__ __align__(16) char smem_raw[];
     C2* tw = (C2*)smem_raw;
     C2* xch = tw + N;
@@ -172,8 +173,8 @@ __global__ void __launch_bounds__(kFastThreads) k_xturn_fast(GridDims g, const t
     constexpr int E = LineSplit<T, N>::E, TL = LineSplit<T, N>::Tl, CPW = 32 / TL;
     constexpr int WPC = XWarps<T, N, C>::value;
     constexpr int RL = RowLen<T, N, true>::value;
-    const int b = blockIdx.y;
-    if (ctl[b].done) return;
+    const int b = entry_of(g, blockIdx.y);
+    if (b < 0 || ctl[b].done) return;
     op.prepare(ctl, b);
     extern __shared__ __align__(16) char smem_raw[];
     C2* tw = (C2*)smem_raw;
@@ -279,8 +280,8 @@ __global__ void __launch_bounds__(32 * kXRegWarps) k_xturn_reg(GridDims g, const
     constexpr int C = 3;
     constexpr int E = LineSplit<T, N>::E, TL = LineSplit<T, N>::Tl, CPW = 32 / TL;
     constexpr int RL = RowLen<T, N, true>::value;
-    const int b = blockIdx.y;
-    if (ctl[b].done) return;
+    const int b = entry_of(g, blockIdx.y);
+    if (b < 0 || ctl[b].done) return;
     op.prepare(ctl, b);
     extern __shared__ __align__(16) char smem_raw[];
     C2* tw = (C2*)smem_raw;
@@ -363,8 +364,8 @@ __global__ void __launch_bounds__(32 * kXRegWarps, XR1MinB<T, N>::value) k_xturn
     constexpr int C = 3;
     constexpr int E = LineSplit<T, N>::E, TL = LineSplit<T, N>::Tl, CPW = 32 / TL;
     constexpr int RL = RowLen<T, N, true>::value;
-    const int b = blockIdx.y;
-    if (ctl[b].done) return;
+    const int b = entry_of(g, blockIdx.y);
+    if (b < 0 || ctl[b].done) return;
     op.prepare(ctl, b);
     extern __shared__ __align__(16) char smem_raw[];
     C2* tw = (C2*)smem_raw;
@@ -530,13 +531,16 @@ __global__ void __launch_bounds__(32 * kXRegWarps, XR1TmaMinB<T, N>::value)
     const long long cstride = g.NL * g.Hzp;            // component stride
     const long long xstride = (long long)g.Ny * g.Hzp;  // x stride
     // this warp's next item (from `it` on) whose entry is still iterating
+    // (items are numbered over the launch's entry slots)
     auto next = [&](int it) {
-        for (; it < nitems; it += wstride)
-            if (!ctl[it / per_entry].done) return it;
+        for (; it < nitems; it += wstride) {
+            const int b = entry_of(g, it / per_entry);
+            if (b >= 0 && !ctl[b].done) return it;
+        }
         return -1;
     };
     auto issue = [&](int m, int it) {  // lane 0: copy m (component m % 3 of item `it`) into slot m % 2
-        const int b = it / per_entry, rem = it - b * per_entry;
+        const int s = it / per_entry, rem = it - s * per_entry, b = entry_of(g, s);
         const int y = rem / ngrp, grp = rem - y * ngrp;
         mbar_expect_tx(&bar[m & 1], X::slot_bytes);
         tma_load_3d(st + (m & 1) * X::SLOT, &map, 2 * grp * CPW, y, (b * C + m % 3) * g.Nx, &bar[m & 1]);
@@ -553,7 +557,7 @@ __global__ void __launch_bounds__(32 * kXRegWarps, XR1TmaMinB<T, N>::value)
     int m = 0;  // the next copy to consume
     while (it >= 0) {
         const int nx = next(it + wstride);
-        const int b = it / per_entry, rem = it - b * per_entry;
+        const int s = it / per_entry, rem = it - s * per_entry, b = entry_of(g, s);
         const int y = rem / ngrp;
         const int kz = (rem - y * ngrp) * CPW + col;
         const bool ok = kz < g.Hzp;
@@ -742,8 +746,8 @@ __global__ void __launch_bounds__(kFastThreads, FastMinB<T, N, C>::value) k_zfwd
                                                            const Ctl* __restrict__ ctl) {
     typedef typename Cx<T>::t C2;
     typedef ZTile<T, N, C> Z;
-    const int b = blockIdx.y;
-    if (ctl[b].done) return;
+    const int b = entry_of(g, blockIdx.y);
+    if (b < 0 || ctl[b].done) return;
     pro.bind(b);
     extern __shared__ __align__(16) char smem_raw[];
     C2* tw = (C2*)smem_raw;
@@ -848,8 +852,8 @@ __global__ void __launch_bounds__(kFastThreads, FastMinB<T, N, C>::value) k_zinv
                                                            Ctl* ctl, double* partials, Fin fin) {
     typedef typename Cx<T>::t C2;
     typedef ZTile<T, N, C> Z;
-    const int b = blockIdx.y;
-    if (ctl[b].done) return;
+    const int b = entry_of(g, blockIdx.y);
+    if (b < 0 || ctl[b].done) return;
     epi.bind(b);
     extern __shared__ __align__(16) char smem_raw[];
     C2* tw = (C2*)smem_raw;
@@ -1018,12 +1022,15 @@ __global__ void __launch_bounds__(kFastThreads) k_ypass_tma(const __grid_constan
     __syncthreads();
     // the tiles of this CTA whose entry is still iterating, in order
     auto next = [&](int id) {
-        for (; id < ntiles; id += gridDim.x)
-            if (!ctl[(id / per_cb) / C].done) return id;
+        for (; id < ntiles; id += gridDim.x) {
+            const int b = entry_of(g, (id / per_cb) / C);
+            if (b >= 0 && !ctl[b].done) return id;
+        }
         return -1;
     };
     auto coords = [&](int id, int& c0, int& r0) {
-        const int cb = id / per_cb, rem = id - cb * per_cb;
+        const int scb = id / per_cb, rem = id - scb * per_cb;  // (entry slot, component), then (x, kz tile)
+        const int cb = entry_of(g, scb / C) * C + scb % C;
         const int x = rem / ntz, kzt = rem - x * ntz;
         r0 = (cb * g.Nx + x) * N;
         c0 = 2 * kzt * Y::KC;

@@ -237,8 +237,8 @@ __global__ void __launch_bounds__(NT, SlabGeom<T, N, NT>::MINB)
     typedef typename Cx<T>::t C2;
     typedef SlabGeom<T, N, NT> G;
     constexpr int E = G::E, TL = G::TL, CPW = G::CPW, SP = G::SP, ROW = G::ROW;
-    const int b = blockIdx.y;
-    if (ctl[b].done) return;
+    const int b = entry_of(g, blockIdx.y);
+    if (b < 0 || ctl[b].done) return;
     const int C = ops.C;
     const int c = blockIdx.x / g.Nx, x = blockIdx.x - c * g.Nx;
     extern __shared__ __align__(16) char smem_raw[];
