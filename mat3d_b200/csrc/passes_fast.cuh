@@ -18,6 +18,8 @@
 // epilogue's global loads are issued before the tile FFT so their latency
 // overlaps it.
 #pragma once
+#include <type_traits>
+
 #include "fft_reg.cuh"
 #include "passes.cuh"
 #include "physics.cuh"
@@ -846,8 +848,30 @@ __global__ void __launch_bounds__(kFastThreads, FastMinB<T, N, C>::value) k_zfwd
     }
 }
 
+// Epilogue items per thread loaded before the z inverse's transform (the
+// rest after it).  Six FP32 components: one (the 96-point tile holds two per
+// thread), so that the kernel fits the 168 registers of three CTAs per SM.
+#ifndef M3D_ZINV_PF6
+#define M3D_ZINV_PF6 1
+#endif
+template <typename T, int C, class Epi> struct ZinvPrefetch {
+    static constexpr int value = (sizeof(T) == 4 && std::is_same<Epi, EpiEM<T, 6>>::value) ? M3D_ZINV_PF6 : 64;
+};
+
+// CTAs per SM of the z inverse: FastMinB, and three for the six-component
+// FP32 EM update of the elastic sweeps (uncapped it takes 250-255 registers,
+// two CTAs per SM; capped at 168 it spills 0-16 bytes and the batch
+// workload's z inverse runs 22-28% faster).
+#ifndef M3D_F32C6_MINB
+#define M3D_F32C6_MINB 3
+#endif
+template <typename T, int N, int C, class Epi> struct ZinvMinB {
+    static constexpr int value =
+        (sizeof(T) == 4 && std::is_same<Epi, EpiEM<T, 6>>::value) ? M3D_F32C6_MINB : FastMinB<T, N, C>::value;
+};
+
 template <typename T, int N, int C, class Epi, class Fin>
-__global__ void __launch_bounds__(kFastThreads, FastMinB<T, N, C>::value) k_zinv_fast(GridDims g, const typename Cx<T>::t* __restrict__ twz,
+__global__ void __launch_bounds__(kFastThreads, ZinvMinB<T, N, C, Epi>::value) k_zinv_fast(GridDims g, const typename Cx<T>::t* __restrict__ twz,
                                                            const typename Cx<T>::t* __restrict__ spec, Epi epi,
                                                            Ctl* ctl, double* partials, Fin fin) {
     typedef typename Cx<T>::t C2;
@@ -874,13 +898,15 @@ __global__ void __launch_bounds__(kFastThreads, FastMinB<T, N, C>::value) k_zinv
             cp_async_pair(raw + gc * Hzp + 2 * k2, okl ? ib + c * cst + gi * Hzp + 2 * k2 : ib, okl);
         }
     }
-    // epilogue loads do not depend on the transform: issue them meanwhile
+    // epilogue loads do not depend on the transform: issue the first PF of
+    // them meanwhile, the rest after it
     constexpr int W = Epi::kW;
     constexpr int NV = Z::TOT / W, PERW = (NV + kFastThreads - 1) / kFastThreads;
-    typename PreOf<Epi>::type pre[Epi::kPrefetch ? PERW : 1];
-    if constexpr (Epi::kPrefetch) {
+    constexpr int PF = Epi::kPrefetch ? (ZinvPrefetch<T, C, Epi>::value < PERW ? ZinvPrefetch<T, C, Epi>::value : PERW) : 0;
+    typename PreOf<Epi>::type pre[PF > 0 ? PF : 1];
+    if constexpr (PF > 0) {
 #pragma unroll
-        for (int k = 0; k < PERW; ++k) {
+        for (int k = 0; k < PF; ++k) {
             const int i = (threadIdx.x + k * kFastThreads) * W;
             const int gi = i / N, z = i - gi * N;
             if (i < Z::TOT && l0 + gi < g.NL) {
@@ -951,9 +977,11 @@ __global__ void __launch_bounds__(kFastThreads, FastMinB<T, N, C>::value) k_zinv
             }
         }
         if constexpr (W > 1) {
-            epi.apply_prew(pre[k], l * N + z0, xc, acc);
+            if (k < PF) epi.apply_prew(pre[k < PF ? k : 0], l * N + z0, xc, acc);
+            else epi.apply_prew(epi.loadw(l * N + z0), l * N + z0, xc, acc);
         } else if constexpr (Epi::kPrefetch) {
-            epi.apply_pre(pre[k], b, l * N + z0, xc[0], acc);
+            if (k < PF) epi.apply_pre(pre[k < PF ? k : 0], b, l * N + z0, xc[0], acc);
+            else epi.apply_pre(epi.load(b, l * N + z0), b, l * N + z0, xc[0], acc);
         } else {
             epi.apply(b, l * N + z0, xc[0], acc);
         }
