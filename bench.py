@@ -869,7 +869,8 @@ def main():
                     help="default workload only: skip the other configs' summaries")
     ap.add_argument("--profile-passes", action="store_true",
                     help="single-RVE workloads: K solves on the host-driven sweep loop with CUDA events around "
-                         "every pass (the launch sequence an ncu capture sees), print the per-pass times")
+                         "every pass (the launch sequence an ncu capture sees), print the per-pass times; "
+                         "batch512: the same for each grid-size group of its first 128 RVEs")
     args = ap.parse_args()
     w = WORKLOADS[args.workload]
 
@@ -890,6 +891,9 @@ def main():
     if world > 1:
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+    if args.profile_passes and w["kind"] == "batch":
+        print(json.dumps(profile_batch_groups(args, w)))
+        return
     if w["kind"] in ("batch", "serve", "2d", "rec"):
         {"batch": run_batch, "serve": run_serve, "2d": run_2d, "rec": run_rec}[w["kind"]](args, w, rank, world, local)
         if world > 1:
@@ -905,6 +909,41 @@ def main():
         print(json.dumps(line))
     if world > 1:
         dist.destroy_process_group()
+
+
+def profile_batch_groups(args, w):
+    """Per-pass CUDA-event times of the batched homogenization's grid-size
+    groups: the batch workload's generator with its first EXTRA_BATCH_COUNT
+    RVEs, each group one multi-RVE solver (every RVE with its 6 load cases as
+    entries) run once with the host-driven loop.  Per group: entry sweeps, the
+    launch rounds (trips) and the summed pass times of the FP32 and FP64
+    sweeps."""
+    import mat3d_b200 as m3d
+    from mat3d_b200 import rve as R
+    names = ["z_forward", "y_forward", "x_turnaround", "y_inverse", "z_inverse"]
+    desc = R.batch_rves(EXTRA_BATCH_COUNT)
+    groups = {}
+    for d in desc:
+        groups.setdefault(d[1], []).append(d)
+    out = {"workload": args.workload, "rves": len(desc), "precision": w["precision"], "tol": w["tol"], "groups": {}}
+    for N, ds in sorted(groups.items()):
+        mem = [R.batch_member(*d) for d in ds]
+        s = m3d.Solver(m3d.KIND_MECH, N, N, N, m3d.ELASTIC, w["precision"], nrve=len(ds), nload=6)
+        for r, (g, mat, _) in enumerate(mem):
+            s.set_material_mech(mat, g, rve=r)
+        s.set_profiling(True)
+        s.homogenize(w["tol"])
+        p, st = s.profile(), s.stats()
+        r = {"rves": len(ds), "entries": 6 * len(ds), "entry_sweeps_fp32": st["sweeps_fp32"],
+             "entry_sweeps_fp64": st["sweeps_fp64"]}
+        for tag in ("fp32", "fp64"):
+            if p[f"n_{tag}"]:
+                r[f"trips_{tag}"] = p[f"n_{tag}"]
+                r[f"ms_{tag}"] = p[f"ms_{tag}"]
+                r[f"pass_ms_{tag}"] = {names[q]: p[f"pass_ms_{tag}"][q] for q in range(5)}
+        out["groups"][N] = r
+        s.close()
+    return out
 
 
 def profile_passes(args, w):

@@ -849,25 +849,35 @@ __global__ void __launch_bounds__(kFastThreads, FastMinB<T, N, C>::value) k_zfwd
 }
 
 // Epilogue items per thread loaded before the z inverse's transform (the
-// rest after it).  Six FP32 components: one (the 96-point tile holds two per
-// thread), so that the kernel fits the 168 registers of three CTAs per SM.
+// rest after it).  The six-component EM update: one (a 96-point FP32 tile
+// holds two per thread), so that the kernel fits the 168 registers of three
+// CTAs per SM.
 #ifndef M3D_ZINV_PF6
 #define M3D_ZINV_PF6 1
 #endif
+#ifndef M3D_ZINV_PF6_64
+#define M3D_ZINV_PF6_64 1
+#endif
 template <typename T, int C, class Epi> struct ZinvPrefetch {
-    static constexpr int value = (sizeof(T) == 4 && std::is_same<Epi, EpiEM<T, 6>>::value) ? M3D_ZINV_PF6 : 64;
+    static constexpr int value =
+        std::is_same<Epi, EpiEM<T, 6>>::value ? (sizeof(T) == 4 ? M3D_ZINV_PF6 : M3D_ZINV_PF6_64) : 64;
 };
 
 // CTAs per SM of the z inverse: FastMinB, and three for the six-component
-// FP32 EM update of the elastic sweeps (uncapped it takes 250-255 registers,
-// two CTAs per SM; capped at 168 it spills 0-16 bytes and the batch
-// workload's z inverse runs 22-28% faster).
+// EM update of the elastic sweeps (uncapped it takes 250-255 registers, two
+// CTAs per SM; capped at 168 it spills 0-16 bytes, and the batch workload's
+// z inverse runs 20-28% faster; FP64 only up to N = 64, where the cap does
+// not spill more than 16 bytes).
 #ifndef M3D_F32C6_MINB
 #define M3D_F32C6_MINB 3
 #endif
+#ifndef M3D_F64C6_MINB
+#define M3D_F64C6_MINB 3
+#endif
 template <typename T, int N, int C, class Epi> struct ZinvMinB {
-    static constexpr int value =
-        (sizeof(T) == 4 && std::is_same<Epi, EpiEM<T, 6>>::value) ? M3D_F32C6_MINB : FastMinB<T, N, C>::value;
+    static constexpr int value = std::is_same<Epi, EpiEM<T, 6>>::value
+                                     ? (sizeof(T) == 4 ? M3D_F32C6_MINB : (N <= 64 ? M3D_F64C6_MINB : 1))
+                                     : FastMinB<T, N, C>::value;
 };
 
 template <typename T, int N, int C, class Epi, class Fin>
