@@ -20,8 +20,9 @@ Workloads (synthetic, seeded; the reference project has no dataset):
               spheres of radius N/10 at inclusion fraction uniform in 5-40%,
               stiffness contrast uniform in 2-100 (inclusion E = contrast x 3 GPa,
               nu .2; matrix 3 GPa, .35); 6 unit load cases each -> full C_eff;
-              FP32 sweeps + FP64 refinement to residual 1e-6; one graph launch
-              per grid size (a step is the whole batch)
+              FP32 sweeps + FP64 refinement to residual 1e-6; one multi-RVE
+              solve (one graph launch) per grid size, the grid sizes run
+              concurrently (a step is the whole batch)
   rec171      microstructure reconstruction (recPlan + runRec(100, 0.8)) on the
               example's 171^3 grid and TPCF; a step is one runRec; value =
               voxels x phase-retrieval passes / device time
