@@ -253,6 +253,103 @@ __global__ void __launch_bounds__(kFastThreads) k_xturn_fast(GridDims g, const t
 }
 
 // ---------------------------------------------------------------------------
+// x turnaround, component-parallel: one CTA of C warps per group of CPW kz
+// columns, warp c transforming component c of the group's columns.  The
+// staged kernel above gives each warp all C components of its own columns,
+// so one warp owns C x CPW staged rows (six FP32 96-point components: 50 KB,
+// four warps per SM); here the same rows are shared by C warps (six: 24 warps
+// per SM at 96^3).  Phases, with a block barrier between them: (1) warp c
+// copies and forward-transforms component c of every column; (2) all threads
+// apply the spectral operator, one (mode, column) point at a time, to the C
+// components of the point; (3) warp c inverse-transforms and stores
+// component c.  Per line and per mode the arithmetic is the staged kernel's
+// (equal bits where the operator keeps no sums; sums of the reference stop
+// rule are added in another order).
+// ---------------------------------------------------------------------------
+template <typename T, int N, int C, int NSUM>
+constexpr size_t xturn_cp_smem() {
+    typedef typename Cx<T>::t C2;
+    constexpr int CPW = 32 / LineSplit<T, N>::Tl;
+    return (size_t)N * sizeof(C2) + (size_t)C * CPW * RowLen<T, N, true>::value * sizeof(C2) + 16 +
+           (size_t)32 * (NSUM > 0 ? NSUM : 1) * sizeof(double);
+}
+
+template <typename T, int N, int C, class Spec>
+__global__ void __launch_bounds__(32 * C) k_xturn_cp(GridDims g, const typename Cx<T>::t* __restrict__ twx,
+                                                     typename Cx<T>::t* __restrict__ spec, Spec op,
+                                                     const Ctl* __restrict__ ctl, double* partials) {
+    typedef typename Cx<T>::t C2;
+    constexpr int E = LineSplit<T, N>::E, TL = LineSplit<T, N>::Tl, CPW = 32 / TL;
+    constexpr int RL = RowLen<T, N, true>::value;
+    const int b = entry_of(g, blockIdx.y);
+    if (b < 0 || ctl[b].done) return;
+    op.prepare(ctl, b);
+    extern __shared__ __align__(16) char smem_raw[];
+    C2* tw = (C2*)smem_raw;
+    C2* stage = tw + N;  // [c][col][RL]
+    double* red = (double*)align_up((char*)(stage + C * CPW * RL), 16);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int col = lane % CPW, t = lane / CPW;
+    const int ngrp = (g.Hzp + CPW - 1) / CPW;
+    const int y = blockIdx.x / ngrp;
+    const int kz0 = (blockIdx.x - y * ngrp) * CPW;
+    const int kz = kz0 + col;
+    const bool ok = kz < g.Hzp;
+    const long long cstride = g.NL * g.Hzp;            // component stride
+    const long long xstride = (long long)g.Ny * g.Hzp;  // x stride
+    C2* cbase = spec + ((long long)b * C * g.NL + y) * g.Hzp + warp * cstride + (ok ? kz : 0);  // component `warp`
+    const int sw = RowLen<T, N, true>::sw ? (col & 1) : 0;
+    C2* row = stage + (warp * CPW + col) * RL;
+#pragma unroll
+    for (int j = 0; j < E; ++j)
+        cp_async(row + ((t + TL * j) ^ sw), cbase + (long long)(t + TL * j) * xstride, (int)sizeof(C2),
+                 ok ? (int)sizeof(C2) : 0);
+    for (int i = threadIdx.x; i < N; i += blockDim.x) tw[i] = twx[i];
+    cp_async_wait_all();
+    __syncthreads();
+    {
+        C2 v[E];
+#pragma unroll
+        for (int j = 0; j < E; ++j) v[j] = row[(t + TL * j) ^ sw];
+        __syncwarp();
+        line_fwd<C2, E, TL>(v, t, row, tw, sw);
+#pragma unroll
+        for (int r = 0; r < E; ++r) row[spec_mode<E, TL>(t, r) ^ sw] = v[r];
+    }
+    __syncthreads();
+    double acc[Spec::NSUM > 0 ? Spec::NSUM : 1] = {};
+    for (int p = threadIdx.x; p < CPW * N; p += blockDim.x) {
+        const int pc = p % CPW, mode = p / CPW;
+        const int pkz = kz0 + pc;
+        if (pkz >= g.Hz) continue;  // past the half spectrum (padding or beyond Hzp)
+        const int psw = RowLen<T, N, true>::sw ? (pc & 1) : 0;
+        C2 m[C];
+#pragma unroll
+        for (int c = 0; c < C; ++c) m[c] = stage[(c * CPW + pc) * RL + (mode ^ psw)];
+        op.apply(b, mode, y, pkz, m, acc, ctl);
+        if constexpr (Spec::kInverse) {
+#pragma unroll
+            for (int c = 0; c < C; ++c) stage[(c * CPW + pc) * RL + (mode ^ psw)] = m[c];
+        }
+    }
+    if constexpr (Spec::NSUM > 0) {
+        block_reduce_store<Spec::NSUM>(acc, red, partials, b, gridDim.x, blockIdx.x);
+    }
+    if constexpr (Spec::kInverse) {
+        __syncthreads();
+        C2 v[E];
+#pragma unroll
+        for (int r = 0; r < E; ++r) v[r] = row[spec_mode<E, TL>(t, r) ^ sw];
+        __syncwarp();
+        line_inv<C2, E, TL>(v, t, row, tw, sw);
+        if (ok) {
+#pragma unroll
+            for (int j = 0; j < E; ++j) cbase[(long long)(t + TL * j) * xstride] = v[j];
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
 // x turnaround with the three components of a column in registers (thermal
 // fields in FP32): each lane loads its E points of all three components
 // straight from global memory (every load of a warp covers CPW consecutive

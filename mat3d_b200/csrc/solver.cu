@@ -323,6 +323,9 @@ struct m3d_solver {
     bool use_xreg = true;
     // thermal x turnaround in rank-one form (M3D_XTURN_R1=0 turns it off)
     bool use_xr1 = true;
+    // six-component x turnaround with a warp per component (M3D_XTURN_CP=0:
+    // the staged kernel, all components of its columns in each warp)
+    bool use_xcp = true;
     template <typename T> bool slab_ok() const;
     template <typename T, int CC, bool MIX, class Fin>
     int pass_slab(Ctl* ctl, T* x, const float* r, typename Cx<T>::t* sp, Fin fin);
@@ -760,6 +763,16 @@ int m3d_solver::pass_x(Spec op, Ctl* ctl, typename Cx<T>::t* sp) {
                 allow_smem(k_xturn_reg<T, NN, Spec>);
                 k_xturn_reg<T, NN, Spec><<<dim3(nblk, gridB()), kXRegWarps * 32, xturn_reg_smem<T, NN, Spec::NSUM>(), stream>>>(
                     g, tw<T>(0), sp, op, ctl, d_part);
+                return;
+            }
+        }
+        if constexpr (CC == 6) {
+            if (use_xcp) {  // six components: one CTA of six warps per column group, a warp per component
+                const int ngrp = (g.Hzp + CPW - 1) / CPW;
+                nblk = Ny * ngrp;
+                allow_smem(k_xturn_cp<T, NN, CC, Spec>);
+                k_xturn_cp<T, NN, CC, Spec><<<dim3(nblk, gridB()), 32 * CC, xturn_cp_smem<T, NN, CC, Spec::NSUM>(),
+                                              stream>>>(g, tw<T>(0), sp, op, ctl, d_part);
                 return;
             }
         }
@@ -1630,6 +1643,8 @@ static int create_impl(int kind, int Nx, int Ny, int Nz, int behav, int precisio
         h->use_xr1 = !(e8 && e8[0] == '0');
         const char* e9 = std::getenv("M3D_XTURN_TMA");
         h->use_xr1_tma = !(e9 && e9[0] == '0');
+        const char* e11 = std::getenv("M3D_XTURN_CP");
+        h->use_xcp = !(e11 && e11[0] == '0');
         const char* e6 = std::getenv("M3D_XTURN_STAGED");
         h->use_xreg = !(e6 && e6[0] == '1');
     }
