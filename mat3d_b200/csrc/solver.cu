@@ -323,8 +323,9 @@ struct m3d_solver {
     bool use_xreg = true;
     // thermal x turnaround in rank-one form (M3D_XTURN_R1=0 turns it off)
     bool use_xr1 = true;
-    // six-component x turnaround with a warp per component (M3D_XTURN_CP=0:
-    // the staged kernel, all components of its columns in each warp)
+    // x turnaround with a warp per component where no rank form applies
+    // (M3D_XTURN_CP=0: the staged kernel, all components of its columns in
+    // each warp)
     bool use_xcp = true;
     template <typename T> bool slab_ok() const;
     template <typename T, int CC, bool MIX, class Fin>
@@ -766,8 +767,8 @@ int m3d_solver::pass_x(Spec op, Ctl* ctl, typename Cx<T>::t* sp) {
                 return;
             }
         }
-        if constexpr (CC == 6) {
-            if (use_xcp) {  // six components: one CTA of six warps per column group, a warp per component
+        if constexpr (CC == 6 || CC == 3) {
+            if (use_xcp) {  // one CTA of CC warps per column group, a warp per component
                 const int ngrp = (g.Hzp + CPW - 1) / CPW;
                 nblk = Ny * ngrp;
                 allow_smem(k_xturn_cp<T, NN, CC, Spec>);

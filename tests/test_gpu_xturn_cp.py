@@ -1,4 +1,4 @@
-"""The six-component x turnaround with a warp per component (`k_xturn_cp`,
+"""The x turnaround with a warp per component (`k_xturn_cp`,
 passes_fast.cuh) against the staged kernel whose warps hold all six
 components of their own columns (`M3D_XTURN_CP=0`).  Per line and per mode
 both do the same arithmetic, so the elastic linear solves (residual rule: the
