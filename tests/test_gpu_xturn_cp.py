@@ -85,3 +85,22 @@ def test_component_parallel_j2(prec, bound, monkeypatch):
     b, sb = solve(32, J2_MAT, prec, 1e-6, False, monkeypatch, behav=m3d.J2, ninc=2)
     assert abs(sa - sb) <= max(2, sb // 50), (sa, sb)
     assert rel(a, b) < bound, rel(a, b)
+
+
+@pytest.mark.parametrize("N", [48, 96, 128])
+@pytest.mark.parametrize("prec,tol", [("fp32", 1e-6), ("fp64", 1e-10)])
+def test_component_parallel_thermal(N, prec, tol, monkeypatch):
+    """Three components (the thermal operators with their rank-one kernels
+    turned off): equal bits to the staged kernel."""
+    monkeypatch.setenv("M3D_XTURN_R1", "0")
+    out = []
+    for cp in ("1", "0"):
+        monkeypatch.setenv("M3D_XTURN_CP", cp)
+        s = m3d.Solver(m3d.KIND_THERMAL, N, N, N, 0, prec, 1)
+        s.set_material_thermal(1.0, 50.0, sphere_rve(N, N / 4, (N / 2 + 1, N / 2, N / 2 - 1)))
+        s.set_load(np.array([0.2, 0.3, 1.0]))
+        s.run(tol, 0, 1, m3d.CRIT_RESIDUAL)
+        out.append((s.field(m3d.FIELD_STRAIN), s.stats()["sweeps"]))
+        s.close()
+    assert out[0][1] == out[1][1]
+    assert np.array_equal(out[0][0], out[1][0])
