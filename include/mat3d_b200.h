@@ -145,6 +145,19 @@ int m3d_homogenize(m3d_solver* h, double tol_field, double tol_eq, int criterion
 /* Copy a field of batch entry b to host memory: AoS doubles out[v*c + comp]
    (c = 6 mech, 3 thermal; scalar fields: out[v]). */
 int m3d_get_field(m3d_solver* h, int which, int b, double* out);
+/* As m3d_get_field, but returns once the copy to host memory is enqueued: the
+   field is first written, on the device, into the handle's export buffer (the
+   state may then be overwritten by the next solve at once) and read into `out`
+   on a copy stream of the handle, so the copy overlaps the handle's next work
+   (material upload, solve).  `out` must stay valid until m3d_wait_field
+   returns, and should be page-locked (pinned) memory, or the copy does not run
+   asynchronously.  A later m3d_get_field(_async) on the handle waits for the
+   pending copy before reusing the export buffer.  Inelastic fields are copied
+   synchronously.  No counterpart in the reference (its fields are host
+   arrays); it serves callers that stream results back while solving. */
+int m3d_get_field_async(m3d_solver* h, int which, int b, double* out);
+/* Wait for the handle's pending m3d_get_field_async copy (no-op if none). */
+int m3d_wait_field(m3d_solver* h);
 /* Volume averages of the strain-like and stress-like fields of entry b. */
 int m3d_get_means(m3d_solver* h, int b, double* strain_mean, double* stress_mean);
 int m3d_get_stats(const m3d_solver* h, m3d_stats* out);

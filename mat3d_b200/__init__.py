@@ -115,7 +115,7 @@ _lib = None
 # every symbol the C ABI header declares
 EXPORTS = [
     "m3d_create", "m3d_destroy", "m3d_set_material_mech", "m3d_set_material_thermal", "m3d_set_load", "m3d_run",
-    "m3d_homogenize", "m3d_get_field", "m3d_get_means", "m3d_get_stats", "m3d_get_increments",
+    "m3d_homogenize", "m3d_get_field", "m3d_get_field_async", "m3d_wait_field", "m3d_get_means", "m3d_get_stats", "m3d_get_increments",
     "m3d_status_string", "m3d_last_error", "m3d_abi_version", "m3d_get_stream", "m3d_set_stream",
     "m3d_set_profiling", "m3d_get_profile", "m3d_thermal_solve_noalloc", "m3d_get_entry_stats",
     "m3d_create_multi", "m3d_set_material_mech_rve", "m3d_set_material_thermal_rve", "m3d_footprint_bytes",
@@ -152,6 +152,8 @@ def load_library(path: str | None = None):
     L.m3d_run.argtypes = [vp, d, d, i, i, i]
     L.m3d_homogenize.argtypes = [vp, d, d, i, i, vp, vp, vp, vp]
     L.m3d_get_field.argtypes = [vp, i, i, vp]
+    L.m3d_get_field_async.argtypes = [vp, i, i, vp]
+    L.m3d_wait_field.argtypes = [vp]
     L.m3d_get_means.argtypes = [vp, i, vp, vp]
     L.m3d_get_stats.argtypes = [vp, ctypes.POINTER(Stats)]
     L.m3d_get_increments.argtypes = [vp, vp, i]
@@ -320,6 +322,20 @@ class Solver:
         _check(self.L, self.L.m3d_get_field(self.h, which, b, _ptr(out)), "get_field")
         flat = out.reshape(-1)
         return flat if scalar else flat.reshape(self.V, self.C).T  # (C, V) view of AoS data
+
+    def field_async(self, out, which=FIELD_STRAIN, b=0):
+        """Enqueue the field's copy into ``out`` (a contiguous float64 array of
+        V*C elements, page-locked for an asynchronous copy) and return at once;
+        the copy overlaps the handle's next work.  ``out`` is complete after
+        wait_field()."""
+        n = self.V * self.C
+        if out.dtype != np.float64 or out.size != n or not out.flags.c_contiguous:
+            raise ValueError(f"out must be a contiguous float64 array of {n} elements")
+        _check(self.L, self.L.m3d_get_field_async(self.h, which, b, _ptr(out)), "get_field_async")
+        return out.reshape(-1).reshape(self.V, self.C).T
+
+    def wait_field(self):
+        _check(self.L, self.L.m3d_wait_field(self.h), "wait_field")
 
     def means(self, b=0):
         e = np.zeros(self.C)

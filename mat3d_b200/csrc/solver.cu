@@ -219,6 +219,10 @@ struct m3d_solver {
     void* d_tw32 = nullptr;  // float2
     LinePlan px{}, py{}, pz{};
     double* d_out = nullptr;  // export scratch (C*V doubles)
+    // asynchronous export: copy stream, export-written and copy-done events
+    cudaStream_t xstream = nullptr;
+    cudaEvent_t ev_exp = nullptr, ev_d2h = nullptr;
+    bool d2h_pending = false;
     size_t alloc_B = 0;
 
     // inelastic state (J2 / damage)
@@ -371,6 +375,9 @@ struct m3d_solver {
     };
     GraphSlot gslot[3];  // 0: linear residual rule, 1: linear reference rule, 2: refinement
     int* d_trips = nullptr;  // [0] loop trips this run, [1] outer trips total, [2] inner trips this round, [3] inner total
+    unsigned long long* d_pstat = nullptr;  // phase-map statistics: [0, 16) counts per id, [16] id sum, [17] first bad voxel
+    int load_phase(int r, const int32_t* phase, int nph, std::vector<long long>& counts, long long& idsum,
+                   long long& bad);
     void drop_graphs() {
         for (GraphSlot& s : gslot) {
             if (s.exec) cudaGraphExecDestroy(s.exec);
@@ -404,6 +411,7 @@ void m3d_solver::free_all() {
     cudaFree(d_trips); d_trips = nullptr;
     cudaFree(d_err); d_err = nullptr;
     cudaFree(d_live); d_live = nullptr;
+    cudaFree(d_pstat); d_pstat = nullptr;
     cudaFree(d_phase); d_phase = nullptr;
     cudaFree(d_x); d_x = nullptr;
     cudaFree(d_delta); d_delta = nullptr;
@@ -1527,19 +1535,36 @@ __global__ void k_export(const TX* __restrict__ x, const uint8_t* __restrict__ p
 }
 
 template <typename TX, int CC>
-static int export_field(m3d_solver* h, const void* x, const double* mats, int b, double* host_out) {
+static int export_field(m3d_solver* h, const void* x, const double* mats, int b, double* host_out,
+                        bool async = false) {
     const long long V = h->g.V;
     if (!h->d_out) {
         cudaError_t e = cudaMalloc(&h->d_out, (size_t)6 * V * sizeof(double));
         if (e != cudaSuccess) return fail(M3D_ERR_OOM, "export buffer allocation failed");
     }
+    if (h->d2h_pending) M3D_CUDA(cudaStreamWaitEvent(h->stream, h->ev_d2h, 0));  // the pending copy reads d_out
     const int r = h->rve_of(b);
     const double* M = mats ? mats + (size_t)r * h->mstride : nullptr;
     k_export<TX, CC><<<592, 256, 0, h->stream>>>((const TX*)x, h->d_phase + (size_t)r * V, M, b, V, h->d_out);
     h->st.kernel_launches += 1;
     M3D_CUDA(cudaGetLastError());
-    M3D_CUDA(cudaMemcpyAsync(host_out, h->d_out, (size_t)CC * V * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
-    M3D_CUDA(cudaStreamSynchronize(h->stream));
+    const size_t bytes = (size_t)CC * V * sizeof(double);
+    if (!async) {
+        M3D_CUDA(cudaMemcpyAsync(host_out, h->d_out, bytes, cudaMemcpyDeviceToHost, h->stream));
+        M3D_CUDA(cudaStreamSynchronize(h->stream));
+        h->d2h_pending = false;
+        return M3D_OK;
+    }
+    if (!h->xstream) {
+        M3D_CUDA(cudaStreamCreateWithFlags(&h->xstream, cudaStreamNonBlocking));
+        M3D_CUDA(cudaEventCreateWithFlags(&h->ev_exp, cudaEventDisableTiming));
+        M3D_CUDA(cudaEventCreateWithFlags(&h->ev_d2h, cudaEventDisableTiming));
+    }
+    M3D_CUDA(cudaEventRecord(h->ev_exp, h->stream));
+    M3D_CUDA(cudaStreamWaitEvent(h->xstream, h->ev_exp, 0));
+    M3D_CUDA(cudaMemcpyAsync(host_out, h->d_out, bytes, cudaMemcpyDeviceToHost, h->xstream));
+    M3D_CUDA(cudaEventRecord(h->ev_d2h, h->xstream));
+    h->d2h_pending = true;
     return M3D_OK;
 }
 
@@ -1714,6 +1739,12 @@ int m3d_create_multi(int kind, int Nx, int Ny, int Nz, int precision, int nrve, 
 int m3d_destroy(m3d_solver* h) {
     if (!h) return M3D_OK;
     if (h->stream) cudaStreamSynchronize(h->stream);
+    if (h->xstream) {
+        cudaStreamSynchronize(h->xstream);
+        cudaStreamDestroy(h->xstream);
+        cudaEventDestroy(h->ev_exp);
+        cudaEventDestroy(h->ev_d2h);
+    }
     for (int k = 0; k <= m3d_solver::kChunk; ++k)
         if (h->pev[k]) cudaEventDestroy(h->pev[k]);
     for (int k = 0; k < m3d_solver::kChunk; ++k)
@@ -1735,6 +1766,73 @@ static void table_layout(m3d_solver* h) {
     h->off_Os = 3 * S * C * C;
     h->off_Q = 3 * S * C * C + S * C;
     h->mstride = (long long)(4 * S * C * C + S * C);
+}
+
+// The caller's int32 phase ids of one RVE -> the uint8 map the sweeps read,
+// with the statistics the material set-up needs: per id below nph its
+// voxel count, the sum of the raw ids, and the first voxel whose id is
+// outside [0, nph).  nph = 0 (thermal): any id, mapped to id != 0 and counted
+// as 0 / 1.  st: [0, 16) counts, [16] id sum (two's complement), [17] first
+// bad voxel (initialised to all ones).
+__global__ void k_phase_in(const int32_t* __restrict__ ids, uint8_t* __restrict__ out, long long V, int nph,
+                           unsigned long long* st) {
+    __shared__ unsigned long long hist[kMaxPhases];
+    if (threadIdx.x < kMaxPhases) hist[threadIdx.x] = 0;
+    __syncthreads();
+    long long sum = 0;
+    unsigned long long bad = ~0ull;
+    for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < V; v += (long long)gridDim.x * blockDim.x) {
+        const int id = ids[v];
+        sum += id;
+        if (nph == 0) {
+            const int p = id != 0 ? 1 : 0;
+            out[v] = (uint8_t)p;
+            atomicAdd(&hist[p], 1ull);
+        } else if (id >= 0 && id < nph) {
+            out[v] = (uint8_t)id;
+            atomicAdd(&hist[id], 1ull);
+        } else if ((unsigned long long)v < bad) {
+            bad = (unsigned long long)v;
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        sum += __shfl_down_sync(0xffffffffu, sum, o);
+        const unsigned long long ob = __shfl_down_sync(0xffffffffu, bad, o);
+        bad = ob < bad ? ob : bad;
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicAdd(&st[kMaxPhases], (unsigned long long)sum);
+        if (bad != ~0ull) atomicMin(&st[kMaxPhases + 1], bad);
+    }
+    __syncthreads();
+    if (threadIdx.x < kMaxPhases && hist[threadIdx.x]) atomicAdd(&st[threadIdx.x], hist[threadIdx.x]);
+}
+
+// RVE r's phase map from the caller's int32 ids, converted on the device: the
+// ids are copied into the spectrum buffer, which holds nothing between solves
+// (every solve writes it before reading it) and always has room for them
+// (>= 12 bytes per voxel), then k_phase_in writes the map and the statistics.
+int m3d_solver::load_phase(int r, const int32_t* phase, int nph, std::vector<long long>& counts, long long& idsum,
+                           long long& bad) {
+    const long long V = g.V;
+    if (!d_pstat) M3D_CUDA(cudaMalloc(&d_pstat, (kMaxPhases + 2) * sizeof(unsigned long long)));
+    M3D_CUDA(cudaMemsetAsync(d_pstat, 0, (kMaxPhases + 1) * sizeof(unsigned long long), stream));
+    M3D_CUDA(cudaMemsetAsync(d_pstat + kMaxPhases + 1, 0xff, sizeof(unsigned long long), stream));
+    int32_t* ids = (int32_t*)d_spec;
+    M3D_CUDA(cudaMemcpyAsync(ids, phase, (size_t)V * sizeof(int32_t), cudaMemcpyHostToDevice, stream));
+    const int nblk = (int)std::min<long long>((V + 255) / 256, 148 * 8);
+    k_phase_in<<<nblk, 256, 0, stream>>>(ids, d_phase + (size_t)r * V, V, nph, d_pstat);
+    M3D_CUDA(cudaGetLastError());
+    unsigned long long hs[kMaxPhases + 2];
+    M3D_CUDA(cudaMemcpyAsync(hs, d_pstat, sizeof(hs), cudaMemcpyDeviceToHost, stream));
+    M3D_CUDA(cudaStreamSynchronize(stream));
+    const int np = nph == 0 ? 2 : nph;
+    counts.assign(np, 0);
+    for (int i = 0; i < np; ++i) counts[i] = (long long)hs[i];
+    idsum = (long long)hs[kMaxPhases];
+    bad = hs[kMaxPhases + 1] == ~0ull ? -1 : (long long)hs[kMaxPhases + 1];
+    return M3D_OK;
 }
 
 static int upload_tables(m3d_solver* h, int r) {
@@ -1762,13 +1860,13 @@ int m3d_set_material_mech_rve(m3d_solver* h, int r, const double* mat, int nph, 
     if (nph < 1 || nph > kMaxPhases) return fail(M3D_ERR_ARG, "nph must be in [1, 16]");
     if (scheme < 0 || scheme > 2) return fail(M3D_ERR_ARG, "invalid scheme");
     const long long V = h->g.V;
-    std::vector<uint8_t> ph8(V);
-    h->counts.assign(nph, 0);
-    for (long long v = 0; v < V; ++v) {
-        const int id = phase[v];
-        if (id < 0 || id >= nph) return fail(M3D_ERR_ARG, "phase id out of range at voxel " + std::to_string(v));
-        ph8[v] = (uint8_t)id;
-        h->counts[id]++;
+    long long idsum = 0, bad = -1;
+    int prc = h->load_phase(r, phase, nph, h->counts, idsum, bad);
+    if (prc) return prc;
+    if (bad >= 0) {  // RVE r's device map is now incomplete: the RVE counts as not set
+        h->rv[r].set = false;
+        h->material_set = false;
+        return fail(M3D_ERR_ARG, "phase id out of range at voxel " + std::to_string(bad));
     }
     h->nph = nph;
     h->mat.assign(mat, mat + nph * 7);
@@ -1832,7 +1930,6 @@ int m3d_set_material_mech_rve(m3d_solver* h, int r, const double* mat, int nph, 
     h->den_ref = (h->scheme == 1) ? 0.5 * h->Cp[0][0] + 0.5 * h->Cp[p1][0] : 0.5 * h->Sp[0][0] + 0.5 * h->Sp[p1][0];
     int rc = upload_tables(h, r);
     if (rc) return rc;
-    M3D_CUDA(cudaMemcpyAsync(h->d_phase + (size_t)r * V, ph8.data(), (size_t)V, cudaMemcpyHostToDevice, h->stream));
     M3D_CUDA(cudaStreamSynchronize(h->stream));
     h->snapshot_rve(r);
     h->material_set = h->all_rves_set();
@@ -1858,16 +1955,10 @@ int m3d_set_material_thermal_rve(m3d_solver* h, int r, double km, double ki, con
     if (!(km > 0) || !(ki > 0)) return fail(M3D_ERR_ARG, "conductivities must be positive");
     if (scheme < 0 || scheme > 2) return fail(M3D_ERR_ARG, "invalid scheme");
     const long long V = h->g.V;
-    std::vector<uint8_t> ph8(V);
-    h->counts.assign(2, 0);
-    long long idsum = 0;
-    for (long long v = 0; v < V; ++v) {
-        const int id = phase[v];
-        idsum += id;
-        // multipKx()/strainUpdate() test `if (RVE(i))` (src/3dTherm/FFT_thermal3D.cpp:186,249)
-        ph8[v] = id != 0 ? 1 : 0;
-        h->counts[ph8[v]]++;
-    }
+    // multipKx()/strainUpdate() test `if (RVE(i))` (src/3dTherm/FFT_thermal3D.cpp:186,249): map id != 0 to 1
+    long long idsum = 0, bad = -1;
+    int prc = h->load_phase(r, phase, 0, h->counts, idsum, bad);
+    if (prc) return prc;
     h->nph = 2;
     h->km = km;
     h->ki = ki;
@@ -1900,7 +1991,6 @@ int m3d_set_material_thermal_rve(m3d_solver* h, int r, double km, double ki, con
     h->den_ref = (h->scheme == 1) ? 0.5 * ki + 0.5 * km : 0.5 / ki + 0.5 / km;  // (:346, :356)
     int rc = upload_tables(h, r);
     if (rc) return rc;
-    M3D_CUDA(cudaMemcpyAsync(h->d_phase + (size_t)r * V, ph8.data(), (size_t)V, cudaMemcpyHostToDevice, h->stream));
     M3D_CUDA(cudaStreamSynchronize(h->stream));
     h->snapshot_rve(r);
     h->material_set = h->all_rves_set();
@@ -2099,23 +2189,48 @@ static int assemble_rve(m3d_solver* h, int r, double* Ceff, double* Seff, double
     return M3D_OK;
 }
 
+static int get_field_impl(m3d_solver* h, int which, int b, double* out, bool async);
+
 extern "C" {
 
-int m3d_get_field(m3d_solver* h, int which, int b, double* out) {
+int m3d_get_field(m3d_solver* h, int which, int b, double* out) { return get_field_impl(h, which, b, out, false); }
+
+int m3d_get_field_async(m3d_solver* h, int which, int b, double* out) {
+    return get_field_impl(h, which, b, out, true);
+}
+
+int m3d_wait_field(m3d_solver* h) {
+    if (!h) return fail(M3D_ERR_ARG, "NULL handle");
+    if (h->d2h_pending) {
+        M3D_CUDA(cudaEventSynchronize(h->ev_d2h));
+        h->d2h_pending = false;
+    }
+    return M3D_OK;
+}
+
+}  // extern "C"
+
+static int get_field_impl(m3d_solver* h, int which, int b, double* out, bool async) {
     if (!h || !out) return fail(M3D_ERR_ARG, "NULL argument");
     if (!h->run_done) return fail(M3D_ERR_STATE, "no finished run");
     if (b < 0 || b >= h->B) return fail(M3D_ERR_ARG, "batch index out of range");
-    if (h->kind == M3D_KIND_MECH && h->behav != M3D_BEHAV_ELASTIC) return h->in.get_field(h, which, b, out);
+    if (h->kind == M3D_KIND_MECH && h->behav != M3D_BEHAV_ELASTIC) {  // synchronous, after any pending copy
+        if (h->d2h_pending) {
+            M3D_CUDA(cudaEventSynchronize(h->ev_d2h));
+            h->d2h_pending = false;
+        }
+        return h->in.get_field(h, which, b, out);
+    }
     if (which != M3D_FIELD_STRAIN && which != M3D_FIELD_STRESS)
         return fail(M3D_ERR_ARG, "field not available for this behaviour");
     const bool state = (which == M3D_FIELD_STRAIN) == (h->rv[h->rve_of(b)].scheme == 1);
     const double* M = state ? nullptr : h->d_mats + h->off_O;
     if (h->C == 6)
-        return h->prec == M3D_PREC_FP32 ? export_field<float, 6>(h, h->d_x, M, b, out) : export_field<double, 6>(h, h->d_x, M, b, out);
-    return h->prec == M3D_PREC_FP32 ? export_field<float, 3>(h, h->d_x, M, b, out) : export_field<double, 3>(h, h->d_x, M, b, out);
+        return h->prec == M3D_PREC_FP32 ? export_field<float, 6>(h, h->d_x, M, b, out, async)
+                                        : export_field<double, 6>(h, h->d_x, M, b, out, async);
+    return h->prec == M3D_PREC_FP32 ? export_field<float, 3>(h, h->d_x, M, b, out, async)
+                                    : export_field<double, 3>(h, h->d_x, M, b, out, async);
 }
-
-}  // extern "C"
 
 // ---- autotuner ----------------------------------------------------------------
 // Launch schedules that give identical arithmetic per line but run at

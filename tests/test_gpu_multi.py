@@ -203,3 +203,35 @@ def test_batch_budget_too_small():
     with pytest.raises(m3d.M3DError):
         bt.homogenize(1e-8)
     bt.close()
+
+
+def test_phase_map_ids_on_device():
+    """The phase map is converted on the device: an id outside [0, nph) is
+    reported at its first voxel and leaves the RVE unset (a solve is refused
+    until it is set again); thermal ids are tested only for != 0, so a map of
+    0/5 gives the field of the same map as 0/1 under the same scheme."""
+    N = 16
+    rve = sphere_rve((N, N, N), 4.0)
+    bad = rve.copy()
+    bad[37] = 2
+    bad[900] = -1
+    s = m3d.Solver(m3d.KIND_MECH, N, N, N, m3d.ELASTIC, "fp64", 1)
+    s.set_material_mech(mech_mat(5.0), rve)
+    with pytest.raises(m3d.M3DError) as ei:
+        s.set_material_mech(mech_mat(5.0), bad)
+    assert "at voxel 37" in str(ei.value)
+    s.set_load(np.array([1e-3, 0, 0, 0, 0, 0.0]))
+    with pytest.raises(m3d.M3DError):
+        s.run(1e-8, 1e-8, 1, m3d.CRIT_RESIDUAL)
+    s.set_material_mech(mech_mat(5.0), rve)
+    s.run(1e-8, 1e-8, 1, m3d.CRIT_RESIDUAL)
+    s.close()
+    out = []
+    for ids in (rve, rve * 5):
+        t = m3d.Solver(m3d.KIND_THERMAL, N, N, N, 0, "fp64", 1)
+        t.set_material_thermal(1.0, 20.0, ids, m3d.SCHEME_PRIMAL)
+        t.set_load(np.array([0.0, 0.0, 1.0]))
+        t.run(1e-10, 0, 1, m3d.CRIT_RESIDUAL)
+        out.append(t.field(m3d.FIELD_STRAIN))
+        t.close()
+    assert np.array_equal(out[0], out[1])
