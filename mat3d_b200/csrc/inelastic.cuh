@@ -36,6 +36,11 @@ __device__ __forceinline__ double vonmises(const double (&s)[6], double (&sd)[6]
                                 2 * sd[5] * sd[5]);
 }
 
+// x^n of the hardening law H ep^n: linear hardening (n = 1, and n - 1 = 0
+// in the Newton derivative) needs no pow call, which in FP64 costs more than
+// the rest of the update.
+__device__ __forceinline__ double hpow(double x, double n) { return n == 1.0 ? x : (n == 0.0 ? 1.0 : pow(x, n)); }
+
 // J2 return map (elastoPlastic, :640-691).  Returns dp (0 when elastic), sets
 // sig, phi.  NR on the plastic multiplier from 0 with the reference's absolute
 // tolerance 1e-5 on the yield function, capped at 200 steps (*nr_fail set).
@@ -54,15 +59,15 @@ __device__ __forceinline__ double j2_update(const PhaseMech& P, const double (&e
     }
     double sd[6];
     const double seff = vonmises(sig, sd);
-    phi = seff - P.Sy - P.H * pow(ep, P.n);
+    phi = seff - P.Sy - P.H * hpow(ep, P.n);
     if (!(phi > 0)) return 0.0;
     double x = 0, xo = 0;
     int it = 0;
     for (;;) {
-        x = xo - (seff - 3 * P.mu * xo - P.Sy - P.H * pow(ep + xo, P.n)) /
-                     (-3 * P.mu - P.H * P.n * pow(ep + xo, P.n - 1));
+        x = xo - (seff - 3 * P.mu * xo - P.Sy - P.H * hpow(ep + xo, P.n)) /
+                     (-3 * P.mu - P.H * P.n * hpow(ep + xo, P.n - 1));
         xo = x;
-        const double res = seff - 3 * P.mu * x - P.Sy - P.H * pow(ep + x, P.n);
+        const double res = seff - 3 * P.mu * x - P.Sy - P.H * hpow(ep + x, P.n);
         if (!(x == x)) { *nr_fail = 1; break; }
         if (fabs(res) < 1e-5) break;
         if (++it >= 200) { *nr_fail = 1; break; }
@@ -141,30 +146,50 @@ struct EpiConstitutive {
         const int n = p.nph * (int)(sizeof(PhaseMech) / sizeof(double));
         for (int i = threadIdx.x; i < n; i += blockDim.x) dst[i] = src[i];
     }
+    // a voxel's inputs: phase, state, and (J2) the last increment's strain,
+    // stress and equivalent plastic strain, or (damage) the damage variable
+    struct In {
+        int k;
+        double e[6], eo[6], so[6], ep;
+    };
+    __device__ __forceinline__ In load(long long v) const {
+        In q;
+        q.k = p.phase[v];
+        const long long V = p.V;
+#pragma unroll
+        for (int c = 0; c < 6; ++c) q.e[c] = eb[c * V + v];
+        if (p.behav == BEHAV_J2) {
+#pragma unroll
+            for (int c = 0; c < 6; ++c) {
+                q.eo[c] = eob[c * V + v];
+                q.so[c] = sob[c * V + v];
+            }
+            q.ep = epb[v];
+        } else {
+            q.ep = db[v];
+        }
+        return q;
+    }
     // xc: increment from the inverse transform (zero for the standalone update)
-    __device__ __forceinline__ void apply(int, long long v, const T (&xc)[6], double* acc) const {
-        const int k = p.phase[v];
-        const PhaseMech& P = sm[k];
+    __device__ __forceinline__ void apply(int b, long long v, const T (&xc)[6], double* acc) const {
+        apply_in(load(v), v, xc, acc);
+    }
+    __device__ __forceinline__ void apply_in(const In& q, long long v, const T (&xc)[6], double* acc) const {
+        const PhaseMech& P = sm[q.k];
         const long long V = p.V;
         double e[6], sg[6];
         double dd = 0;
 #pragma unroll
         for (int c = 0; c < 6; ++c) {
             const double inc = (double)xc[c];
-            e[c] = (double)eb[c * V + v] + inc;
+            e[c] = q.e[c] + inc;
             dd += ((c >= 3) ? 2.0 : 1.0) * inc * inc;
         }
         if (p.behav == BEHAV_J2) {
-            double eo[6], so[6];
-#pragma unroll
-            for (int c = 0; c < 6; ++c) {
-                eo[c] = (double)eob[c * V + v];
-                so[c] = (double)sob[c * V + v];
-            }
             double phi;
-            j2_update(P, e, eo, so, (double)epb[v], sg, phi, p.nr_fail);
+            j2_update(P, e, q.eo, q.so, q.ep, sg, phi, p.nr_fail);
         } else {
-            double d = db[v];
+            double d = q.ep;
             damage_update(P, e, d, sg);
             db[v] = d;
         }
@@ -235,15 +260,22 @@ struct SpecBasic {
 // The z-inverse epilogue wrapper: increment = xc (already scaled by 1/V).
 template <typename T>
 struct EpiBasic {
+    static constexpr bool kJ2 = true;  // the inelastic update (its z inverse's CTAs per SM: M3D_J2_MINB)
     static constexpr int NSUM = 13;
-    static constexpr bool kPrefetch = false;  // 19 values per voxel: loaded at use
+    // 19 values per voxel.  FP64 transforms: one voxel's inputs prefetched
+    // before the transform, then each next voxel's while the current one is
+    // updated (j2_256 in FP64: 9.81 -> 9.28 s per solve).  FP32 transforms:
+    // loaded at use (the rolling prefetch measured 19% slower there: 2.26 ->
+    // 2.69 ms per 256^3 z inverse, at 240 instead of 180 registers).
+    static constexpr bool kPrefetch = sizeof(T) == 8;
+    static constexpr bool kRolling = sizeof(T) == 8;
     static constexpr int kW = 1;
     EpiConstitutive<T> c;
-    struct Pre {};
+    typedef typename EpiConstitutive<T>::In Pre;
     __device__ __forceinline__ void bind(int b) { c.bind(b); }
-    __device__ __forceinline__ Pre load(int, long long) const { return Pre{}; }
-    __device__ __forceinline__ void apply_pre(const Pre&, int b, long long v, T (&xc)[6], double* acc) const {
-        c.apply(b, v, xc, acc);
+    __device__ __forceinline__ Pre load(int, long long v) const { return c.load(v); }
+    __device__ __forceinline__ void apply_pre(const Pre& q, int, long long v, T (&xc)[6], double* acc) const {
+        c.apply_in(q, v, xc, acc);
     }
     __device__ __forceinline__ void load_smem(char* s, int b = 0) { c.load_smem(s, b); }
     __device__ __forceinline__ void apply(int b, long long v, T (&xc)[6], double* acc) const { c.apply(b, v, xc, acc); }

@@ -955,9 +955,17 @@ __global__ void __launch_bounds__(kFastThreads, FastMinB<T, N, C>::value) k_zfwd
 #ifndef M3D_ZINV_PF6_64
 #define M3D_ZINV_PF6_64 1
 #endif
+template <class Epi, class = void> struct EpiIsJ2 { static constexpr bool value = false; };
+template <class Epi> struct EpiIsJ2<Epi, decltype((void)Epi::kJ2, void())> { static constexpr bool value = true; };
+// epilogues that load each next item while the current one is processed
+template <class Epi, class = void> struct EpiRolling { static constexpr bool value = false; };
+template <class Epi> struct EpiRolling<Epi, decltype((void)Epi::kRolling, void())> {
+    static constexpr bool value = Epi::kRolling;
+};
 template <typename T, int C, class Epi> struct ZinvPrefetch {
     static constexpr int value =
-        std::is_same<Epi, EpiEM<T, 6>>::value ? (sizeof(T) == 4 ? M3D_ZINV_PF6 : M3D_ZINV_PF6_64) : 64;
+        std::is_same<Epi, EpiEM<T, 6>>::value ? (sizeof(T) == 4 ? M3D_ZINV_PF6 : M3D_ZINV_PF6_64)
+                                              : (EpiIsJ2<Epi>::value ? 1 : 64);
 };
 
 // CTAs per SM of the z inverse: FastMinB, and three for the six-component
@@ -971,10 +979,13 @@ template <typename T, int C, class Epi> struct ZinvPrefetch {
 #ifndef M3D_F64C6_MINB
 #define M3D_F64C6_MINB 3
 #endif
+#ifndef M3D_J2_MINB
+#define M3D_J2_MINB 1
+#endif
 template <typename T, int N, int C, class Epi> struct ZinvMinB {
     static constexpr int value = std::is_same<Epi, EpiEM<T, 6>>::value
                                      ? (sizeof(T) == 4 ? M3D_F32C6_MINB : (N <= 64 ? M3D_F64C6_MINB : 1))
-                                     : FastMinB<T, N, C>::value;
+                                     : (EpiIsJ2<Epi>::value ? M3D_J2_MINB : FastMinB<T, N, C>::value);
 };
 
 template <typename T, int N, int C, class Epi, class Fin>
@@ -1065,12 +1076,28 @@ __global__ void __launch_bounds__(kFastThreads, ZinvMinB<T, N, C, Epi>::value) k
     __syncthreads();
     const T invV = (T)(1.0 / (double)g.V);
     double acc[Epi::NSUM > 0 ? Epi::NSUM : 1] = {};
+    constexpr bool ROLL = W == 1 && Epi::kPrefetch && EpiRolling<Epi>::value && PF < PERW;
+    typename PreOf<Epi>::type roll;  // rolling epilogues: the next item's inputs
+    if constexpr (ROLL) {
+        const int i = (threadIdx.x + PF * kFastThreads) * W;
+        const int gi = i / N;
+        if (i < Z::TOT && l0 + gi < g.NL) roll = epi.load(b, (l0 + gi) * N + (i - gi * N));
+    }
 #pragma unroll
     for (int k = 0; k < PERW; ++k) {
         const int i = (threadIdx.x + k * kFastThreads) * W;
         if (i >= Z::TOT) break;
         const int gi = i / N, z0 = i - gi * N;
         const long long l = l0 + gi;
+        typename PreOf<Epi>::type cur;
+        if constexpr (ROLL) {
+            if (k >= PF) {
+                cur = roll;
+                const int i1 = i + kFastThreads * W;
+                const int g1 = i1 / N;
+                if (k + 1 < PERW && i1 < Z::TOT && l0 + g1 < g.NL) roll = epi.load(b, (l0 + g1) * N + (i1 - g1 * N));
+            }
+        }
         if (l >= g.NL) continue;
         T xc[W][C];
 #pragma unroll
@@ -1088,6 +1115,7 @@ __global__ void __launch_bounds__(kFastThreads, ZinvMinB<T, N, C, Epi>::value) k
             else epi.apply_prew(epi.loadw(l * N + z0), l * N + z0, xc, acc);
         } else if constexpr (Epi::kPrefetch) {
             if (k < PF) epi.apply_pre(pre[k < PF ? k : 0], b, l * N + z0, xc[0], acc);
+            else if constexpr (ROLL) epi.apply_pre(cur, b, l * N + z0, xc[0], acc);
             else epi.apply_pre(epi.load(b, l * N + z0), b, l * N + z0, xc[0], acc);
         } else {
             epi.apply(b, l * N + z0, xc[0], acc);

@@ -205,15 +205,21 @@ int m3d_solver::run_inelastic(double tol_field, double tol_eq, int nInc, int cri
         for (;;) {
             for (int k = 0; k < chunk; ++k) {
                 prof_mark(k);
+                prof_pass(0);
                 pass_zfwd<T, 6>(pro, d_ctl, sp);
+                prof_pass(1);
                 pass_y<T>(-1, 6, d_ctl, sp);
+                prof_pass(2);
                 const int xblk = pass_x<T, 6>(spec, d_ctl, sp);
                 if (criterion == M3D_CRIT_REFERENCE) {
                     k_finalize_j2<<<B, 256, 0, stream>>>(d_ctl, d_part, 2, xblk, POLJ2_CHECK, (double)V, in.d_S0);
                     st.kernel_launches += 1;
                 }
+                prof_pass(3);
                 pass_y<T>(+1, 6, d_ctl, sp);
+                prof_pass(4);
                 pass_zinv<T, 6>(epi, d_ctl, sp, FinJ2{POLJ2_SWEEP, (double)V, in.d_S0, d_counter});
+                prof_pass(5);
             }
             M3D_CUDA(cudaGetLastError());
             prof_mark(chunk);
