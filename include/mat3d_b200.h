@@ -219,8 +219,11 @@ int m3d_thermal_solve_noalloc(int Nx, int Ny, int Nz, double km, double ki, cons
    cases in one graph launch); the groups of different grid sizes run
    concurrently (one host thread and CUDA stream each) when they fit the
    device-memory budget together, else one after another, each split only
-   where the budget requires.  device_ms is the span from the first group's
-   start to the last group's end on the device. */
+   where the budget requires.  Each group's handle is created, its materials
+   set, its schedule tuned (m3d_batch_set_autotune) and its solve graph
+   captured (a one-sweep solve) before the timed launches; device_ms is the
+   span from the first group's start to the last group's end on the device,
+   wall_ms the whole call. */
 typedef struct m3d_batch m3d_batch;
 typedef struct {
     long long sweeps, sweeps_fp64, sweeps_fp32;  /* summed over all entries (RVE x load case) */

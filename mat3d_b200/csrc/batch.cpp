@@ -273,7 +273,7 @@ int m3d_batch_homogenize(m3d_batch* b, double tol_field, int max_iter, double* C
     if (together)
         for (GroupPlan& gp : plans) gp.R = (int)gp.ids.size();
     // handles of the first chunks, materials set and (sequentially, on an idle
-    // device) the schedules tuned
+    // device) the schedules tuned and the solve graphs captured
     for (GroupPlan& gp : plans) {
         const int r = std::min<int>(gp.R, (int)gp.ids.size());
         rc = m3d_create_multi(b->kind, gp.Nx, gp.Ny, gp.Nz, b->prec, r, C, &gp.h);
@@ -286,6 +286,12 @@ int m3d_batch_homogenize(m3d_batch* b, double tol_field, int max_iter, double* C
             rc = m3d_autotune(gp.h, 3, &t);
             if (rc) break;
             b->st.autotuned += 1;
+        }
+        // capture the handle's solve graph now (a one-sweep solve), so that
+        // the group's timed launch below carries no host-side capture
+        {
+            const int hs = m3d_homogenize(gp.h, tol_field, 0, M3D_CRIT_RESIDUAL, 1, nullptr, nullptr, nullptr, nullptr);
+            if (hs != M3D_OK && hs != M3D_NOT_CONVERGED) { rc = hs; break; }
         }
         if (cudaEventCreate(&gp.e0) != cudaSuccess || cudaEventCreate(&gp.e1) != cudaSuccess) {
             rc = bfail(M3D_ERR_CUDA, "event creation failed");
