@@ -979,13 +979,18 @@ template <typename T, int C, class Epi> struct ZinvPrefetch {
 #ifndef M3D_F64C6_MINB
 #define M3D_F64C6_MINB 3
 #endif
+// CTAs per SM of the inelastic update's z inverse in FP32 (1: uncapped, 180
+// registers; a 168-register cap for three CTAs timed 2202-2458 us per 256^3
+// launch against 2256-2274 us uncapped, no reliable gain).  FP64 keeps its
+// 240 registers for the rolling prefetch (a 168 cap spills 2.4 KB).
 #ifndef M3D_J2_MINB
 #define M3D_J2_MINB 1
 #endif
 template <typename T, int N, int C, class Epi> struct ZinvMinB {
     static constexpr int value = std::is_same<Epi, EpiEM<T, 6>>::value
                                      ? (sizeof(T) == 4 ? M3D_F32C6_MINB : (N <= 64 ? M3D_F64C6_MINB : 1))
-                                     : (EpiIsJ2<Epi>::value ? M3D_J2_MINB : FastMinB<T, N, C>::value);
+                                     : (EpiIsJ2<Epi>::value ? (sizeof(T) == 4 ? M3D_J2_MINB : 1)
+                                                            : FastMinB<T, N, C>::value);
 };
 
 template <typename T, int N, int C, class Epi, class Fin>
