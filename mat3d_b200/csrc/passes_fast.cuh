@@ -274,8 +274,15 @@ constexpr size_t xturn_cp_smem() {
            (size_t)32 * (NSUM > 0 ? NSUM : 1) * sizeof(double);
 }
 
+// CTAs per SM of the six-component FP32 kernel at N = 96: three (a cap of
+// 112 registers instead of 152, 140 bytes of spill; the batch workload's
+// 96^3 group's x turnaround 157 -> 142 ms on one box, bitwise the same).  At
+// 64^3 the same cap timed equal; FP64 and N = 256 spill up to 1 KB under it.
+#ifndef M3D_XCP_MINB
+#define M3D_XCP_MINB 3
+#endif
 template <typename T, int N, int C, class Spec>
-__global__ void __launch_bounds__(32 * C) k_xturn_cp(GridDims g, const typename Cx<T>::t* __restrict__ twx,
+__global__ void __launch_bounds__(32 * C, (C == 6 && sizeof(T) == 4 && N == 96) ? M3D_XCP_MINB : 1) k_xturn_cp(GridDims g, const typename Cx<T>::t* __restrict__ twx,
                                                      typename Cx<T>::t* __restrict__ spec, Spec op,
                                                      const Ctl* __restrict__ ctl, double* partials) {
     typedef typename Cx<T>::t C2;
