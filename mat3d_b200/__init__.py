@@ -135,7 +135,9 @@ EXPORTS = [
 
 
 def load_library(path: str | None = None):
-    """Load libmat3d_b200.so (built in-tree by ``python -m mat3d_b200.build``)."""
+    """Load libmat3d_b200.so (built in-tree by ``python -m mat3d_b200.build``).
+    With ``path``, load that build instead and use it for every object created
+    afterwards."""
     global _lib
     if _lib is not None and path is None:
         return _lib
@@ -232,8 +234,7 @@ def load_library(path: str | None = None):
     L.m3drec_save_images.argtypes = [vp, ctypes.c_char_p]
     L.m3drec_write_vti.argtypes = [vp, ctypes.c_char_p, vp]
     L.m3drec_fft3.argtypes = [vp, vp, i, i, i, i, i]
-    if path is None:
-        _lib = L
+    _lib = L
     return L
 
 
